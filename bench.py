@@ -1,0 +1,333 @@
+"""Throughput of the OpenCFD-Comb hot path on B200: Mcell-steps/s of whole reference time steps
+(two RK3 flow half-steps, chemistry between them when the workload reacts).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--workload flatplate|isotropic]
+  python bench.py --impl reference ...      (the reference algorithm on the host cores)
+
+Workload (default): the Mach 2.25 flat-plate boundary layer, 1024x160x128 cells, HYBRID
+UD7L/WENO7/WENO5 with the pressure sensor, CD6 viscous terms, Steger-Warming splitting,
+boundary-layer boundary conditions with the Rai blowing/suction strip, seeded synthetic state.
+Multi-GPU runs are independent replicas (one per rank, weak scaling): the single-rank solver has
+no exchange step, so no collective is invented; ranks meet only for the timing barrier and the
+max-over-ranks reduction.
+
+The device-resident number (value) times K graph-replayed steps with CUDA events on the library
+stream; the state (several GB) is far larger than the 126 MB L2, so no flush is needed. e2e times
+the same steps through the C ABI with the state uploaded from pinned host memory and the
+conserved variables downloaded every step. The roofline object names the kernel class with the
+largest share of a step, timed live with per-launch CUDA events.
+"""
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "opencfd-comb_b200"))
+
+METRIC = "Mcell-steps/s on 1 B200: plain FP64 vs surrogate chemistry at ≤1% T error"
+UNIT = "Mcell-steps/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=40)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="flatplate", choices=["flatplate", "isotropic"])
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--e2e-steps", type=int, default=5)
+    return ap.parse_args()
+
+
+def make_case(workload, nz=None):
+    from ocfd_b200 import cases
+    if workload == "isotropic":
+        return cases.isotropic(n=64), "isotropic-64^3-WENO5-CD6-SW (decaying turbulence, M_t 0.3, Re_lambda 70)"
+    c = cases.flatplate(nx=1024, ny=160, nz=nz or 128, scheme="HYBRID")
+    return c, "flatplate-1024x160x%d-M2.25-HYBRID(UD7L/WENO7/WENO5)-CD6-SW-BoundaryLayerBC" % (nz or 128)
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as fh:
+            d = json.load(fh)
+        return d.get("hbm_gbs", 6650.0), "measured"
+    return 6650.0, "fallback"
+
+
+class Clocks:
+    """nvidia-smi sampling of SM clocks and throttle reasons during the timed region."""
+
+    def __init__(self, gpu_index=0):
+        self.samples = []
+        self.proc = None
+        self.idx = gpu_index
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.idx),
+                 "--query-gpu=clocks.sm,clocks.max.sm,clocks_event_reasons.hw_slowdown,"
+                 "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_power_cap", "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.samples.append([x.strip() for x in line.split(",")])
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]
+        mx = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for s in self.samples for k in range(4) if len(s) > 2 + k and "Active" in s[2 + k]
+                          and "Not" not in s[2 + k]})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.samples)}
+
+
+# algorithmic bytes per cell of one launch of each kernel class (double precision):
+#  flux_x : read d,u,v,w,p,Et (6) ; write du (5)                          = 11 doubles
+#  flux_y / flux_z : read d,u,v,w,p,Et (6) ; read + write du (10)         = 16 doubles
+#  visc_ev: read u,v,w,T,d,di (6) ; write Ev1..Ev3 (12)                   = 18 doubles
+#  visc_div: read Ev (12) ; read + write du(2..5) (8)                     = 20 doubles
+#  rk_prims: read f,fn,du,di,d (17) ; write f,d,u,v,w,T,p,Et,di (13)      = 30 doubles
+ALG_BYTES_PER_CELL = {"flux_x": 88, "flux_y": 128, "flux_z": 128, "visc_ev": 144, "visc_div": 160,
+                      "rk_prims": 240}
+
+
+def main_reference(a):
+    """The reference's algorithm on the host cores: the C++ restatement of the Fortran (no
+    Fortran compiler exists on this image, so the reference binary itself cannot be built)."""
+    if int(os.environ.get("RANK", "0")) != 0:
+        return 0
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle
+    cores = pyoracle.lib().ocfd_cpu_set_threads(os.cpu_count() or 1)
+    # size the per-step sample so that warmup + steps take about two minutes
+    probe, _ = make_case(a.workload, nz=8) if a.workload == "flatplate" else make_case(a.workload)
+    o = pyoracle.OracleSolver(probe)
+    o.init_state()
+    t0 = time.perf_counter()
+    o.step(probe.dt, 0.0)
+    rate = probe.ncell / (time.perf_counter() - t0)
+    o.close()
+    if a.workload == "flatplate":
+        nz = int(max(8, min(128, 120.0 * rate / (1024 * 160 * (a.steps + a.warmup)))))
+        c, name = make_case(a.workload, nz=nz)
+        sample = "per step: one full time step of a 1024x160x%d slab of the workload (z periodic)" % nz
+    else:
+        c, name = make_case(a.workload)
+        sample = "per step: one full time step of the 64^3 workload"
+    o = pyoracle.OracleSolver(c)
+    o.init_state()
+    for s in range(a.warmup):
+        o.step(c.dt, s * c.dt)
+    t0 = time.perf_counter()
+    for s in range(a.steps):
+        o.step(c.dt, (a.warmup + s) * c.dt)
+    el = time.perf_counter() - t0
+    o.close()
+    val = c.ncell * a.steps / el / 1e6
+    out = {"metric": METRIC, "value": val, "unit": UNIT, "n_gpus": a.gpus, "steps": a.steps, "warmup": a.warmup,
+           "ms_per_step": el * 1e3 / a.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+           "dtype": "f64", "data": "synthetic (seeded)", "impl": "reference",
+           "config": {"workload": make_case(a.workload, nz=8)[1].replace("x8-", "x128-") if a.workload == "flatplate" else name,
+                      "sample_cells": c.ncell},
+           "cpu_baseline": {"value": val, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample},
+           "e2e": {"value": val, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out))
+    return 0
+
+
+def main_ours(a):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        vis = os.environ.get("CUDA_VISIBLE_DEVICES")
+        devs = vis.split(",") if vis else [str(i) for i in range(64)]
+        os.environ["CUDA_VISIBLE_DEVICES"] = devs[local]
+    import numpy as np
+    import torch
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(0)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+
+    from ocfd_b200 import abi, solver
+    L = solver.lib()
+    import ctypes as C
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(x):
+        if dist is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    c, name = make_case(a.workload)
+    g = solver.Solver(c)
+    g.init_state()
+    dt = c.dt
+    tt = 0.0
+    chk = solver._chk
+    chk(L.ocfd_gpu_run(dt, tt, a.warmup, 0, 1))
+    tt += a.warmup * dt
+
+    # ---- device-resident throughput ----
+    barrier()
+    l0 = L.ocfd_gpu_launch_count()
+    with Clocks(0) as clk:
+        chk(L.ocfd_gpu_event_record(0))
+        chk(L.ocfd_gpu_run(dt, tt, a.steps, 0, 1))
+        chk(L.ocfd_gpu_event_record(1))
+        ms = C.c_double()
+        chk(L.ocfd_gpu_event_elapsed(0, 1, C.byref(ms)))
+    tt += a.steps * dt
+    launches = L.ocfd_gpu_launch_count() - l0
+    barrier()
+    el_ms = max_over_ranks(ms.value)
+    value = world * c.ncell * a.steps / (el_ms * 1e-3) / 1e6
+
+    # ---- roofline: per-kernel-class event timing of 2 plain-launch steps ----
+    solver.Solver.profile(True)
+    for s in range(2):
+        g.tt = tt
+        g.step(dt)
+        tt += dt
+    prof = solver.Solver.profile_read()
+    solver.Solver.profile(False)
+    step_ms = sum(v[0] for v in prof.values()) / 2.0
+    dom = max((k for k in prof if k in ALG_BYTES_PER_CELL), key=lambda k: prof[k][0])
+    dom_ms = prof[dom][0] / max(prof[dom][1], 1)
+    hbm, hbm_kind = peaks()
+    alg = ALG_BYTES_PER_CELL[dom] * c.ncell
+    achieved = alg / (dom_ms * 1e-3) / 1e9
+    traffic = None
+    tfile = os.path.join(ROOT, "profiles", "traffic_per_cell.json")
+    if os.path.exists(tfile):
+        with open(tfile) as fh:
+            tr = json.load(fh)
+        if dom in tr:
+            traffic = tr[dom] * c.ncell
+    fp64 = solver.fp64_peak_gflops()
+    roof = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm, "unit": "GB/s",
+            "frac": achieved / hbm, "traffic": traffic, "peak_kind": hbm_kind,
+            "alg_bytes_per_launch": alg, "avg_launch_ms": dom_ms,
+            "share_of_step": prof[dom][0] / 2.0 / step_ms if step_ms > 0 else None,
+            "fp64_fma_peak_gflops_measured": fp64,
+            "kernel_shares": {k: round(v[0] / 2.0 / step_ms, 4) for k, v in prof.items() if v[1] > 0}}
+
+    # ---- e2e through the C ABI with host buffers ----
+    e2e = None
+    if not a.no_e2e:
+        nx, ny, nz = c.shape
+        hs = c.halo_shape()
+        H = hs[0] * hs[1] * hs[2]
+        N = c.ncell
+        ns = c.params.n_spec
+        nbytes_f, nbytes_di, nbytes_pr = 8 * 5 * N, 8 * ns * H, 8 * 7 * H
+        bufs = []
+
+        def pinned(nb, shape):
+            p = C.c_void_p()
+            chk(L.ocfd_gpu_pinned_alloc(nb, C.byref(p)))
+            bufs.append(p)
+            arr = np.ctypeslib.as_array(C.cast(p, C.POINTER(C.c_double)), shape=shape)
+            return arr
+
+        hf = pinned(nbytes_f, (5, nz, ny, nx))
+        hdi = pinned(nbytes_di, (ns,) + hs)
+        hpr = pinned(nbytes_pr, (7,) + hs)
+        chk(L.ocfd_gpu_download_state(abi.dptr(hf), abi.dptr(hdi), abi.dptr(hpr)))
+        barrier()
+        chk(L.ocfd_gpu_event_record(2))
+        for s in range(a.e2e_steps):
+            chk(L.ocfd_gpu_upload_state(abi.dptr(hf), abi.dptr(hdi), abi.dptr(hpr)))
+            chk(L.ocfd_gpu_run(dt, tt, 1, 0, 1))
+            tt += dt
+            chk(L.ocfd_gpu_download_state(abi.dptr(hf), abi.dptr(hdi), None))
+        chk(L.ocfd_gpu_event_record(3))
+        ms2 = C.c_double()
+        chk(L.ocfd_gpu_event_elapsed(2, 3, C.byref(ms2)))
+        e2e_ms = max_over_ranks(ms2.value)
+        e2e = {"value": world * N * a.e2e_steps / (e2e_ms * 1e-3) / 1e6, "unit": UNIT,
+               "h2d_bytes_per_step": nbytes_f + nbytes_di + nbytes_pr, "d2h_bytes_per_step": nbytes_f + nbytes_di,
+               "steps": a.e2e_steps}
+        for p in bufs:
+            L.ocfd_gpu_pinned_free(p)
+    g.close()
+
+    # ---- CPU baseline (rank 0, N = 1): the oracle on a bounded sample ----
+    cpu = None
+    if rank == 0 and world == 1 and not a.no_cpu:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import pyoracle
+        cores = pyoracle.lib().ocfd_cpu_set_threads(os.cpu_count() or 1)
+        if a.workload == "flatplate":
+            cs, _ = make_case("flatplate", nz=16)
+            sample = "one time step of a 1024x160x16 slab of the workload (z periodic), after one warm-up step"
+        else:
+            cs, _ = make_case("isotropic")
+            sample = "one time step of the 64^3 workload after one warm-up step"
+        o = pyoracle.OracleSolver(cs)
+        o.init_state()
+        o.step(cs.dt, 0.0)
+        t0 = time.perf_counter()
+        o.step(cs.dt, cs.dt)
+        el = time.perf_counter() - t0
+        o.close()
+        cpu = {"value": cs.ncell / el / 1e6, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample}
+
+    if rank == 0:
+        out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps,
+               "warmup": a.warmup, "ms_per_step": el_ms / a.steps, "higher_is_better": True, "scaling": "weak",
+               "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
+               "config": {"workload": name, "cells_per_gpu": c.ncell, "dt": dt, "chemistry": "off (non-reacting air)",
+                          "parallelism": "replicas x%d (no data-path collective)" % world,
+                          "l2": "state %.1f GB per GPU >> 126 MB L2; no flush" % (L.ocfd_gpu_launch_count() and 0 or
+                                                                                   (8 * (20 * c.ncell) / 1e9))},
+               "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches),
+               "clocks": clk.summary()}
+        print(json.dumps(out))
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    a = parse()
+    sys.exit(main_reference(a) if a.impl == "reference" else main_ours(a))

@@ -1,0 +1,241 @@
+/*
+ * ocfd_gpu.h -- C ABI of the B200 (sm_100a) implementation of the OpenCFD-Comb
+ * per-step hot path: flux-split WENO5/WENO7/OMP6/UD7L/HYBRID inviscid flux,
+ * CD6/CD8 viscous + heat flux, SSP-RK3 update, species transport and the
+ * finite-rate chemistry integrators.
+ *
+ * The Fortran driver of the reference keeps parsing its control files and
+ * keeps its output formats; it replaces the two hot call sites of its time
+ * loop with the entry points below (bind(C) interface in INTEGRATION.md):
+ *
+ *   code/flow-solver/OCFD_NS_Solver.f90:28,37  call flow_time_advance(dt1)
+ *        -> ocfd_gpu_flow_advance(dt1, tt)
+ *   code/flow-solver/OCFD_NS_Solver.f90:30-35  Chemical_time_advance x nsub + comput_T_P
+ *        -> ocfd_gpu_chem_advance(dt2, nsub)
+ *
+ * Array conventions (all arrays are Fortran column-major, contiguous):
+ *   "halo" arrays    : (1-LAP:nx+LAP, 1-LAP:ny+LAP, 1-LAP:nz+LAP)    H doubles
+ *   "interior" arrays: (nx, ny, nz)                                   N doubles
+ *   f                : f(nx,ny,nz,5)            (code/head/MODULE_flow.f90:11)
+ *   di               : di(halo, N_SPEC)         (code/head/MODULE_flow.f90:12)
+ *   prims            : d,u,v,w,T,p,Et stacked, 7 halo arrays
+ * All calls return 0 on success or a negative OCFD_ERR_* code; the text of
+ * the last error is in ocfd_gpu_last_error().  The library owns all device
+ * memory; no host pointer is retained after a call returns.  One host thread,
+ * one stream, not re-entrant (the reference's single MPI rank).
+ */
+#ifndef OCFD_GPU_H
+#define OCFD_GPU_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define OCFD_MAX_SPEC 16
+#define OCFD_MAX_REAC 64
+#define OCFD_NTCT_MAX 10  /* code/Chemical/CHEM_modules.f90:25 */
+
+/* error codes */
+#define OCFD_OK 0
+#define OCFD_ERR_PARAM (-1)       /* bad or unsupported parameter (reference: stop in OCFD_readpara.f90) */
+#define OCFD_ERR_CUDA (-2)        /* CUDA runtime error / no device / kernel image missing */
+#define OCFD_ERR_NAN (-3)         /* NaN in the conserved state (reference: OCFD_debug.f90:20-26) */
+#define OCFD_ERR_NEGATIVE_ET (-4) /* more than 10 cells with Et<=0 (OCFD_handle_NegativeT.f90:16-19) */
+#define OCFD_ERR_STATE (-5)       /* call order violated (e.g. advance before init) */
+#define OCFD_ERR_TIMEOUT (-6)     /* a bounded device wait ran out (persistent chemistry queue) */
+#define OCFD_ERR_UNSUPPORTED (-7) /* reference feature outside the built scope */
+
+/* scheme / option ids: code/head/MODULE_parameter.f90:13-30 */
+#define OCFD_SCHEME_WENO5 1
+#define OCFD_SCHEME_WENO7 2
+#define OCFD_SCHEME_OMP6 3
+#define OCFD_SCHEME_UD7L 4
+#define OCFD_SCHEME_CD6 5
+#define OCFD_SCHEME_CD8 6
+#define OCFD_SCHEME_HYBRID 10
+#define OCFD_SPLIT_SW 1
+#define OCFD_SPLIT_LLF 2
+#define OCFD_BC_NONE 0
+#define OCFD_BC_BOUNDARYLAYER 2
+#define OCFD_BC_JET 4
+#define OCFD_CHEM_EULER 1
+#define OCFD_CHEM_RK2 2
+#define OCFD_CHEM_RK3 3
+#define OCFD_CHEM_IMPLICIT (-1)
+
+/* Flat mirror of the reference's Para / Scheme records (code/head/MODULE_parameter.f90:49-96)
+ * as they come out of read_control_parameter (code/mpi-io/OCFD_readpara.f90:26-284).
+ * Derived quantities of set_parameters (OCFD_readpara.f90:347-431: hx/hy/hz, Bound_index,
+ * [Ka,Kb], UD7L coefficients) are computed inside the library from these fields. */
+typedef struct ocfd_params {
+  int nx, ny, nz;          /* = nx_global.. (single rank) */
+  int lap;                 /* halo width, must be 4 */
+  int n_spec;
+  int iperiodic[3];
+  double periodic_span[3][3]; /* [dir][component]: Periodic_ISpan, _JSpan, _KSpan */
+  int scheme_invis, scheme_vis;
+  int scheme_boundary[6];  /* i-, i+, j-, j+, k-, k+ : 0 WENO5 deleted-stencil, 1 WENO5 full, -1 none */
+  int ghost_cell[6];       /* 0 none, 1/2 second-order extrapolation (OCFD_GhostCell.f90:166-364) */
+  int if_scheme_character; /* must be 0 (characteristic flux not built) */
+  int if_viscous;
+  int flux_splitting;      /* OCFD_SPLIT_SW / OCFD_SPLIT_LLF */
+  int if_mass_force;
+  double mass_force[3];
+  int ibc;                 /* OCFD_BC_NONE / OCFD_BC_BOUNDARYLAYER */
+  double bc_para[100];
+  double hybrid_para[100];
+  double ud7l_diss;
+  double aoa;              /* radians (rparameters(20) = AoA*PI/180) */
+  int if_realgas;          /* 0 perfect gas (Cv = 2.5 R), 1 NASA-fit thermo */
+  int chem_timeadv;        /* 1, 2, 3, -1 */
+  int wall_catalysis;      /* must be 0 */
+  int istep_show;          /* unused by the library; kept for the mirror */
+} ocfd_params;
+
+/* Species thermodynamics: read_Spec (code/Chemical/CHEM_thermdyn.f90:16-51). Ri and the
+ * range-continuity offsets Ect are derived inside the library exactly as read_Spec does. */
+typedef struct ocfd_thermo {
+  int n_spec;
+  int n_tct;                         /* number of fit ranges */
+  double tct[OCFD_NTCT_MAX];         /* range boundaries Tct(1..n_tct-1) */
+  double tct_max;
+  double mi[OCFD_MAX_SPEC];          /* molar mass kg/mol */
+  int spec_flag[OCFD_MAX_SPEC];      /* 1 monoatomic, 2 diatomic */
+  double coef[OCFD_MAX_SPEC][OCFD_NTCT_MAX][7]; /* A,B,C,D,E,F,G per range */
+} ocfd_thermo;
+
+/* Reaction mechanism: read_Reac (code/Chemical/CHEM_reactions.f90:15-69). */
+typedef struct ocfd_kinetics {
+  int n_spec, n_reac;
+  int rereac;                         /* 0 Gibbs Kc, 1 Arrhenius reverse, 2 Park fit */
+  int af_type[OCFD_MAX_REAC];         /* 0 normal, 1 Troe fall-off, 2 dual Arrhenius */
+  int tr_reac[OCFD_MAX_REAC];         /* three-body flag */
+  double fc_troe[OCFD_MAX_REAC];
+  double af[OCFD_MAX_REAC][2], bf[OCFD_MAX_REAC][2], ef[OCFD_MAX_REAC][2];
+  double ar[OCFD_MAX_REAC], br[OCFD_MAX_REAC], er[OCFD_MAX_REAC];
+  double park[OCFD_MAX_REAC][5];
+  int vf[OCFD_MAX_REAC][OCFD_MAX_SPEC], vr[OCFD_MAX_REAC][OCFD_MAX_SPEC];
+  double treff[OCFD_MAX_REAC][OCFD_MAX_SPEC];
+} ocfd_kinetics;
+
+/* Transport model: Trans record (code/Chemical/TRANSPORT_modules.f90:16-22). */
+typedef struct ocfd_transport {
+  int flag_vis, flag_cond, flag_diff;  /* 0 Sutherland/Pr/Sc, 1 Wilke fits */
+  double amu0, pr, sc, amk0;
+  double mu_an[OCFD_MAX_SPEC][5];
+  double k_an[OCFD_MAX_SPEC][5];
+  double d_an[OCFD_MAX_SPEC][OCFD_MAX_SPEC][4];
+} ocfd_transport;
+
+/* Boundary-layer boundary data (code/boundary-condition/OCFD_BC_Boundarylayers.f90:4-17).
+ * Inlet / upper arrays are already re-scaled as init_bcdata_boundary does. The random phases
+ * of the wall disturbance (random_number at :523,595) are supplied by the caller. */
+typedef struct ocfd_bcdata {
+  const double* inlet;        /* BcData_inlet 0: (5+Ns); 1: ny*(5+Ns) as [comp][j]; 2: (5+Ns)*ny*nz as [comp][k][j] */
+  const double* upper;        /* BcData_upper 0: (5+Ns); 1: nx*(5+Ns) as [comp][i]; 2: (5+Ns)*nx*nz */
+  const double* wall_pertb;   /* nx*nz, BC%wall_pertb(i,k), i fastest; NULL = zero */
+  int n_tm;                   /* bc_dis_mt temporal modes */
+  const double* tm;           /* TM(1..n_tm) normalised amplitudes */
+  const double* fait;         /* fait(1..n_tm) random phases in [0,1) */
+} ocfd_bcdata;
+
+/* ---- library lifecycle ---- */
+
+/* Replaces the device-relevant part of NS_solver's setup (OCFD_NS_Solver.f90:12-18, init_mesh
+ * OCFD_flow-solver/OCFD_mesh.f90:1-57). coords = Axx,Ayy,Azz (3 halo arrays) as read_mesh* fills
+ * them; the library applies the periodic exchange, the periodic coordinate shift, the Jacobian
+ * (comput_Jacobian3d, OCFD_mesh.f90:60-107) and Akx1..Asz1 on the device. metrics (optional,
+ * NULL = compute) = Akx,Aky,Akz,Aix,Aiy,Aiz,Asx,Asy,Asz,Ajac (10 halo arrays) as for
+ * Iflag_Gridtype=31. kin may be NULL when chemistry is off; bc may be NULL for BC_NONE. */
+int ocfd_gpu_init(const ocfd_params* p, const ocfd_thermo* th, const ocfd_kinetics* kin,
+                  const ocfd_transport* tr, const ocfd_bcdata* bc,
+                  const double* coords, const double* metrics);
+
+/* Builds the solver state from primitive fields as the reference's start-up does: the tail of
+ * init3d (Rescaling_di, conserved f from d,u,v,w,T via comput_E; OCFD_init.f90:8-25) followed by
+ * comput_flow_variables and OCFD_bc (OCFD_NS_Solver.f90:17-18). prim5 = d,u,v,w,T (5 interior
+ * arrays: the content of the restart file opencfd-comb.dat, OCFD_IO.f90:5-36), di = Ns interior
+ * arrays. Halo points take allocate_flow_data's initial values (OCFD_allocate_data.f90:53-67). */
+int ocfd_gpu_init_state(const double* prim5, const double* di, double tt);
+
+/* Uploads the Fortran module state: f (N*5), di (H*Ns), prims (7*H: d,u,v,w,T,p,Et). */
+int ocfd_gpu_upload_state(const double* f, const double* di, const double* prims);
+
+/* flow_time_advance(dt1) (code/flow-solver/OCFD_Time_Adv.f90:7-92): 3 RK stages; tt is the
+ * solver time at the call (used by the wall disturbance, OCFD_BC_Boundarylayers.f90:147). */
+int ocfd_gpu_flow_advance(double dt1, double tt);
+
+/* nsub x Chemical_time_advance(dt2) (OCFD_Time_Adv.f90:169-196) followed by comput_T_P
+ * (Comput_flow_variables.f90:30-46), as OCFD_NS_Solver.f90:30-35. */
+int ocfd_gpu_chem_advance(double dt2, int nsub);
+
+/* One full reference time step (OCFD_NS_Solver.f90:28-37): flow(dt/2), chemistry (if
+ * if_reaction), flow(dt/2). Captured as a CUDA graph after the first call with a given dt. */
+int ocfd_gpu_step(double dt, double tt, int if_reaction, int nsub);
+
+/* nsteps consecutive ocfd_gpu_step calls (solver time tt0, tt0+dt, ...) replayed back to back on
+ * the device with one status check at the end; the reference's time loop without I/O steps. */
+int ocfd_gpu_run(double dt, double tt0, int nsteps, int if_reaction, int nsub);
+
+/* Downloads the state; any pointer may be NULL to skip that part. */
+int ocfd_gpu_download_state(double* f, double* di, double* prims);
+
+/* show_flow_msg reductions (OCFD_Time_Adv.f90:210-223): mean total and kinetic energy. */
+int ocfd_gpu_diag(double* e_mean, double* k_mean);
+
+/* Downloads the hybrid-scheme sensor Rhybrid (halo array) for decision-map comparisons. */
+int ocfd_gpu_download_rhybrid(double* rhybrid);
+
+/* Downloads the ten Jacobian arrays (Akx..Asz, Ajac; 10 halo arrays). */
+int ocfd_gpu_download_metrics(double* metrics);
+
+/* Batched 0-D chemistry: chemical_timeAdv (CHEM_reactions.f90:374-390) applied nsub[r]
+ * times with step dt[r]/nsub[r] to n independent reactors, di (n*Ns, reactor-major) and E
+ * (n) updated in place. nsub == NULL means 1 sub-step each. Runs as one persistent
+ * work-queue kernel on the device; host buffers in and out. */
+int ocfd_gpu_chem_batch(int n, double* di, double* e, const double* dt, const int* nsub);
+
+/* Same as ocfd_gpu_chem_batch with device pointers (no host copies). */
+int ocfd_gpu_chem_batch_device(int n, double* d_di, double* d_e, const double* d_dt,
+                               const int* d_nsub);
+
+/* Sets up the chemistry tables alone (no grid) for ocfd_gpu_chem_batch: read_Spec + read_Reac
+ * content, IF_RealGas and CHEM_TimeAdv. */
+int ocfd_gpu_chem_setup(const ocfd_thermo* th, const ocfd_kinetics* kin, int realgas, int timeadv);
+
+/* Per-kernel-class CUDA-event timing of the non-graph launches (enable resets the totals). */
+int ocfd_gpu_profile(int enable);
+int ocfd_gpu_profile_read(int cls, double* ms, long long* count);
+const char* ocfd_gpu_profile_name(int cls);
+int ocfd_gpu_profile_nclass(void);
+/* The library's CUDA stream (cudaStream_t), for callers that time or order work around it. */
+void* ocfd_gpu_stream(void);
+/* CUDA events on the library stream (slots 0..15) and the time between two of them. */
+int ocfd_gpu_event_record(int slot);
+int ocfd_gpu_event_elapsed(int a, int b, double* ms);
+/* Page-locked host buffers for fast host<->device copies of the state. */
+int ocfd_gpu_pinned_alloc(size_t bytes, void** ptr);
+int ocfd_gpu_pinned_free(void* ptr);
+/* Kernels in one captured Strang step. */
+int ocfd_gpu_step_launches(void);
+/* Kernels launched by the library since init (graph replays count their kernels). */
+long long ocfd_gpu_launch_count(void);
+/* 1 when the grid is a tensor product and metrics are kept as three 1-D arrays. */
+int ocfd_gpu_is_separable(void);
+
+/* Statistics of the last advance: number of Et<=0 repairs, Newton non-converged cells. */
+int ocfd_gpu_stats(long long* neg_et, long long* newton_fail);
+
+const char* ocfd_gpu_last_error(void);
+int ocfd_gpu_finalize(void);
+
+/* Measures the device's FP64 FMA throughput (GFLOP/s) with a register-resident loop
+ * (roofline denominator for the FP64-bound kernels). */
+double ocfd_gpu_fp64_peak_gflops(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

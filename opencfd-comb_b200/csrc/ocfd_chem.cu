@@ -1,0 +1,37 @@
+// Chemistry kernels (k_chem_cells, k_chem_batch) in their own translation unit.
+#include <stdexcept>
+#include "ocfd_chem.cuh"
+#include "ocfd_launch.h"
+
+namespace ocfd {
+
+#define NS_CASES(...)                                          \
+  switch (ns) {                                                \
+    case 1: { constexpr int NSV = 1; __VA_ARGS__; } break;     \
+    case 2: { constexpr int NSV = 2; __VA_ARGS__; } break;     \
+    case 3: { constexpr int NSV = 3; __VA_ARGS__; } break;     \
+    case 4: { constexpr int NSV = 4; __VA_ARGS__; } break;     \
+    case 5: { constexpr int NSV = 5; __VA_ARGS__; } break;     \
+    case 6: { constexpr int NSV = 6; __VA_ARGS__; } break;     \
+    case 7: { constexpr int NSV = 7; __VA_ARGS__; } break;     \
+    case 8: { constexpr int NSV = 8; __VA_ARGS__; } break;     \
+    case 9: { constexpr int NSV = 9; __VA_ARGS__; } break;     \
+    default: throw std::runtime_error("N_SPEC must be 1..9");  \
+  }
+
+void launch_chem_cells(int ns, long long ncell, double* f, double* Et, double* T, double* p, double* di, double dt2,
+                       int nsub, int* nfail, cudaStream_t st) {
+  unsigned nb = (unsigned)((ncell + 127) / 128);
+  NS_CASES(k_chem_cells<NSV><<<nb, 128, 0, st>>>(f, Et, T, p, di, dt2, nsub, nfail));
+}
+
+void launch_chem_batch(int ns, int sms, int n, double* di, double* e, const double* dt, const int* nsub,
+                       const int* perm, int* counter, int* nfail, cudaStream_t st) {
+  NS_CASES({
+    int per = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_chem_batch<NSV>, 128, 0);
+    if (per < 1) per = 1;
+    k_chem_batch<NSV><<<sms * per, 128, 0, st>>>(n, di, e, dt, nsub, perm, counter, nfail);
+  });
+}
+}  // namespace ocfd

@@ -1,0 +1,608 @@
+// Device-side constants and per-point math of the OpenCFD-Comb hot path (sm_100a).
+//
+// Every routine keeps the reference's evaluation order (left-to-right sums, gfortran's
+// integer-power chains, single-precision literals where the Fortran has them) so that, with
+// --fmad=false, the kernels reproduce the CPU restatement bit for bit wherever no
+// transcendental function (exp/log/pow/sin) is involved.
+#pragma once
+#include <cstdint>
+#include "../../include/ocfd_gpu.h"
+
+#define OCFD_L 4  // halo width LAP
+
+namespace ocfd {
+
+// ---------------------------------------------------------------- constant memory
+struct DevConst {
+  int nx, ny, nz, ns;
+  int HX, HY, HZ;
+  long long H, N;
+  int iper[3];
+  int bound[3][2];  // Bound_index(side, dir) of set_parameters (OCFD_readpara.f90:360-369)
+  int sb[6];        // Scheme_boundary
+  int ghost[6];
+  int scheme, split, Ka1, Kb1, Ka2, Kb2;
+  double UD7L[8];
+  double theta1, theta2;
+  double h[3], h1[3];      // hx,hy,hz and 1/h
+  double cd6[3][3];        // 1/(60h), -3/(20h), 3/(4h)
+  double cd8[3][4];        // 0.8/h, -0.2/h, 3.8095e-2/h, -3.5714e-3/h
+  double h2x[3], h12x[3];  // 2h, 12h (closures)
+  int cd8_on;
+  int if_viscous, if_mass_force;
+  double mass_force[3];
+  int realgas;
+  // thermo (read_Spec)
+  int n_tct;
+  double tct[OCFD_NTCT_MAX], tct_max;
+  double Mi[OCFD_MAX_SPEC], Ri[OCFD_MAX_SPEC];
+  double cf[OCFD_MAX_SPEC][OCFD_NTCT_MAX][8];  // A,B,C,D,E,F,G,Ect
+  // transport
+  int flag_vis, flag_cond, flag_diff;
+  double amu0, pr, sc;
+  double mu_an[OCFD_MAX_SPEC][4], k_an[OCFD_MAX_SPEC][4];
+  double d_an[OCFD_MAX_SPEC][OCFD_MAX_SPEC][4];
+  // kinetics
+  int nreac, rereac, timeadv;
+  int af_type[OCFD_MAX_REAC], tr_reac[OCFD_MAX_REAC];
+  double fc_troe[OCFD_MAX_REAC];
+  double af[OCFD_MAX_REAC][2], bf[OCFD_MAX_REAC][2], ef[OCFD_MAX_REAC][2];
+  double ar[OCFD_MAX_REAC], br[OCFD_MAX_REAC], er[OCFD_MAX_REAC];
+  double park[OCFD_MAX_REAC][5];
+  signed char vf[OCFD_MAX_REAC][OCFD_MAX_SPEC], vr[OCFD_MAX_REAC][OCFD_MAX_SPEC];
+  int sgm[OCFD_MAX_REAC];
+  double treff[OCFD_MAX_REAC][OCFD_MAX_SPEC];
+};
+
+// defined once (ocfd_gpu.cu); the sweep / chemistry translation units share it through
+// relocatable device code
+#ifdef OCFD_DEFINE_CONST
+__constant__ DevConst cC;
+#else
+extern __constant__ DevConst cC;
+#endif
+
+// geometry: either 19 full metric arrays or three 1-D derivative arrays (tensor-product grids)
+struct Geo {
+  const double* m[19];   // Akx,Aky,Akz,Aix,Aiy,Aiz,Asx,Asy,Asz,Ajac,Akx1..Asz1 (halo layout)
+  const double* d1[3];   // dx/dxi(i), dy/deta(j), dz/dzeta(k), halo-inclusive, index s+L-1
+};
+enum { G_AKX = 0, G_AKY, G_AKZ, G_AIX, G_AIY, G_AIZ, G_ASX, G_ASY, G_ASZ, G_AJAC, G_AKX1 };
+
+__device__ __forceinline__ int hidx(int i, int j, int k) {
+  return (i + OCFD_L - 1) + cC.HX * ((j + OCFD_L - 1) + cC.HY * (k + OCFD_L - 1));
+}
+__device__ __forceinline__ int nidx(int i, int j, int k) { return (i - 1) + cC.nx * ((j - 1) + cC.ny * (k - 1)); }
+__device__ __forceinline__ int hstride(int dir) { return dir == 0 ? 1 : (dir == 1 ? cC.HX : cC.HX * cC.HY); }
+
+// gfortran -O3 integer-power chains (GCC powi table): x**3 = x**2*x, x**4 = (x**2)**2, x**5 = x**2*x**3
+__device__ __forceinline__ double q2(double x) { return x * x; }
+__device__ __forceinline__ double q3(double x) { double a = x * x; return a * x; }
+__device__ __forceinline__ double q4(double x) { double a = x * x; return a * a; }
+__device__ __forceinline__ double q5(double x) { double a = x * x; double b = a * x; return a * b; }
+// libgcc __powidf2: x**n for a run-time integer n (square-and-multiply, then reciprocal)
+__device__ __forceinline__ double powi_rt(double x, int m) {
+  unsigned n = m < 0 ? -(unsigned)m : (unsigned)m;
+  double y = (n & 1u) ? x : 1.0;
+  while (n >>= 1) {
+    x = x * x;
+    if (n & 1u) y = y * x;
+  }
+  return m < 0 ? 1.0 / y : y;
+}
+__device__ __forceinline__ double fsgn(double x) { return signbit(x) ? -1.0 : 1.0; }
+
+// ---------------------------------------------------------------- metrics
+// Separable (1-D grid) metrics: the Jacobian formula of comput_Jacobian3d with all cross
+// derivatives exactly zero reduces to these products (OCFD_mesh.f90:88-98).
+template <bool SEP>
+__device__ __forceinline__ void metric_dir(const Geo& g, int dir, int i, int j, int k, int q, double& A1, double& A2,
+                                           double& A3) {
+  if (SEP) {
+    double xi = g.d1[0][i + OCFD_L - 1], yj = g.d1[1][j + OCFD_L - 1], zk = g.d1[2][k + OCFD_L - 1];
+    double jac = 1.0 / (xi * yj * zk);
+    double a = dir == 0 ? jac * (yj * zk) : (dir == 1 ? jac * (zk * xi) : jac * (xi * yj));
+    double d = a / jac;
+    A1 = dir == 0 ? d : 0.0;
+    A2 = dir == 1 ? d : 0.0;
+    A3 = dir == 2 ? d : 0.0;
+  } else {
+    A1 = __ldg(g.m[G_AKX1 + 3 * dir] + q);
+    A2 = __ldg(g.m[G_AKX1 + 3 * dir + 1] + q);
+    A3 = __ldg(g.m[G_AKX1 + 3 * dir + 2] + q);
+  }
+}
+template <bool SEP>
+__device__ __forceinline__ double metric_jac(const Geo& g, int i, int j, int k, int q) {
+  if (SEP) {
+    double xi = g.d1[0][i + OCFD_L - 1], yj = g.d1[1][j + OCFD_L - 1], zk = g.d1[2][k + OCFD_L - 1];
+    return 1.0 / (xi * yj * zk);
+  }
+  return __ldg(g.m[G_AJAC] + q);
+}
+// the nine Akx..Asz and the nine Akx1..Asz1 at one point
+template <bool SEP>
+__device__ __forceinline__ void metric_all(const Geo& g, int i, int j, int k, int q, double* a, double* a1) {
+  if (SEP) {
+    double xi = g.d1[0][i + OCFD_L - 1], yj = g.d1[1][j + OCFD_L - 1], zk = g.d1[2][k + OCFD_L - 1];
+    double jac = 1.0 / (xi * yj * zk);
+    double akx = jac * (yj * zk), aiy = jac * (zk * xi), asz = jac * (xi * yj);
+#pragma unroll
+    for (int m = 0; m < 9; m++) { a[m] = 0.0; a1[m] = 0.0; }
+    a[0] = akx; a[4] = aiy; a[8] = asz;
+    a1[0] = akx / jac; a1[4] = aiy / jac; a1[8] = asz / jac;
+  } else {
+#pragma unroll
+    for (int m = 0; m < 9; m++) {
+      a[m] = __ldg(g.m[m] + q);
+      a1[m] = __ldg(g.m[G_AKX1 + m] + q);
+    }
+  }
+}
+
+// ---------------------------------------------------------------- thermodynamics (CHEM_thermdyn.f90)
+__device__ __forceinline__ int trange(double T) {
+  int jc = 0;
+  for (int j = 0; j < cC.n_tct - 1; j++)
+    if (T > cC.tct[j]) jc = j + 1;
+  return jc;
+}
+template <int NS>
+__device__ __forceinline__ double dev_E(const double* di, double T) {
+  if (cC.realgas == 0) {
+    double e = 0.0;
+#pragma unroll
+    for (int k = 0; k < NS; k++) e = e + 2.5 * cC.Ri[k] * di[k] * T;
+    return e;
+  }
+  int jc = trange(T);
+  double A1 = 0, B1 = 0, C1 = 0, D1 = 0, E1 = 0, Ec = 0;
+#pragma unroll
+  for (int k = 0; k < NS; k++) {
+    const double* c = cC.cf[k][jc];
+    double R1 = cC.Ri[k];
+    A1 = A1 + (c[0] - 1.0) * R1 * di[k];
+    B1 = B1 + c[1] * R1 * di[k];
+    C1 = C1 + c[2] * R1 * di[k];
+    D1 = D1 + c[3] * R1 * di[k];
+    E1 = E1 + c[4] * R1 * di[k];
+    Ec = Ec + c[7] * R1 * di[k];
+  }
+  if (T <= cC.tct_max) return A1 * T + B1 * q2(T) / 2.0 + C1 * q3(T) / 3.0 + D1 * q4(T) / 4.0 + E1 * q5(T) / 5.0 + Ec;
+  double tm = cC.tct_max;
+  double cv2 = A1 + B1 * tm + C1 * q2(tm) + D1 * q3(tm) + E1 * q4(tm);
+  return A1 * tm + B1 * q2(tm) / 2.0 + C1 * q3(tm) / 3.0 + D1 * q4(tm) / 4.0 + E1 * q5(tm) / 5.0 + Ec + cv2 * (T - tm);
+}
+template <int NS>
+__device__ __forceinline__ double dev_Cp(double d, const double* di, double T) {
+  if (cC.realgas == 0) {
+    double cp = 0.0;
+#pragma unroll
+    for (int k = 0; k < NS; k++) cp = cp + 3.5 * cC.Ri[k] * di[k];
+    return cp / d;
+  }
+  int jc = trange(T);
+  double A1 = 0, B1 = 0, C1 = 0, D1 = 0, E1 = 0;
+#pragma unroll
+  for (int k = 0; k < NS; k++) {
+    const double* c = cC.cf[k][jc];
+    double R1 = cC.Ri[k];
+    A1 = A1 + c[0] * R1 * di[k];
+    B1 = B1 + c[1] * R1 * di[k];
+    C1 = C1 + c[2] * R1 * di[k];
+    D1 = D1 + c[3] * R1 * di[k];
+    E1 = E1 + c[4] * R1 * di[k];
+  }
+  double t = T <= cC.tct_max ? T : cC.tct_max;
+  return (A1 + B1 * t + C1 * q2(t) + D1 * q3(t) + E1 * q4(t)) / d;
+}
+// T from internal energy; Newton (tol 1e-3 K, at most 31 iterations) for the fitted gas
+template <int NS>
+__device__ __forceinline__ double dev_T(const double* di, double Ein, int* nfail) {
+  if (cC.realgas == 0) {
+    double rcv = 0.0;
+#pragma unroll
+    for (int k = 0; k < NS; k++) rcv = rcv + 2.5 * cC.Ri[k] * di[k];
+    return Ein / rcv;
+  }
+  double A1[OCFD_NTCT_MAX], B1[OCFD_NTCT_MAX], C1[OCFD_NTCT_MAX], D1[OCFD_NTCT_MAX], E1[OCFD_NTCT_MAX],
+      Ec[OCFD_NTCT_MAX];
+  const int nt = cC.n_tct;
+  for (int j = 0; j < nt; j++) {
+    double a = 0, b = 0, c = 0, d = 0, e = 0, g = 0;
+#pragma unroll
+    for (int k = 0; k < NS; k++) {
+      const double* cf = cC.cf[k][j];
+      double R1 = cC.Ri[k];
+      a = a + (cf[0] - 1.0) * R1 * di[k];
+      b = b + cf[1] * R1 * di[k];
+      c = c + cf[2] * R1 * di[k];
+      d = d + cf[3] * R1 * di[k];
+      e = e + cf[4] * R1 * di[k];
+      g = g + cf[7] * R1 * di[k];
+    }
+    A1[j] = a; B1[j] = b; C1[j] = c; D1[j] = d; E1[j] = e; Ec[j] = g;
+  }
+  double T1 = Ein / A1[0], T2 = T1;
+  int ks = 0;
+  bool conv = false;
+  while (ks <= 30) {
+    int jc = trange(T1);
+    double Et1, Ex;
+    if (T1 <= cC.tct_max) {
+      Et1 = A1[jc] * T1 + B1[jc] * q2(T1) / 2.0 + C1[jc] * q3(T1) / 3.0 + D1[jc] * q4(T1) / 4.0 +
+            E1[jc] * q5(T1) / 5.0 + Ec[jc];
+      Ex = A1[jc] + B1[jc] * T1 + C1[jc] * q2(T1) + D1[jc] * q3(T1) + E1[jc] * q4(T1);
+    } else {
+      double tm = cC.tct_max;
+      Ex = A1[jc] + B1[jc] * tm + C1[jc] * q2(tm) + D1[jc] * q3(tm) + E1[jc] * q4(tm);
+      Et1 = A1[jc] * tm + B1[jc] * q2(tm) / 2.0 + C1[jc] * q3(tm) / 3.0 + D1[jc] * q4(tm) / 4.0 +
+            E1[jc] * q5(tm) / 5.0 + Ec[jc] + Ex * (T1 - tm);
+    }
+    T2 = T1 - (Et1 - Ein) / Ex;
+    ks = ks + 1;
+    double err = fabs(T2 - T1);
+    T1 = T2;
+    if (err < 1.0e-3) { conv = true; break; }
+  }
+  if (!conv && nfail) atomicAdd(nfail, 1);
+  return T2;
+}
+template <int NS>
+__device__ __forceinline__ double dev_P(const double* di, double T) {
+  double p = 0.0;
+#pragma unroll
+  for (int k = 0; k < NS; k++) p = p + cC.Ri[k] * di[k] * T;
+  return p;
+}
+template <int NS>
+__device__ __forceinline__ double dev_dens(const double* ai, double T, double p) {
+  double r1 = 0.0;
+#pragma unroll
+  for (int k = 0; k < NS; k++) r1 = r1 + cC.Ri[k] * ai[k];
+  return p / (T * r1);
+}
+__device__ __forceinline__ double dev_hi(int k, double T) {
+  if (cC.realgas == 0) return 3.5 * cC.Ri[k] * T;
+  int jc = trange(T);
+  const double* c = cC.cf[k][jc];
+  if (T <= cC.tct_max)
+    return (c[0] * T + c[1] * q2(T) / 2.0 + c[2] * q3(T) / 3.0 + c[3] * q4(T) / 4.0 + c[4] * q5(T) / 5.0 + c[7]) *
+           cC.Ri[k];
+  double tm = cC.tct_max;
+  double cpm = c[0] + c[1] * tm + c[2] * q2(tm) + c[3] * q3(tm) + c[4] * q4(tm);
+  return (c[0] * tm + c[1] * q2(tm) / 2.0 + c[2] * q3(tm) / 3.0 + c[3] * q4(tm) / 4.0 + c[4] * q5(tm) / 5.0 + c[7] +
+          cpm * (T - tm)) *
+         cC.Ri[k];
+}
+__device__ __forceinline__ double dev_gibbs(int k, double T, double logT) {
+  int jc = trange(T);
+  const double* c = cC.cf[k][jc];
+  if (T <= cC.tct_max)
+    return c[0] * (1.0 - logT) * T - c[1] * q2(T) / 2.0 - c[2] * q3(T) / 6.0 - c[3] * q4(T) / 12.0 -
+           c[4] * q5(T) / 20.0 + c[5] - c[6] * T;
+  double tm = cC.tct_max;
+  double cpm = c[0] + c[1] * tm + c[2] * q2(tm) + c[3] * q3(tm) + c[4] * q4(tm);
+  double hm = c[0] * tm + c[1] * q2(tm) / 2.0 + c[2] * q3(tm) / 3.0 + c[3] * q4(tm) / 4.0 + c[4] * q5(tm) / 5.0 + c[5];
+  double sm = c[0] * log(tm) + c[1] * tm + c[2] * q2(tm) / 2.0 + c[3] * q3(tm) / 3.0 + c[4] * q4(tm) / 4.0 + c[6];
+  return hm + cpm * (T - tm) - T * (sm + cpm * log(T / tm));
+}
+
+// ---------------------------------------------------------------- transport (TRANSPORT_modules.f90)
+template <int NS>
+__device__ __forceinline__ double dev_viscosity(double T, const double* Xi) {
+  if (cC.flag_vis == 0) {
+    const double TA = 288.15, TC = 110.4;
+    return cC.amu0 * sqrt(q3(T / TA)) * (TA + TC) / (TC + T);
+  }
+  double L = log(T);
+  double mui[NS];
+#pragma unroll
+  for (int m = 0; m < NS; m++)
+    mui[m] = exp(cC.mu_an[m][0] + cC.mu_an[m][1] * L + cC.mu_an[m][2] * q2(L) + cC.mu_an[m][3] * q3(L)) * 0.1;
+  double mu = 0.0;
+#pragma unroll
+  for (int k = 0; k < NS; k++) {
+    double pk0 = 0.0;
+#pragma unroll
+    for (int j = 0; j < NS; j++) {
+      double s = 1.0 + sqrt(mui[k] / mui[j] * sqrt(cC.Mi[j] / cC.Mi[k]));
+      double pkj = q2(s) / sqrt(8.0 * (1.0 + cC.Mi[k] / cC.Mi[j]));
+      pk0 = pk0 + Xi[j] * pkj;
+    }
+    mu = mu + Xi[k] * mui[k] / pk0;
+  }
+  return mu;
+}
+template <int NS>
+__device__ __forceinline__ double dev_conductivity(double amu, double cp, double T, const double* Xi) {
+  if (cC.flag_cond == 0) return amu * cp / cC.pr;
+  double L = log(T);
+  double a1 = 0.0, a2 = 0.0;
+#pragma unroll
+  for (int m = 0; m < NS; m++) {
+    double ki = exp(cC.k_an[m][0] + cC.k_an[m][1] * L + cC.k_an[m][2] * q2(L) + cC.k_an[m][3] * q3(L)) * 1.0e-5;
+    a1 = a1 + Xi[m] * ki;
+    a2 = a2 + Xi[m] / ki;
+  }
+  return 0.5 * (a1 + 1.0 / a2);
+}
+template <int NS>
+__device__ __forceinline__ void dev_diffusion(double* amd, double amu, double T, double d, double p, const double* Xi) {
+  if (cC.flag_diff == 0) {
+    double d0 = 0.0;
+#pragma unroll
+    for (int m = 0; m < NS; m++) d0 = d0 + Xi[m] * cC.Mi[m];
+#pragma unroll
+    for (int m = 0; m < NS; m++) amd[m] = amu * (1.0 - Xi[m] * cC.Mi[m] / d0) / ((1.0 - Xi[m]) * cC.sc * d + 1.0e-20);
+    return;
+  }
+  double L = log(T);
+#pragma unroll
+  for (int k = 0; k < NS; k++) {
+    double ds = 0.0;
+#pragma unroll
+    for (int j = 0; j < NS; j++) {
+      if (j == k) continue;
+      int a = k < j ? k : j, b = k < j ? j : k;  // D2(k,j) = D2(min,max) (symmetric fill of the reference)
+      double D2 = exp(cC.d_an[a][b][0] + cC.d_an[a][b][1] * L + cC.d_an[a][b][2] * q2(L) + cC.d_an[a][b][3] * q3(L)) *
+                  1.0e-4;
+      ds = ds + Xi[j] / D2;
+    }
+    amd[k] = (1.0 - Xi[k]) / (ds + 1.0e-20) * 1.013e5 / p;
+  }
+}
+
+// ---------------------------------------------------------------- reconstructions
+// single interface; v points at the stencil centre v(i) (OCFD_Schemes.f90 / OCFD_Schemes_1.f90).
+// VS is the element stride of v (1 when v is contiguous, the line count in shared memory otherwise).
+template <int VS>
+__device__ __forceinline__ double weno5P(const double* v) {
+  const double ep = 1.0e-6, C03 = 3.0 / 10.0, C13 = 3.0 / 5.0, C23 = 1.0 / 10.0;
+  const double vm2 = v[-2 * VS], vm1 = v[-VS], v0 = v[0], v1 = v[VS], v2 = v[2 * VS];
+  double S0 = 13.0 / 12.0 * q2(v0 - 2.0 * v1 + v2) + 1.0 / 4.0 * q2(3.0 * v0 - 4.0 * v1 + v2);
+  double S1 = 13.0 / 12.0 * q2(vm1 - 2.0 * v0 + v1) + 1.0 / 4.0 * q2(vm1 - v1);
+  double S2 = 13.0 / 12.0 * q2(vm2 - 2.0 * vm1 + v0) + 1.0 / 4.0 * q2(vm2 - 4.0 * vm1 + 3.0 * v0);
+  double a0 = C03 / q2(ep + S0);
+  double a1 = C13 / q2(ep + S1);
+  double a2 = C23 / q2(ep + S2);
+  double am = a0 + a1 + a2;
+  double q03 = 1.0 / 3.0 * v0 + 5.0 / 6.0 * v1 - 1.0 / 6.0 * v2;
+  double q13 = -(1.0 / 6.0 * vm1) + 5.0 / 6.0 * v0 + 1.0 / 3.0 * v1;
+  double q23 = 1.0 / 3.0 * vm2 - 7.0 / 6.0 * vm1 + 11.0 / 6.0 * v0;
+  return (a0 * q03 + a1 * q13 + a2 * q23) / am;
+}
+template <int VS>
+__device__ __forceinline__ double weno5M(const double* v) {
+  const double ep = 1.0e-6, C03 = 3.0 / 10.0, C13 = 3.0 / 5.0, C23 = 1.0 / 10.0;
+  const double vm1 = v[-VS], v0 = v[0], v1 = v[VS], v2 = v[2 * VS], v3 = v[3 * VS];
+  double S0 = 13.0 / 12.0 * q2(v1 - 2.0 * v0 + vm1) + 1.0 / 4.0 * q2(3.0 * v1 - 4.0 * v0 + vm1);
+  double S1 = 13.0 / 12.0 * q2(v2 - 2.0 * v1 + v0) + 1.0 / 4.0 * q2(v2 - v0);
+  double S2 = 13.0 / 12.0 * q2(v3 - 2.0 * v2 + v1) + 1.0 / 4.0 * q2(v3 - 4.0 * v2 + 3.0 * v1);
+  double a0 = C03 / q2(ep + S0);
+  double a1 = C13 / q2(ep + S1);
+  double a2 = C23 / q2(ep + S2);
+  double am = a0 + a1 + a2;
+  double q03 = 1.0 / 3.0 * v1 + 5.0 / 6.0 * v0 - 1.0 / 6.0 * vm1;
+  double q13 = -(1.0 / 6.0 * v2) + 5.0 / 6.0 * v1 + 1.0 / 3.0 * v0;
+  double q23 = 1.0 / 3.0 * v3 - 7.0 / 6.0 * v2 + 11.0 / 6.0 * v1;
+  return (a0 * q03 + a1 * q13 + a2 * q23) / am;
+}
+// WENO5 with the out-of-domain sub-stencil removed; del 1 = left, 2 = right (DEL_LIFT / DEL_RIGHT)
+template <int VS>
+__device__ __forceinline__ double weno5P_bnd(const double* v, int del) {
+  const double ep = 1.0e-6, C03 = 3.0 / 10.0, C13 = 3.0 / 5.0, C23 = 1.0 / 10.0;
+  const double vm2 = v[-2 * VS], vm1 = v[-VS], v0 = v[0], v1 = v[VS], v2 = v[2 * VS];
+  double a0 = 0.0, q03 = 0.0, a2 = 0.0, q23 = 0.0;
+  if (del != 2) {
+    double S0 = 13.0 / 12.0 * q2(v0 - 2.0 * v1 + v2) + 1.0 / 4.0 * q2(3.0 * v0 - 4.0 * v1 + v2);
+    a0 = C03 / q2(ep + S0);
+    q03 = 1.0 / 3.0 * v0 + 5.0 / 6.0 * v1 - 1.0 / 6.0 * v2;
+  }
+  double S1 = 13.0 / 12.0 * q2(vm1 - 2.0 * v0 + v1) + 1.0 / 4.0 * q2(vm1 - v1);
+  double a1 = C13 / q2(ep + S1);
+  double q13 = -(1.0 / 6.0 * vm1) + 5.0 / 6.0 * v0 + 1.0 / 3.0 * v1;
+  if (del != 1) {
+    double S2 = 13.0 / 12.0 * q2(vm2 - 2.0 * vm1 + v0) + 1.0 / 4.0 * q2(vm2 - 4.0 * vm1 + 3.0 * v0);
+    a2 = C23 / q2(ep + S2);
+    q23 = 1.0 / 3.0 * vm2 - 7.0 / 6.0 * vm1 + 11.0 / 6.0 * v0;
+  }
+  double am = a0 + a1 + a2;
+  return (a0 * q03 + a1 * q13 + a2 * q23) / am;
+}
+template <int VS>
+__device__ __forceinline__ double weno5M_bnd(const double* v, int del) {
+  const double ep = 1.0e-6, C03 = 3.0 / 10.0, C13 = 3.0 / 5.0, C23 = 1.0 / 10.0;
+  const double vm1 = v[-VS], v0 = v[0], v1 = v[VS], v2 = v[2 * VS], v3 = v[3 * VS];
+  double a0 = 0.0, q03 = 0.0, a2 = 0.0, q23 = 0.0;
+  if (del != 1) {
+    double S0 = 13.0 / 12.0 * q2(v1 - 2.0 * v0 + vm1) + 1.0 / 4.0 * q2(3.0 * v1 - 4.0 * v0 + vm1);
+    a0 = C03 / q2(ep + S0);
+    q03 = 1.0 / 3.0 * v1 + 5.0 / 6.0 * v0 - 1.0 / 6.0 * vm1;
+  }
+  double S1 = 13.0 / 12.0 * q2(v2 - 2.0 * v1 + v0) + 1.0 / 4.0 * q2(v2 - v0);
+  double a1 = C13 / q2(ep + S1);
+  double q13 = -(1.0 / 6.0 * v2) + 5.0 / 6.0 * v1 + 1.0 / 3.0 * v0;
+  if (del != 2) {
+    double S2 = 13.0 / 12.0 * q2(v3 - 2.0 * v2 + v1) + 1.0 / 4.0 * q2(v3 - 4.0 * v2 + 3.0 * v1);
+    a2 = C23 / q2(ep + S2);
+    q23 = 1.0 / 3.0 * v3 - 7.0 / 6.0 * v2 + 11.0 / 6.0 * v1;
+  }
+  double am = a0 + a1 + a2;
+  return (a0 * q03 + a1 * q13 + a2 * q23) / am;
+}
+
+// WENO7-JS (Balsara-Shu smoothness), OCFD_Schemes.f90:59-197
+#define W7C                                                                                                  \
+  const double C0 = 1.0 / 35.0, C1 = 12.0 / 35.0, C2 = 18.0 / 35.0, C3 = 4.0 / 35.0;                       \
+  const double a11 = -2.0 / 6.0, a12 = 9.0 / 6.0, a13 = -18.0 / 6.0, a14 = 11.0 / 6.0;                      \
+  const double a21 = 1.0 / 6.0, a23 = 3.0 / 6.0, a24 = 2.0 / 6.0;                                          \
+  const double a31 = -2.0 / 6.0, a32 = -3.0 / 6.0, a34 = -1.0 / 6.0;                                       \
+  const double a41 = -11.0 / 6.0, a42 = 18.0 / 6.0, a43 = -9.0 / 6.0, a44 = 2.0 / 6.0;                      \
+  const double b12 = 4.0, b13 = -5.0, b14 = 2.0, b22 = -2.0, b41 = 2.0, b42 = -5.0, b43 = 4.0, c12 = 3.0;   \
+  const double d12 = 13.0 / 12.0, d13 = 1043.0 / 960.0, d14 = 1.0 / 12.0;                                   \
+  const double e11 = -3.0 / 12.0, e12 = 13.0 / 12.0, e13 = -23.0 / 12.0, e14 = 25.0 / 12.0;                 \
+  const double e21 = 1.0 / 12.0, e22 = -5.0 / 12.0, e23 = 13.0 / 12.0, e24 = 3.0 / 12.0;                    \
+  const double e31 = -1.0 / 12.0, e32 = 7.0 / 12.0, e33 = 7.0 / 12.0, e34 = -1.0 / 12.0;                    \
+  const double e41 = 3.0 / 12.0, e42 = 13.0 / 12.0, e43 = -5.0 / 12.0, e44 = 1.0 / 12.0;                    \
+  const double ep = 1.0e-8;
+
+// generic WENO7 on seven values w0..w6 ordered upwind -> downwind (P: v(i-3..i+3); M: v(i+4..i-2))
+__device__ __forceinline__ double weno7_core(double w0, double w1, double w2, double w3, double w4, double w5,
+                                             double w6) {
+  W7C
+  double S10 = a11 * w0 + a12 * w1 + a13 * w2 + a14 * w3;
+  double S11 = a21 * w1 - w2 + a23 * w3 + a24 * w4;
+  double S12 = a31 * w2 + a32 * w3 + w4 + a34 * w5;
+  double S13 = a41 * w3 + a42 * w4 + a43 * w5 + a44 * w6;
+  double S20 = -w0 + b12 * w1 + b13 * w2 + b14 * w3;
+  double S21 = w2 + b22 * w3 + w4;
+  double S22 = w3 + b22 * w4 + w5;
+  double S23 = b41 * w3 + b42 * w4 + b43 * w5 - w6;
+  double S30 = -w0 + c12 * (w1 - w2) + w3;
+  double S31 = -w1 + c12 * (w2 - w3) + w4;
+  double S32 = -w2 + c12 * (w3 - w4) + w5;
+  double S33 = -w3 + c12 * (w4 - w5) + w6;
+  double S0 = S10 * S10 + d12 * S20 * S20 + d13 * S30 * S30 + d14 * S10 * S30;
+  double S1 = S11 * S11 + d12 * S21 * S21 + d13 * S31 * S31 + d14 * S11 * S31;
+  double S2 = S12 * S12 + d12 * S22 * S22 + d13 * S32 * S32 + d14 * S12 * S32;
+  double S3 = S13 * S13 + d12 * S23 * S23 + d13 * S33 * S33 + d14 * S13 * S33;
+  double a0 = C0 / q2(ep + S0);
+  double a1 = C1 / q2(ep + S1);
+  double a2 = C2 / q2(ep + S2);
+  double a3 = C3 / q2(ep + S3);
+  double am = a0 + a1 + a2 + a3;
+  double q0 = e11 * w0 + e12 * w1 + e13 * w2 + e14 * w3;
+  double q1 = e21 * w1 + e22 * w2 + e23 * w3 + e24 * w4;
+  double q2_ = e31 * w2 + e32 * w3 + e33 * w4 + e34 * w5;
+  double q3_ = e41 * w3 + e42 * w4 + e43 * w5 + e44 * w6;
+  return (a0 * q0 + a1 * q1 + a2 * q2_ + a3 * q3_) / am;
+}
+template <int VS>
+__device__ __forceinline__ double weno7P(const double* v) {
+  return weno7_core(v[-3 * VS], v[-2 * VS], v[-VS], v[0], v[VS], v[2 * VS], v[3 * VS]);
+}
+template <int VS>
+__device__ __forceinline__ double weno7M(const double* v) {
+  return weno7_core(v[4 * VS], v[3 * VS], v[2 * VS], v[VS], v[0], v[-VS], v[-2 * VS]);
+}
+
+__device__ __forceinline__ double minmod2(double x1, double x2) {
+  return 0.5 * (fsgn(x1) + fsgn(x2)) * fmin(fabs(x1), fabs(x2));
+}
+__device__ __forceinline__ double minmod4(double x1, double x2, double x3, double x4) {
+  double m = 0.5 * (fsgn(x1) + fsgn(x2));
+  m = m * fabs(0.5 * (fsgn(x1) + fsgn(x3)));
+  m = m * fabs(0.5 * (fsgn(x1) + fsgn(x4)));
+  m = m * fmin(fmin(fmin(fabs(x1), fabs(x2)), fabs(x3)), fabs(x4));
+  return m;
+}
+// OMP6 (Leng & Li 2013) on eight values w0..w7 ordered upwind -> downwind:
+// P: v(i-3..i+4), M: v(i+4..i-3). The reference's flux- limiter is not the mirror image of the
+// flux+ one in one term: its lc uses 0.5*(v(i+1)-v(i)) (OCFD_Schemes.f90:270), i.e. w3-w4,
+// where flux+ uses 0.5*(v(i)-v(i-1)) = w3-w2 (OCFD_Schemes.f90:233). PLUS selects which.
+template <bool PLUS>
+__device__ __forceinline__ double omp6_core(double w0, double w1, double w2, double w3, double w4, double w5,
+                                            double w6, double w7) {
+  const double m_ = 0.015, n_ = 0.0;
+  const double a = 0.5 * (m_ + n_), b = 0.5 * (m_ - n_);
+  const double o1 = a, o2 = 1.0 / 60.0 - b - 6.0 * a, o3 = -2.0 / 15.0 + 6.0 * b + 15.0 * a,
+               o4 = 37.0 / 60.0 - 15.0 * b - 20.0 * a, o5 = 37.0 / 60.0 + 20.0 * b + 15.0 * a,
+               o6 = -2.0 / 15.0 - 6.0 * a - 15.0 * b, o7 = 1.0 / 60.0 + a + 6.0 * b, o8 = -b;
+  const double kappa = 4.0, ep = (double)1.0e-10f;
+  // reference P: a1*v(i+4)+a2*v(i+3)+...+a8*v(i-3)
+  double mid = o1 * w7 + o2 * w6 + o3 * w5 + o4 * w4 + o5 * w3 + o6 * w2 + o7 * w1 + o8 * w0;
+  double mp = w3 + minmod2(w4 - w3, kappa * (w3 - w2));
+  if ((mid - w3) * (mid - mp) >= ep) {
+    double d1 = w1 + w3 - 2.0 * w2;
+    double d2 = w2 + w4 - 2.0 * w3;
+    double d3 = w3 + w5 - 2.0 * w4;
+    double ul = w3 + kappa * (w3 - w2);
+    double md = 0.5 * (w3 + w4) - 0.5 * minmod4(4.0 * d2 - d3, 4.0 * d3 - d2, d2, d3);
+    double lc = w3 + 0.5 * (PLUS ? (w3 - w2) : (w3 - w4)) + kappa * minmod4(4.0 * d1 - d2, 4.0 * d2 - d1, d2, d1) / 3.0;
+    double fmn = fmax(fmin(fmin(w3, w4), md), fmin(fmin(w3, ul), lc));
+    double fmx = fmin(fmax(fmax(w3, w4), md), fmax(fmax(w3, ul), lc));
+    mid = mid + minmod2(fmx - mid, fmn - mid);
+  }
+  return mid;
+}
+template <int VS>
+__device__ __forceinline__ double omp6P(const double* v) {
+  return omp6_core<true>(v[-3 * VS], v[-2 * VS], v[-VS], v[0], v[VS], v[2 * VS], v[3 * VS], v[4 * VS]);
+}
+template <int VS>
+__device__ __forceinline__ double omp6M(const double* v) {
+  return omp6_core<false>(v[4 * VS], v[3 * VS], v[2 * VS], v[VS], v[0], v[-VS], v[-2 * VS], v[-3 * VS]);
+}
+template <int VS>
+__device__ __forceinline__ double ud7lP(const double* v) {
+  const double* U = cC.UD7L;
+  return U[0] * v[-3 * VS] + U[1] * v[-2 * VS] + U[2] * v[-VS] + U[3] * v[0] + U[4] * v[VS] + U[5] * v[2 * VS] +
+         U[6] * v[3 * VS] + U[7] * v[4 * VS];
+}
+template <int VS>
+__device__ __forceinline__ double ud7lM(const double* v) {
+  const double* U = cC.UD7L;
+  return U[0] * v[4 * VS] + U[1] * v[3 * VS] + U[2] * v[2 * VS] + U[3] * v[VS] + U[4] * v[0] + U[5] * v[-VS] +
+         U[6] * v[-2 * VS] + U[7] * v[-3 * VS];
+}
+
+__device__ __forceinline__ int hybrid_index(double R0) {
+  if (R0 <= cC.theta1) return 1;
+  if (R0 <= cC.theta2) return 2;
+  return 3;
+}
+
+// Numerical flux at interface i (0..n) of a pencil of length n in direction dir, for the
+// positive (PLUS) or negative split flux, including the boundary closures of OCFD2d_flux1/2
+// (OCFD_inviscous.f90:209-362). v points at v(i).
+template <int SCHEME, bool PLUS, int VS>
+__device__ __forceinline__ double interface_flux(const double* v, int i, int n, int dir, int scm) {
+  const int Ka = PLUS ? cC.Ka1 : cC.Ka2, Kb = PLUS ? cC.Kb1 : cC.Kb2;
+  const int b0 = cC.bound[dir][0], b1 = cC.bound[dir][1];
+  const int s0 = cC.sb[2 * dir], s1 = cC.sb[2 * dir + 1];
+  if (b0 == 1 && i <= -Ka && s0 != -1) {
+    if (s0 == 0) {
+      if (PLUS) {
+        if (i <= 1) {  // (2 f(1) + 5 f(2) - f(3)) / 6 at i = 0 and 1
+          const double* f1 = v + (1 - i) * VS;
+          return (2.0 * f1[0] + 5.0 * f1[VS] - f1[2 * VS]) / 6.0;
+        }
+        if (i == 2) return weno5P_bnd<VS>(v, 1);
+        return weno5P<VS>(v);
+      } else {
+        if (i == 0) return (2.0 * v[3 * VS] - 7.0 * v[2 * VS] + 11.0 * v[VS]) / 6.0;
+        if (i == 1) return weno5M_bnd<VS>(v, 1);
+        return weno5M<VS>(v);
+      }
+    }
+    return PLUS ? weno5P<VS>(v) : weno5M<VS>(v);
+  }
+  if (b1 == 1 && i >= n - Kb + 1 && s1 != -1) {
+    if (s1 == 0) {
+      if (PLUS) {
+        if (i == n) return (2.0 * v[-2 * VS] - 7.0 * v[-VS] + 11.0 * v[0]) / 6.0;
+        if (i == n - 1) return weno5P_bnd<VS>(v, 2);
+        return weno5P<VS>(v);
+      } else {
+        if (i >= n - 1) {  // (2 f(n) + 5 f(n-1) - f(n-2)) / 6 at i = n-1 and n
+          const double* fn = v + (n - i) * VS;
+          return (2.0 * fn[0] + 5.0 * fn[-VS] - fn[-2 * VS]) / 6.0;
+        }
+        if (i == n - 2) return weno5M_bnd<VS>(v, 2);
+        return weno5M<VS>(v);
+      }
+    }
+    return PLUS ? weno5P<VS>(v) : weno5M<VS>(v);
+  }
+  if (SCHEME == OCFD_SCHEME_WENO5) return PLUS ? weno5P<VS>(v) : weno5M<VS>(v);
+  if (SCHEME == OCFD_SCHEME_WENO7) return PLUS ? weno7P<VS>(v) : weno7M<VS>(v);
+  if (SCHEME == OCFD_SCHEME_OMP6) return PLUS ? omp6P<VS>(v) : omp6M<VS>(v);
+  if (SCHEME == OCFD_SCHEME_UD7L) return PLUS ? ud7lP<VS>(v) : ud7lM<VS>(v);
+  // HYBRID
+  if (scm == 1) return PLUS ? ud7lP<VS>(v) : ud7lM<VS>(v);
+  if (scm == 2) return PLUS ? weno7P<VS>(v) : weno7M<VS>(v);
+  return PLUS ? weno5P<VS>(v) : weno5M<VS>(v);
+}
+
+}  // namespace ocfd

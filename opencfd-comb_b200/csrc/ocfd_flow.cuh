@@ -1,0 +1,894 @@
+// Flow kernels of the OpenCFD-Comb hot path on sm_100a.
+//
+//  k_flux        one sweep direction of du_inviscous / du_scaler_invis
+//                (OCFD_inviscous.f90:47-202, OCFD_scaler_inviscous.f90:1-84): a tile of pencils is
+//                split (Steger-Warming / LLF, OCFD_flux_split.f90) into shared memory once per
+//                point, every interface of the tile is reconstructed once (WENO5/7, OMP6, UD7L,
+//                HYBRID + boundary closures), and the flux difference is combined into du.
+//  k_visc_ev     first pass of du_viscous (OCFD_viscous.f90:38-108): CD6/CD8 gradients, stresses,
+//                heat flux -> Ev1/Ev2/Ev3.
+//  k_visc_div    second pass (OCFD_viscous.f90:114-129): divergence of Ev into du(2..5).
+//  k_rk_prims    OCFD_time_adv_RK3 + comput_flow_variables + Rescaling_di + comput_T_P.
+//  k_repair_et   handle_NegativeEt replay (OCFD_handle_NegativeT.f90).
+//  k_bc_*        OCFD_bc, ocfd_bc_BoundaryLayer, Flow_Ghost_Extent_2nd.
+#pragma once
+#include "ocfd_device.cuh"
+
+namespace ocfd {
+
+// per-step error / statistics words (device)
+struct DevStatus {
+  int neg_count;          // cells with Et <= 0 in the current stage
+  int neg_list[16];       // their interior linear indices (first 16)
+  int error;              // OCFD_ERR_* raised on the device
+  int nan_count;
+  int newton_fail;
+  unsigned long long neg_total;
+};
+
+// ---------------------------------------------------------------- flux splitting at one point
+template <int SPLIT>
+__device__ __forceinline__ void split_point(double Et1, double p1, double c1, double d1, double u1, double v1,
+                                            double w1, double A1, double A2, double A3, double* fp, double* fm) {
+  if (SPLIT == OCFD_SPLIT_SW) {
+    double gamma = p1 / Et1 + 1.0;
+    double tmp1 = 2.0 * (gamma - 1.0);
+    double tmp3 = (3.0 - gamma) / (2.0 * (gamma - 1.0));
+    double ss = sqrt(A1 * A1 + A2 * A2 + A3 * A3);
+    double ss1 = 1.0 / ss;
+    double ak1 = A1 * ss1, ak2 = A2 * ss1, ak3 = A3 * ss1;
+    double vs = A1 * u1 + A2 * v1 + A3 * w1;
+    double E1 = vs, E2 = vs - c1 * ss, E3 = vs + c1 * ss;
+    double E1P = (E1 + fabs(E1)) * 0.5, E2P = (E2 + fabs(E2)) * 0.5, E3P = (E3 + fabs(E3)) * 0.5;
+    double E1M = E1 - E1P, E2M = E2 - E2P, E3M = E3 - E3P;
+    double tmp0 = d1 / (2.0 * gamma);
+    double uc1 = u1 - c1 * ak1, uc2 = u1 + c1 * ak1;
+    double vc1 = v1 - c1 * ak2, vc2 = v1 + c1 * ak2;
+    double wc1 = w1 - c1 * ak3, wc2 = w1 + c1 * ak3;
+    double vvc1 = (uc1 * uc1 + vc1 * vc1 + wc1 * wc1) * 0.5;
+    double vvc2 = (uc2 * uc2 + vc2 * vc2 + wc2 * wc2) * 0.5;
+    double vv = (gamma - 1.0) * (u1 * u1 + v1 * v1 + w1 * w1);
+    double W2 = tmp3 * c1 * c1;
+    fp[0] = tmp0 * (tmp1 * E1P + E2P + E3P);
+    fp[1] = tmp0 * (tmp1 * E1P * u1 + E2P * uc1 + E3P * uc2);
+    fp[2] = tmp0 * (tmp1 * E1P * v1 + E2P * vc1 + E3P * vc2);
+    fp[3] = tmp0 * (tmp1 * E1P * w1 + E2P * wc1 + E3P * wc2);
+    fp[4] = tmp0 * (E1P * vv + E2P * vvc1 + E3P * vvc2 + W2 * (E2P + E3P));
+    fm[0] = tmp0 * (tmp1 * E1M + E2M + E3M);
+    fm[1] = tmp0 * (tmp1 * E1M * u1 + E2M * uc1 + E3M * uc2);
+    fm[2] = tmp0 * (tmp1 * E1M * v1 + E2M * vc1 + E3M * vc2);
+    fm[3] = tmp0 * (tmp1 * E1M * w1 + E2M * wc1 + E3M * wc2);
+    fm[4] = tmp0 * (E1M * vv + E2M * vvc1 + E3M * vvc2 + W2 * (E2M + E3M));
+  } else {
+    double ss = sqrt(A1 * A1 + A2 * A2 + A3 * A3);
+    double un = A1 * u1 + A2 * v1 + A3 * w1;
+    double lam = fabs(un) + ss * c1;
+    double E0 = Et1 + 0.5 * d1 * (u1 * u1 + v1 * v1 + w1 * w1);
+    fp[0] = 0.5 * (d1 * un + lam * d1);
+    fp[1] = 0.5 * (d1 * u1 * un + A1 * p1 + lam * d1 * u1);
+    fp[2] = 0.5 * (d1 * v1 * un + A2 * p1 + lam * d1 * v1);
+    fp[3] = 0.5 * (d1 * w1 * un + A3 * p1 + lam * d1 * w1);
+    fp[4] = 0.5 * ((E0 + p1) * un + lam * E0);
+    fm[0] = 0.5 * (d1 * un - lam * d1);
+    fm[1] = 0.5 * (d1 * u1 * un + A1 * p1 - lam * d1 * u1);
+    fm[2] = 0.5 * (d1 * v1 * un + A2 * p1 - lam * d1 * v1);
+    fm[3] = 0.5 * (d1 * w1 * un + A3 * p1 - lam * d1 * w1);
+    fm[4] = 0.5 * ((E0 + p1) * un - lam * E0);
+  }
+}
+
+// tile shapes: x sweeps run along the contiguous index, so a tile is a long chunk of few
+// lines; y / z sweeps put 32 contiguous i-lines across the warp and a short chunk along j / k.
+template <int DIR>
+struct Tile {
+  static constexpr int C = 64, NL = 4;
+};
+template <>
+struct Tile<1> {
+  static constexpr int C = 16, NL = 32;
+};
+template <>
+struct Tile<2> {
+  static constexpr int C = 16, NL = 32;
+};
+
+struct FluxArgs {
+  const double *d, *u, *v, *w, *p, *Et;  // halo arrays
+  const double* fs;                      // scalar (species density) for SCALAR sweeps
+  const double* Rh;                      // hybrid sensor (halo array)
+  double* out;                           // du (5 x N) or Dus (N)
+  Geo g;
+};
+
+template <int DIR, int SCHEME, int SPLIT, bool SEP, bool SCALAR>
+__global__ void __launch_bounds__(256) k_flux(FluxArgs a) {
+  constexpr int C = Tile<DIR>::C, NL = Tile<DIR>::NL, P = C + 8, NC = SCALAR ? 1 : 5;
+  constexpr int VS = DIR == 0 ? 1 : NL;  // stride of consecutive sweep points in shared memory
+  extern __shared__ double smem[];
+  double* sfp = smem;                // [NC][..]
+  double* sfm = smem + NC * P * NL;  // [NC][..]
+  double* sh1 = sfm + NC * P * NL;   // [NC][(C+1) x NL]
+  double* sh2 = sh1 + NC * (C + 1) * NL;
+  auto sidx = [&](int c, int p, int l) { return DIR == 0 ? (c * NL + l) * P + p : (c * P + p) * NL + l; };
+  auto hidx2 = [&](int c, int t, int l) { return DIR == 0 ? (c * NL + l) * (C + 1) + t : (c * (C + 1) + t) * NL + l; };
+
+  const int n = DIR == 0 ? cC.nx : (DIR == 1 ? cC.ny : cC.nz);
+  const int s0 = (DIR == 0 ? blockIdx.x : blockIdx.y) * C + 1;  // first cell of the chunk
+  const int l0 = DIR == 0 ? blockIdx.y * NL + 1 : blockIdx.x * NL + 1;
+  const int bz = blockIdx.z + 1;
+  const int nl_max = DIR == 0 ? cC.ny : cC.nx;
+  const int ncell = min(C, n - s0 + 1);
+  const int stride = hstride(DIR);
+  auto coords = [&](int s, int l, int& i, int& j, int& k) {
+    if (DIR == 0) { i = s; j = l0 + l; k = bz; }
+    else if (DIR == 1) { i = l0 + l; j = s; k = bz; }
+    else { i = l0 + l; j = bz; k = s; }
+  };
+
+  // phase 1: split fluxes of every point of the tile (cells plus 4 on each side)
+  for (int idx = threadIdx.x; idx < P * NL; idx += blockDim.x) {
+    int p, l;
+    if (DIR == 0) { p = idx % P; l = idx / P; }
+    else { l = idx % NL; p = idx / NL; }
+    int s = s0 - 4 + p;
+    double fp[5], fm[5];
+    if (l0 + l <= nl_max && p < ncell + 8) {
+      int i, j, k;
+      coords(s, l, i, j, k);
+      int q = hidx(i, j, k);
+      double A1, A2, A3;
+      metric_dir<SEP>(a.g, DIR, i, j, k, q, A1, A2, A3);
+      if (SCALAR) {
+        double vs = A1 * __ldg(a.u + q) + A2 * __ldg(a.v + q) + A3 * __ldg(a.w + q);
+        double fsq = __ldg(a.fs + q);
+        fp[0] = 0.5 * (vs + fabs(vs)) * fsq;
+        fm[0] = 0.5 * (vs - fabs(vs)) * fsq;
+      } else {
+        double pp = __ldg(a.p + q), et = __ldg(a.Et + q), dd = __ldg(a.d + q);
+        double gamma = pp / et + 1.0;
+        double cc = sqrt(gamma * pp / dd);  // comput_cc
+        split_point<SPLIT>(et, pp, cc, dd, __ldg(a.u + q), __ldg(a.v + q), __ldg(a.w + q), A1, A2, A3, fp, fm);
+      }
+    } else {
+#pragma unroll
+      for (int c = 0; c < NC; c++) fp[c] = fm[c] = 0.0;
+    }
+#pragma unroll
+    for (int c = 0; c < NC; c++) {
+      sfp[sidx(c, p, l)] = fp[c];
+      sfm[sidx(c, p, l)] = fm[c];
+    }
+  }
+  __syncthreads();
+
+  // phase 2: numerical fluxes at interfaces s0-1 .. s0-1+ncell
+  for (int idx = threadIdx.x; idx < (C + 1) * NL; idx += blockDim.x) {
+    int t, l;
+    if (DIR == 0) { t = idx % (C + 1); l = idx / (C + 1); }
+    else { l = idx % NL; t = idx / NL; }
+    if (l0 + l > nl_max || t > ncell) continue;
+    int ig = s0 - 1 + t;  // reference interface index hh(ig), between cells ig and ig+1
+    int scm = 0;
+    if (SCHEME == OCFD_SCHEME_HYBRID) {
+      int i, j, k;
+      coords(ig, l, i, j, k);
+      int q = hidx(i, j, k);
+      scm = hybrid_index(fmax(__ldg(a.Rh + q), __ldg(a.Rh + q + stride)));
+    }
+#pragma unroll
+    for (int c = 0; c < NC; c++) {
+      const double* vp = sfp + sidx(c, t + 3, l);
+      const double* vm = sfm + sidx(c, t + 3, l);
+      sh1[hidx2(c, t, l)] = interface_flux<SCHEME, true, VS>(vp, ig, n, DIR, scm);
+      sh2[hidx2(c, t, l)] = interface_flux<SCHEME, false, VS>(vm, ig, n, DIR, scm);
+    }
+  }
+  __syncthreads();
+
+  // phase 3: flux difference into du
+  const double h1 = cC.h1[DIR];
+  const long long N = cC.N;
+  for (int idx = threadIdx.x; idx < C * NL; idx += blockDim.x) {
+    int t, l;
+    if (DIR == 0) { t = idx % C; l = idx / C; }
+    else { l = idx % NL; t = idx / NL; }
+    if (l0 + l > nl_max || t >= ncell) continue;
+    int i, j, k;
+    coords(s0 + t, l, i, j, k);
+    int nn = nidx(i, j, k);
+    double ajac = 0.0;
+    if (DIR == 2) ajac = metric_jac<SEP>(a.g, i, j, k, hidx(i, j, k));
+#pragma unroll
+    for (int c = 0; c < NC; c++) {
+      double val = (sh1[hidx2(c, t + 1, l)] - sh1[hidx2(c, t, l)] + sh2[hidx2(c, t + 1, l)] - sh2[hidx2(c, t, l)]) * h1;
+      double* o = a.out + (size_t)c * N + nn;
+      if (DIR == 0) *o = val;
+      else if (DIR == 1) *o = *o + val;
+      else *o = -(*o + val) * ajac;
+    }
+    if (DIR == 2 && !SCALAR && cC.if_mass_force == 1) {
+      int q = hidx(i, j, k);
+      double dd = a.d[q];
+      double* o = a.out + nn;
+      o[N] = o[N] + dd * cC.mass_force[0];
+      o[2 * N] = o[2 * N] + dd * cC.mass_force[1];
+      o[3 * N] = o[3 * N] + dd * cC.mass_force[2];
+      o[4 * N] = o[4 * N] + dd * (a.u[q] * cC.mass_force[0] + a.v[q] * cC.mass_force[1] + a.w[q] * cC.mass_force[2]);
+    }
+  }
+}
+
+template <int DIR, bool SCALAR>
+constexpr size_t flux_smem() {
+  constexpr int C = Tile<DIR>::C, NL = Tile<DIR>::NL, P = C + 8, NC = SCALAR ? 1 : 5;
+  return sizeof(double) * (size_t)(2 * NC * P * NL + 2 * NC * (C + 1) * NL);
+}
+
+// ---------------------------------------------------------------- CD6 / CD8 derivative
+// OCFD_dx0/dy0/dz0 (OCFD_dxyz_viscous.f90) at one interior point q, sweep index ii of n.
+__device__ __forceinline__ double cdiff(const double* __restrict__ f, int q, int dir, int ii, int n) {
+  const int s = hstride(dir);
+  if (!cC.iper[dir]) {
+    const double h2 = cC.h2x[dir], h12 = cC.h12x[dir];
+    if (ii == 1) return (-3.0 * f[q] + 4.0 * f[q + s] - f[q + 2 * s]) / h2;
+    if (ii == 2) return (f[q + s] - f[q - s]) / h2;
+    if (ii == 3) return (8.0 * (f[q + s] - f[q - s]) - (f[q + 2 * s] - f[q - 2 * s])) / h12;
+    if (ii == n) return (f[q - 2 * s] - 4.0 * f[q - s] + 3.0 * f[q]) / h2;
+    if (ii == n - 1) return (f[q + s] - f[q - s]) / h2;
+    if (ii == n - 2) return (8.0 * (f[q + s] - f[q - s]) - (f[q + 2 * s] - f[q - 2 * s])) / h12;
+    if (cC.cd8_on && (ii == 4 || ii == n - 3)) {
+      const double* a = cC.cd6[dir];
+      return a[0] * (f[q + 3 * s] - f[q - 3 * s]) + a[1] * (f[q + 2 * s] - f[q - 2 * s]) + a[2] * (f[q + s] - f[q - s]);
+    }
+  }
+  if (!cC.cd8_on) {
+    const double* a = cC.cd6[dir];
+    return a[0] * (f[q + 3 * s] - f[q - 3 * s]) + a[1] * (f[q + 2 * s] - f[q - 2 * s]) + a[2] * (f[q + s] - f[q - s]);
+  }
+  const double* c = cC.cd8[dir];
+  return c[0] * (f[q + s] - f[q - s]) + c[1] * (f[q + 2 * s] - f[q - 2 * s]) + c[2] * (f[q + 3 * s] - f[q - 3 * s]) +
+         c[3] * (f[q + 4 * s] - f[q - 4 * s]);
+}
+
+__device__ __forceinline__ bool cell_of(long long t, int& i, int& j, int& k) {
+  if (t >= cC.N) return false;
+  i = (int)(t % cC.nx) + 1;
+  long long r = t / cC.nx;
+  j = (int)(r % cC.ny) + 1;
+  k = (int)(r / cC.ny) + 1;
+  return true;
+}
+
+struct ViscArgs {
+  const double *d, *u, *v, *w, *T, *di;
+  const double *amu, *amk;        // precomputed transport (NS > 1) or nullptr
+  const double *qpx, *qpy, *qpz;  // species enthalpy fluxes (NS > 1) or nullptr
+  double* ev[3][4];               // Ev1, Ev2, Ev3 (halo arrays)
+  Geo g;
+};
+
+template <int NS, bool SEP>
+__global__ void __launch_bounds__(256) k_visc_ev(ViscArgs a) {
+  int i, j, k;
+  if (!cell_of((long long)blockIdx.x * blockDim.x + threadIdx.x, i, j, k)) return;
+  const int q = hidx(i, j, k), nn = nidx(i, j, k);
+  double g[4][3];  // d(u,v,w,T)/d(xi,eta,zeta)
+  const double* fl[4] = {a.u, a.v, a.w, a.T};
+  const int ii[3] = {i, j, k};
+  const int nd[3] = {cC.nx, cC.ny, cC.nz};
+#pragma unroll
+  for (int m = 0; m < 4; m++)
+#pragma unroll
+    for (int dd = 0; dd < 3; dd++) g[m][dd] = cdiff(fl[m], q, dd, ii[dd], nd[dd]);
+  double A[9], A1[9];
+  metric_all<SEP>(a.g, i, j, k, q, A, A1);
+  // A: Akx Aky Akz Aix Aiy Aiz Asx Asy Asz
+  double ux = g[0][0] * A[0] + g[0][1] * A[3] + g[0][2] * A[6];
+  double vx = g[1][0] * A[0] + g[1][1] * A[3] + g[1][2] * A[6];
+  double wx = g[2][0] * A[0] + g[2][1] * A[3] + g[2][2] * A[6];
+  double Tx = g[3][0] * A[0] + g[3][1] * A[3] + g[3][2] * A[6];
+  double uy = g[0][0] * A[1] + g[0][1] * A[4] + g[0][2] * A[7];
+  double vy = g[1][0] * A[1] + g[1][1] * A[4] + g[1][2] * A[7];
+  double wy = g[2][0] * A[1] + g[2][1] * A[4] + g[2][2] * A[7];
+  double Ty = g[3][0] * A[1] + g[3][1] * A[4] + g[3][2] * A[7];
+  double uz = g[0][0] * A[2] + g[0][1] * A[5] + g[0][2] * A[8];
+  double vz = g[1][0] * A[2] + g[1][1] * A[5] + g[1][2] * A[8];
+  double wz = g[2][0] * A[2] + g[2][1] * A[5] + g[2][2] * A[8];
+  double Tz = g[3][0] * A[2] + g[3][1] * A[5] + g[3][2] * A[8];
+  double div = ux + vy + wz;
+  double amu1, amuk;
+  if (a.amu) {
+    amu1 = a.amu[nn];
+    amuk = a.amk[nn];
+  } else {  // comput_Amu_Amk_AMD inline (Comput_flow_variables.f90:69-98)
+    double d0[NS], Xi[NS], X0 = 0.0;
+#pragma unroll
+    for (int m = 0; m < NS; m++) {
+      d0[m] = a.di[(size_t)m * cC.H + q];
+      Xi[m] = d0[m] / cC.Mi[m];
+      X0 = X0 + Xi[m];
+    }
+#pragma unroll
+    for (int m = 0; m < NS; m++) Xi[m] = Xi[m] / X0;
+    double T = a.T[q];
+    amu1 = dev_viscosity<NS>(T, Xi);
+    double cp = dev_Cp<NS>(a.d[q], d0, T);
+    amuk = dev_conductivity<NS>(amu1, cp, T, Xi);
+  }
+  const double tmp2_3 = 2.0 / 3.0;
+  double s11 = (2.0 * ux - tmp2_3 * div) * amu1;
+  double s22 = (2.0 * vy - tmp2_3 * div) * amu1;
+  double s33 = (2.0 * wz - tmp2_3 * div) * amu1;
+  double s12 = (uy + vx) * amu1, s13 = (uz + wx) * amu1, s23 = (vz + wy) * amu1;
+  double qx = 0.0, qy = 0.0, qz = 0.0;
+  if (a.qpx) { qx = a.qpx[nn]; qy = a.qpy[nn]; qz = a.qpz[nn]; }
+  double uq = a.u[q], vq = a.v[q], wq = a.w[q];
+  double E1 = uq * s11 + vq * s12 + wq * s13 + amuk * Tx + qx;
+  double E2 = uq * s12 + vq * s22 + wq * s23 + amuk * Ty + qy;
+  double E3 = uq * s13 + vq * s23 + wq * s33 + amuk * Tz + qz;
+#pragma unroll
+  for (int dd = 0; dd < 3; dd++) {
+    double B1 = A1[3 * dd], B2 = A1[3 * dd + 1], B3 = A1[3 * dd + 2];
+    a.ev[dd][0][q] = B1 * s11 + B2 * s12 + B3 * s13;
+    a.ev[dd][1][q] = B1 * s12 + B2 * s22 + B3 * s23;
+    a.ev[dd][2][q] = B1 * s13 + B2 * s23 + B3 * s33;
+    a.ev[dd][3][q] = B1 * E1 + B2 * E2 + B3 * E3;
+  }
+}
+
+template <bool SEP>
+__global__ void __launch_bounds__(256) k_visc_div(const double* const* ev, double* du, Geo g) {
+  int i, j, k;
+  if (!cell_of((long long)blockIdx.x * blockDim.x + threadIdx.x, i, j, k)) return;
+  const int q = hidx(i, j, k), nn = nidx(i, j, k);
+  double ajac = metric_jac<SEP>(g, i, j, k, q);
+#pragma unroll
+  for (int m = 0; m < 4; m++) {
+    double uk = cdiff(ev[m], q, 0, i, cC.nx);
+    double ui = cdiff(ev[4 + m], q, 1, j, cC.ny);
+    double us = cdiff(ev[8 + m], q, 2, k, cC.nz);
+    double* o = du + (size_t)(m + 1) * cC.N + nn;
+    *o = *o + (uk + ui + us) * ajac;
+  }
+}
+
+// ---------------------------------------------------------------- species: viscous part
+// du_scaler_viscous (OCFD_scaler_viscous.f90:4-79). ci = fs/d over the full halo range first.
+static __global__ void k_ci(const double* fs, const double* d, double* ci, long long H) {
+  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < H) ci[t] = fs[t] / d[t];
+}
+template <bool SEP>
+__global__ void __launch_bounds__(256) k_scal_ev(int ks, const double* ci, const double* d, const double* T,
+                                                 const double* amd, double* qpx, double* qpy, double* qpz, double* e1,
+                                                 double* e2, double* e3, Geo g) {
+  int i, j, k;
+  if (!cell_of((long long)blockIdx.x * blockDim.x + threadIdx.x, i, j, k)) return;
+  const int q = hidx(i, j, k), nn = nidx(i, j, k);
+  double uk = cdiff(ci, q, 0, i, cC.nx), ui = cdiff(ci, q, 1, j, cC.ny), us = cdiff(ci, q, 2, k, cC.nz);
+  double A[9], A1[9];
+  metric_all<SEP>(g, i, j, k, q, A, A1);
+  double hi = dev_hi(ks, T[q]);
+  double cix = uk * A[0] + ui * A[3] + us * A[6];
+  double ciy = uk * A[1] + ui * A[4] + us * A[7];
+  double ciz = uk * A[2] + ui * A[5] + us * A[8];
+  double dD = d[q] * amd[(size_t)ks * cC.N + nn];
+  double E1 = dD * cix, E2 = dD * ciy, E3 = dD * ciz;
+  if (ks == 0) {
+    qpx[nn] = 0.0 + E1 * hi;
+    qpy[nn] = 0.0 + E2 * hi;
+    qpz[nn] = 0.0 + E3 * hi;
+  } else {
+    qpx[nn] = qpx[nn] + E1 * hi;
+    qpy[nn] = qpy[nn] + E2 * hi;
+    qpz[nn] = qpz[nn] + E3 * hi;
+  }
+  e1[q] = E1 * A1[0] + E2 * A1[1] + E3 * A1[2];
+  e2[q] = E1 * A1[3] + E2 * A1[4] + E3 * A1[5];
+  e3[q] = E1 * A1[6] + E2 * A1[7] + E3 * A1[8];
+}
+template <bool SEP>
+__global__ void __launch_bounds__(256) k_scal_div(const double* e1, const double* e2, const double* e3, double* dus,
+                                                  Geo g) {
+  int i, j, k;
+  if (!cell_of((long long)blockIdx.x * blockDim.x + threadIdx.x, i, j, k)) return;
+  const int q = hidx(i, j, k), nn = nidx(i, j, k);
+  double uk = cdiff(e1, q, 0, i, cC.nx), ui = cdiff(e2, q, 1, j, cC.ny), us = cdiff(e3, q, 2, k, cC.nz);
+  dus[nn] = dus[nn] + (uk + ui + us) * metric_jac<SEP>(g, i, j, k, q);
+}
+// Scalar_time_adv_RK3 (OCFD_Time_Adv.f90:134-166)
+static __global__ void k_scal_rk(int krk, double dt, const double* dus, const double* din, double* di) {
+  int i, j, k;
+  if (!cell_of((long long)blockIdx.x * blockDim.x + threadIdx.x, i, j, k)) return;
+  const int q = hidx(i, j, k), nn = nidx(i, j, k);
+  const double ra[3] = {0.0, 3.0 / 4.0, 1.0 / 3.0}, rb[3] = {1.0, 1.0 / 4.0, 2.0 / 3.0};
+  if (krk == 1) di[q] = din[nn] + dt * dus[nn];
+  else di[q] = ra[krk - 1] * din[nn] + rb[krk - 1] * (di[q] + dt * dus[nn]);
+}
+
+// comput_Amu_Amk_AMD for NS > 1 (Comput_flow_variables.f90:69-98)
+template <int NS>
+__global__ void __launch_bounds__(128) k_transport(const double* d, const double* T, const double* p,
+                                                   const double* di, double* amu, double* amk, double* amd) {
+  int i, j, k;
+  if (!cell_of((long long)blockIdx.x * blockDim.x + threadIdx.x, i, j, k)) return;
+  const int q = hidx(i, j, k), nn = nidx(i, j, k);
+  double d0[NS], Xi[NS], X0 = 0.0;
+#pragma unroll
+  for (int m = 0; m < NS; m++) {
+    d0[m] = di[(size_t)m * cC.H + q];
+    Xi[m] = d0[m] / cC.Mi[m];
+    X0 = X0 + Xi[m];
+  }
+#pragma unroll
+  for (int m = 0; m < NS; m++) Xi[m] = Xi[m] / X0;
+  double Tq = T[q];
+  double mu = dev_viscosity<NS>(Tq, Xi);
+  double cp = dev_Cp<NS>(d[q], d0, Tq);
+  amu[nn] = mu;
+  amk[nn] = dev_conductivity<NS>(mu, cp, Tq, Xi);
+  double ad[NS];
+  dev_diffusion<NS>(ad, mu, Tq, d[q], p[q], Xi);
+#pragma unroll
+  for (int m = 0; m < NS; m++) amd[(size_t)m * cC.N + nn] = ad[m];
+}
+
+// ---------------------------------------------------------------- halo exchange (single rank)
+// exchange_boundary_x/y/z (OCFD_mpi.f90:201-236): in a periodic direction the LAP face planes
+// wrap around; a non-periodic face halo is left untouched (MPI_PROC_NULL).
+struct ExchArgs {
+  double* f[24];
+  int nf;
+  int dirmask;  // which directions to exchange (bit d)
+};
+static __global__ void k_exchange(ExchArgs a) {
+  // thread grid: x = face point, y = field
+  const int fidx = blockIdx.y;
+  if (fidx >= a.nf) return;
+  double* f = a.f[fidx];
+  const int L = OCFD_L;
+  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long nxz = (long long)L * cC.ny * cC.nz, nyz = (long long)L * cC.nx * cC.nz,
+                  nzz = (long long)L * cC.nx * cC.ny;
+  if ((a.dirmask & 1) && cC.iper[0] && t < nxz) {
+    int l = (int)(t % L), j = (int)((t / L) % cC.ny) + 1, k = (int)(t / L / cC.ny) + 1;
+    f[hidx(cC.nx + 1 + l, j, k)] = f[hidx(1 + l, j, k)];
+    f[hidx(1 - L + l, j, k)] = f[hidx(cC.nx + 1 - L + l, j, k)];
+  }
+  if ((a.dirmask & 2) && cC.iper[1] && t < nyz) {
+    int i = (int)(t % cC.nx) + 1, l = (int)((t / cC.nx) % L), k = (int)(t / cC.nx / L) + 1;
+    f[hidx(i, cC.ny + 1 + l, k)] = f[hidx(i, 1 + l, k)];
+    f[hidx(i, 1 - L + l, k)] = f[hidx(i, cC.ny + 1 - L + l, k)];
+  }
+  if ((a.dirmask & 4) && cC.iper[2] && t < nzz) {
+    int i = (int)(t % cC.nx) + 1, j = (int)((t / cC.nx) % cC.ny) + 1, l = (int)(t / cC.nx / cC.ny);
+    f[hidx(i, j, cC.nz + 1 + l)] = f[hidx(i, j, 1 + l)];
+    f[hidx(i, j, 1 - L + l)] = f[hidx(i, j, cC.nz + 1 - L + l)];
+  }
+}
+
+static __global__ void k_copy(const double* src, double* dst, long long n) {
+  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < n) dst[t] = src[t];
+}
+
+// comput_Rhybrid, shock sensor 1 (OCFD_SetHybrid.f90:34-43) and forced patches (:80-102)
+static __global__ void k_sensor1(const double* p, double* Rh, int npatch, const int* patches) {
+  int i, j, k;
+  if (!cell_of((long long)blockIdx.x * blockDim.x + threadIdx.x, i, j, k)) return;
+  const int q = hidx(i, j, k), sy = cC.HX, sz = cC.HX * cC.HY;
+  double r = fabs((p[q - 1] - 2.0 * p[q] + p[q + 1]) / (p[q - 1] + 2.0 * p[q] + p[q + 1])) +
+             fabs((p[q - sy] - 2.0 * p[q] + p[q + sy]) / (p[q - sy] + 2.0 * p[q] + p[q + sy])) +
+             fabs((p[q - sz] - 2.0 * p[q] + p[q + sz]) / (p[q - sz] + 2.0 * p[q] + p[q + sz]));
+  for (int m = 0; m < npatch; m++) {
+    const int* b = patches + 6 * m;
+    if (i >= b[0] && i <= b[1] && j >= b[2] && j <= b[3] && k >= b[4] && k <= b[5]) r = r + 100.0;
+  }
+  Rh[q] = r;
+}
+// sensor 2 (|grad p| / mean): gradient magnitude, then scaled by the host-reduced mean
+template <bool SEP>
+__global__ void k_sensor2(const double* p, double* Rh, double* partial, Geo g) {
+  int i, j, k;
+  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  double r = 0.0;
+  if (cell_of(t, i, j, k)) {
+    const int q = hidx(i, j, k);
+    double pk = cdiff(p, q, 0, i, cC.nx), pi = cdiff(p, q, 1, j, cC.ny), ps = cdiff(p, q, 2, k, cC.nz);
+    double A[9], A1[9];
+    metric_all<SEP>(g, i, j, k, q, A, A1);
+    double px = pk * A[0] + pi * A[3] + ps * A[6];
+    double py = pk * A[1] + pi * A[4] + ps * A[7];
+    double pz = pk * A[2] + pi * A[5] + ps * A[8];
+    r = sqrt(px * px + py * py + pz * pz);
+    Rh[q] = r;
+  }
+  // deterministic block partial sums (fixed tree order)
+  __shared__ double sh[256];
+  sh[threadIdx.x] = r;
+  __syncthreads();
+  for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+    if (threadIdx.x < s) sh[threadIdx.x] = sh[threadIdx.x] + sh[threadIdx.x + s];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) partial[blockIdx.x] = sh[0];
+}
+static __global__ void k_sensor2_scale(double* Rh, const double* partial, int nblk, int npatch, const int* patches) {
+  // every block re-derives the same total in the same order (deterministic)
+  __shared__ double tot;
+  if (threadIdx.x == 0) {
+    double s = 0.0;
+    for (int b = 0; b < nblk; b++) s = s + partial[b];
+    double dp_av = s / (1.0 * cC.nx * cC.ny * cC.nz);
+    tot = 1.0 / (dp_av + 1.0e-30);
+  }
+  __syncthreads();
+  int i, j, k;
+  if (!cell_of((long long)blockIdx.x * blockDim.x + threadIdx.x, i, j, k)) return;
+  const int q = hidx(i, j, k);
+  double r = Rh[q] * tot;
+  for (int m = 0; m < npatch; m++) {
+    const int* b = patches + 6 * m;
+    if (i >= b[0] && i <= b[1] && j >= b[2] && j <= b[3] && k >= b[4] && k <= b[5]) r = r + 100.0;
+  }
+  Rh[q] = r;
+}
+
+// ---------------------------------------------------------------- RK3 + primitive variables
+struct PrimArgs {
+  double* f;
+  const double *fn, *du;
+  double *d, *u, *v, *w, *T, *p, *Et;  // Et = buffer written this stage
+  double* di;
+  DevStatus* st;
+  int krk;  // 1..3 RK stage; 0 = no update (start-up conversion only)
+  double dt;
+};
+template <int NS>
+__global__ void __launch_bounds__(256) k_rk_prims(PrimArgs a) {
+  int i, j, k;
+  if (!cell_of((long long)blockIdx.x * blockDim.x + threadIdx.x, i, j, k)) return;
+  const int q = hidx(i, j, k), nn = nidx(i, j, k);
+  const long long N = cC.N;
+  const double ra[3] = {0.0, 3.0 / 4.0, 1.0 / 3.0}, rb[3] = {1.0, 1.0 / 4.0, 2.0 / 3.0};
+  double f[5];
+#pragma unroll
+  for (int m = 0; m < 5; m++) {
+    size_t o = (size_t)m * N + nn;
+    if (a.krk == 1) f[m] = a.fn[o] + a.dt * a.du[o];
+    else if (a.krk > 1) f[m] = ra[a.krk - 1] * a.fn[o] + rb[a.krk - 1] * (a.f[o] + a.dt * a.du[o]);
+    else f[m] = a.f[o];
+    a.f[o] = f[m];
+  }
+  double dd = f[0];
+  double uu = f[1] / f[0], vv = f[2] / f[0], ww = f[3] / f[0];
+  double et = f[4] - (f[1] * uu + f[2] * vv + f[3] * ww) * 0.5;
+  a.d[q] = dd; a.u[q] = uu; a.v[q] = vv; a.w[q] = ww;
+  a.Et[q] = et;
+  if (!(et > 0.0)) {
+    if (et <= 0.0) {
+      int slot = atomicAdd(&a.st->neg_count, 1);
+      if (slot < 16) a.st->neg_list[slot] = nn;
+    } else {
+      atomicAdd(&a.st->nan_count, 1);
+    }
+  }
+  // Rescaling_di: di >= 0 and sum(di) = d
+  double di0[NS];
+  double d0 = 0.0;
+#pragma unroll
+  for (int m = 0; m < NS; m++) {
+    double x = a.di[(size_t)m * cC.H + q];
+    if (x < 0.0) x = 0.0;
+    di0[m] = x;
+    d0 = d0 + x;
+  }
+  double tmp = dd / d0;
+#pragma unroll
+  for (int m = 0; m < NS; m++) {
+    di0[m] = di0[m] * tmp;
+    a.di[(size_t)m * cC.H + q] = di0[m];
+  }
+  double TT = dev_T<NS>(di0, et, &a.st->newton_fail);
+  a.T[q] = TT;
+  a.p[q] = dev_P<NS>(di0, TT);
+}
+
+// handle_NegativeEt replayed in loop order: a repaired cell averages its six neighbours, taking
+// this pass's value for interior neighbours earlier in (i,j,k) order and the previous value
+// (other Et buffer) for later ones and for halo points. More than 10 such cells stop the run.
+template <int NS>
+__global__ void k_repair_et(double* f, double* Et_new, const double* Et_old, double* T, double* p, const double* di,
+                            DevStatus* st) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  int cnt = st->neg_count;
+  if (cnt == 0) return;
+  st->neg_total += (unsigned long long)cnt;
+  if (cnt > 10) {
+    st->error = OCFD_ERR_NEGATIVE_ET;
+    st->neg_count = 0;
+    return;
+  }
+  int lst[16];
+  for (int m = 0; m < cnt; m++) lst[m] = st->neg_list[m];
+  for (int a = 1; a < cnt; a++)  // insertion sort into loop order
+    for (int b = a; b > 0 && lst[b - 1] > lst[b]; b--) { int t = lst[b]; lst[b] = lst[b - 1]; lst[b - 1] = t; }
+  for (int m = 0; m < cnt; m++) {
+    int nn = lst[m];
+    int i = nn % cC.nx + 1, j = (nn / cC.nx) % cC.ny + 1, k = nn / cC.nx / cC.ny + 1;
+    auto nb = [&](int ii, int jj, int kk) {
+      bool inside = ii >= 1 && ii <= cC.nx && jj >= 1 && jj <= cC.ny && kk >= 1 && kk <= cC.nz;
+      int qq = hidx(ii, jj, kk);
+      if (inside && nidx(ii, jj, kk) < nn) return Et_new[qq];
+      return Et_old[qq];
+    };
+    int q = hidx(i, j, k);
+    double e0 = Et_new[q];
+    double e1 = (nb(i + 1, j, k) + nb(i - 1, j, k) + nb(i, j + 1, k) + nb(i, j - 1, k) + nb(i, j, k + 1) +
+                 nb(i, j, k - 1)) /
+                6.0;
+    Et_new[q] = e1;
+    f[4 * cC.N + nn] = f[4 * cC.N + nn] + (e1 - e0);
+    double d0[NS];
+    for (int s = 0; s < NS; s++) d0[s] = di[(size_t)s * cC.H + q];
+    double TT = dev_T<NS>(d0, e1, &st->newton_fail);
+    T[q] = TT;
+    p[q] = dev_P<NS>(d0, TT);
+  }
+  st->neg_count = 0;
+}
+
+// ---------------------------------------------------------------- boundary conditions
+struct BcArgs {
+  double *f, *d, *u, *v, *w, *T, *p, *Et, *di;
+  const double *inlet, *upper, *wall_pertb;
+  const int* nonref;
+  int inlet_kind, upper_kind, outlet;
+  double ht, Tw, xinit, disA;
+  const double* X;  // Axx (halo array) for the wall start
+  Geo g;
+};
+
+template <int NS>
+__device__ __forceinline__ void set_point(const BcArgs& a, int q, const double* vals) {
+  a.d[q] = vals[0]; a.u[q] = vals[1]; a.v[q] = vals[2]; a.w[q] = vals[3]; a.T[q] = vals[4];
+#pragma unroll
+  for (int m = 0; m < NS; m++) a.di[(size_t)m * cC.H + q] = vals[5 + m];
+}
+// inlet i = 1 (OCFD_BC_Boundarylayers.f90:60-104)
+template <int NS>
+__global__ void k_bc_inlet(BcArgs a) {
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= cC.ny * cC.nz) return;
+  int j = t % cC.ny + 1, k = t / cC.ny + 1;
+  double vals[5 + NS];
+  for (int c = 0; c < 5 + NS; c++) {
+    if (a.inlet_kind == 0) vals[c] = a.inlet[c];
+    else if (a.inlet_kind == 1) vals[c] = a.inlet[c * cC.ny + (j - 1)];
+    else vals[c] = a.inlet[((size_t)c * cC.nz + (k - 1)) * cC.ny + (j - 1)];
+  }
+  set_point<NS>(a, hidx(1, j, k), vals);
+}
+// upper j = ny where the point is Dirichlet (:107-144)
+template <int NS>
+__global__ void k_bc_upper(BcArgs a) {
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= cC.nx * cC.nz) return;
+  int i = t % cC.nx + 1, k = t / cC.nx + 1;
+  if (a.nonref[t] != 0) return;
+  double vals[5 + NS];
+  for (int c = 0; c < 5 + NS; c++) {
+    if (a.upper_kind == 0) vals[c] = a.upper[c];
+    else if (a.upper_kind == 1) vals[c] = a.upper[c * cC.nx + (i - 1)];
+    else vals[c] = a.upper[((size_t)c * cC.nz + (k - 1)) * cC.nx + (i - 1)];
+  }
+  set_point<NS>(a, hidx(i, cC.ny, k), vals);
+}
+// wall j = 1: blowing/suction, isothermal or adiabatic, dp/dy = 0, non-catalytic (:147-201)
+template <int NS, bool SEP>
+__global__ void k_bc_wall(BcArgs a, const double* ht) {
+  a.ht = *ht;  // h(t) lives in device memory so that a captured graph sees each step's value
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= cC.nx * cC.nz) return;
+  int i = t % cC.nx + 1, k = t / cC.nx + 1;
+  int q1 = hidx(i, 1, k), q2 = hidx(i, 2, k), q3 = hidx(i, 3, k);
+  if (a.X[q1] < a.xinit) {
+    a.d[q1] = a.d[q2]; a.u[q1] = a.u[q2]; a.v[q1] = a.v[q2]; a.w[q1] = a.w[q2]; a.T[q1] = a.T[q2];
+    for (int m = 0; m < NS; m++) a.di[(size_t)m * cC.H + q1] = a.di[(size_t)m * cC.H + q2];
+    return;
+  }
+  double A[9], A1[9];
+  metric_all<SEP>(a.g, i, 1, k, q1, A, A1);
+  double Aix = A[3], Aiy = A[4], Aiz = A[5];
+  double tmp = 1.0 / sqrt(Aix * Aix + Aiy * Aiy + Aiz * Aiz);
+  double A0 = a.disA * a.ht * a.wall_pertb[t];
+  a.u[q1] = A0 * Aix * tmp;
+  a.v[q1] = A0 * Aiy * tmp;
+  a.w[q1] = A0 * Aiz * tmp;
+  double T1 = a.Tw > 0 ? a.Tw : (4.0 * a.T[q2] - a.T[q3]) / 3.0;
+  a.T[q1] = T1;
+  double di2[NS], di3[NS], di1[NS];
+  for (int m = 0; m < NS; m++) {
+    di2[m] = a.di[(size_t)m * cC.H + q2];
+    di3[m] = a.di[(size_t)m * cC.H + q3];
+  }
+  double p2 = dev_P<NS>(di2, a.T[q2]);
+  double p3 = dev_P<NS>(di3, a.T[q3]);
+  double p1 = (4.0 * p2 - p3) / 3.0;
+  double d2 = a.d[q2];
+  for (int m = 0; m < NS; m++) di1[m] = di2[m] / d2;
+  double d1 = dev_dens<NS>(di1, T1, p1);
+  a.d[q1] = d1;
+  for (int m = 0; m < NS; m++) a.di[(size_t)m * cC.H + q1] = di1[m] * d1;
+}
+// outlet i = nx, first / second order extrapolation (:203-231)
+template <int NS>
+__global__ void k_bc_outlet(BcArgs a) {
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= cC.ny * cC.nz) return;
+  int j = t % cC.ny + 1, k = t / cC.ny + 1;
+  int q = hidx(cC.nx, j, k), q1 = hidx(cC.nx - 1, j, k), q2 = hidx(cC.nx - 2, j, k);
+  if (a.outlet == 1) {
+    a.d[q] = a.d[q1]; a.u[q] = a.u[q1]; a.v[q] = a.v[q1]; a.w[q] = a.w[q1]; a.T[q] = a.T[q1];
+    for (int m = 0; m < NS; m++) a.di[(size_t)m * cC.H + q] = a.di[(size_t)m * cC.H + q1];
+  } else {
+    a.d[q] = 2.0 * a.d[q1] - a.d[q2]; a.u[q] = 2.0 * a.u[q1] - a.u[q2]; a.v[q] = 2.0 * a.v[q1] - a.v[q2];
+    a.w[q] = 2.0 * a.w[q1] - a.w[q2]; a.T[q] = 2.0 * a.T[q1] - a.T[q2];
+    for (int m = 0; m < NS; m++)
+      a.di[(size_t)m * cC.H + q] = 2.0 * a.di[(size_t)m * cC.H + q1] - a.di[(size_t)m * cC.H + q2];
+  }
+}
+// OCFD_bc lines 33-184: every domain-face cell gets di re-scaled, Et and p re-derived from T and
+// f rebuilt, once per face it lies on (edges twice, corners three times, as the sequential face
+// loops of the reference do). group 0: i faces; 1: j faces without i faces; 2: k faces only.
+template <int NS>
+__device__ __forceinline__ void face_apply(const BcArgs& a, int i, int j, int k, int times) {
+  const int q = hidx(i, j, k), nn = nidx(i, j, k);
+  const long long N = cC.N;
+  double dd = a.d[q], uu = a.u[q], vv = a.v[q], ww = a.w[q], TT = a.T[q];
+  double di1[NS];
+  for (int m = 0; m < NS; m++) di1[m] = a.di[(size_t)m * cC.H + q];
+  double et = 0.0, pp = 0.0;
+  for (int r = 0; r < times; r++) {
+    double d0 = 0.0;
+    for (int m = 0; m < NS; m++) d0 = d0 + di1[m];
+    double dtmp = dd / d0;
+    for (int m = 0; m < NS; m++) di1[m] = di1[m] * dtmp;
+    et = dev_E<NS>(di1, TT);
+    pp = dev_P<NS>(di1, TT);
+  }
+  for (int m = 0; m < NS; m++) a.di[(size_t)m * cC.H + q] = di1[m];
+  a.Et[q] = et;
+  a.p[q] = pp;
+  a.f[nn] = dd;
+  a.f[N + nn] = dd * uu;
+  a.f[2 * N + nn] = dd * vv;
+  a.f[3 * N + nn] = dd * ww;
+  a.f[4 * N + nn] = et + dd * (uu * uu + vv * vv + ww * ww) * 0.5;
+}
+template <int NS>
+__global__ void k_bc_faces(BcArgs a, int group) {
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int nx = cC.nx, ny = cC.ny, nz = cC.nz;
+  int i, j, k;
+  if (group == 0) {
+    if (t >= 2 * ny * nz) return;
+    i = (t & 1) ? nx : 1;
+    int r = t >> 1;
+    j = r % ny + 1;
+    k = r / ny + 1;
+  } else if (group == 1) {
+    if (t >= 2 * (nx - 2) * nz) return;
+    j = (t & 1) ? ny : 1;
+    int r = t >> 1;
+    i = r % (nx - 2) + 2;
+    k = r / (nx - 2) + 1;
+  } else {
+    if (t >= 2 * (nx - 2) * (ny - 2)) return;
+    k = (t & 1) ? nz : 1;
+    int r = t >> 1;
+    i = r % (nx - 2) + 2;
+    j = r / (nx - 2) + 2;
+  }
+  int times = (i == 1) + (i == nx) + (j == 1) + (j == ny) + (k == 1) + (k == nz);
+  face_apply<NS>(a, i, j, k, times);
+}
+// Flow_Ghost_Extent_2nd (OCFD_GhostCell.f90:166-364): face halos of faces with Ghost_Cell = 1/2
+template <int NS>
+__global__ void k_bc_ghost(BcArgs a, int face) {
+  const int dir = face / 2, side = face % 2;
+  const int n = dir == 0 ? cC.nx : (dir == 1 ? cC.ny : cC.nz);
+  const int na = dir == 0 ? cC.ny : cC.nx, nb = dir == 2 ? cC.ny : cC.nz;
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= na * nb * OCFD_L) return;
+  int aa = t % na + 1, l = (t / na) % OCFD_L + 1, bb = t / na / OCFD_L + 1;
+  int ig = side == 0 ? 1 - l : n + l, ib = side == 0 ? 1 : n, im = side == 0 ? 2 - ig : 2 * n - ig;
+  auto at = [&](int s) {
+    if (dir == 0) return hidx(s, aa, bb);
+    if (dir == 1) return hidx(aa, s, bb);
+    return hidx(aa, bb, s);
+  };
+  int qg = at(ig), qb = at(ib), qm = at(im);
+  const double s1 = 0.8, s2 = 1.2;
+  a.u[qg] = 2.0 * a.u[qb] - a.u[qm]; a.v[qg] = 2.0 * a.v[qb] - a.v[qm]; a.w[qg] = 2.0 * a.w[qb] - a.w[qm];
+  double dg = 2.0 * a.d[qb] - a.d[qm], Tg = 2.0 * a.T[qb] - a.T[qm];
+  if (dg < s1 * a.d[qb]) dg = s1 * a.d[qb];
+  if (dg > s2 * a.d[qb]) dg = s2 * a.d[qb];
+  if (Tg < s1 * a.T[qb]) Tg = s1 * a.T[qb];
+  if (Tg > s2 * a.T[qb]) Tg = s2 * a.T[qb];
+  a.d[qg] = dg;
+  a.T[qg] = Tg;
+  double di1[NS], d0 = 0.0;
+  for (int m = 0; m < NS; m++) {
+    di1[m] = 2.0 * a.di[(size_t)m * cC.H + qb] - a.di[(size_t)m * cC.H + qm];
+    d0 = d0 + di1[m];
+  }
+  double dtmp = dg / d0;
+  for (int m = 0; m < NS; m++) {
+    di1[m] = di1[m] * dtmp;
+    a.di[(size_t)m * cC.H + qg] = di1[m];
+  }
+  a.Et[qg] = dev_E<NS>(di1, Tg);
+  a.p[qg] = dev_P<NS>(di1, Tg);
+}
+
+// start-up: d,u,v,w,T,di from primitive input, Rescaling_di, conserved f (OCFD_init.f90:8-25)
+template <int NS>
+__global__ void k_init_state(const double* prim5, const double* din, double* f, double* d, double* u, double* v,
+                             double* w, double* T, double* di) {
+  int i, j, k;
+  if (!cell_of((long long)blockIdx.x * blockDim.x + threadIdx.x, i, j, k)) return;
+  const int q = hidx(i, j, k), nn = nidx(i, j, k);
+  const long long N = cC.N;
+  double dd = prim5[nn], uu = prim5[N + nn], vv = prim5[2 * N + nn], ww = prim5[3 * N + nn], TT = prim5[4 * N + nn];
+  d[q] = dd; u[q] = uu; v[q] = vv; w[q] = ww; T[q] = TT;
+  double di1[NS], d0 = 0.0;
+  for (int m = 0; m < NS; m++) {
+    double x = din[(size_t)m * N + nn];
+    if (x < 0.0) x = 0.0;
+    di1[m] = x;
+    d0 = d0 + x;
+  }
+  double tmp = dd / d0;
+  for (int m = 0; m < NS; m++) {
+    di1[m] = di1[m] * tmp;
+    di[(size_t)m * cC.H + q] = di1[m];
+  }
+  f[nn] = dd;
+  f[N + nn] = dd * uu;
+  f[2 * N + nn] = dd * vv;
+  f[3 * N + nn] = dd * ww;
+  double et1 = dev_E<NS>(di1, TT);
+  f[4 * N + nn] = et1 + dd * (uu * uu + vv * vv + ww * ww) * 0.5;
+}
+
+// show_flow_msg sums with a fixed reduction tree (two passes, deterministic)
+template <bool SEP>
+__global__ void k_diag(const double* f, const double* d, const double* u, const double* v, const double* w,
+                       double* partial, Geo g) {
+  __shared__ double s1[256], s2[256];
+  int i, j, k;
+  double e = 0.0, kk = 0.0;
+  if (cell_of((long long)blockIdx.x * blockDim.x + threadIdx.x, i, j, k)) {
+    const int q = hidx(i, j, k), nn = nidx(i, j, k);
+    double tmp0 = 1.0 / metric_jac<SEP>(g, i, j, k, q);
+    e = f[4 * cC.N + nn] * tmp0;
+    kk = d[q] * (u[q] * u[q] + v[q] * v[q] + w[q] * w[q]) * 0.5 * tmp0;
+  }
+  s1[threadIdx.x] = e;
+  s2[threadIdx.x] = kk;
+  __syncthreads();
+  for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+    if (threadIdx.x < s) {
+      s1[threadIdx.x] = s1[threadIdx.x] + s1[threadIdx.x + s];
+      s2[threadIdx.x] = s2[threadIdx.x] + s2[threadIdx.x + s];
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    partial[2 * blockIdx.x] = s1[0];
+    partial[2 * blockIdx.x + 1] = s2[0];
+  }
+}
+
+}  // namespace ocfd

@@ -1,0 +1,1320 @@
+// libocfd_gpu.so -- C ABI of the B200 (sm_100a) OpenCFD-Comb hot path (include/ocfd_gpu.h).
+//
+// Host side: parameter derivation (set_parameters, OCFD_readpara.f90:347-431), one device arena,
+// the per-stage launch sequence of flow_time_advance (OCFD_Time_Adv.f90:7-92), Strang step
+// capture into a CUDA graph, status words read back after every call, per-kernel event timing.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#define OCFD_DEFINE_CONST
+#include "ocfd_chem.cuh"
+#include "ocfd_device.cuh"
+#include "ocfd_flow.cuh"
+#include "ocfd_launch.h"
+
+using namespace ocfd;
+
+namespace {
+
+std::string g_err;
+
+struct CudaError : std::runtime_error {
+  int code;
+  CudaError(const std::string& s, int c) : std::runtime_error(s), code(c) {}
+};
+#define CK(x)                                                                                      \
+  do {                                                                                             \
+    cudaError_t e_ = (x);                                                                          \
+    if (e_ != cudaSuccess)                                                                         \
+      throw CudaError(std::string(#x) + ": " + cudaGetErrorString(e_), OCFD_ERR_CUDA);             \
+  } while (0)
+#define LAUNCH_CHECK() CK(cudaGetLastError())
+
+// kernel classes for event timing
+enum KClass { KC_FLUX_X = 0, KC_FLUX_Y, KC_FLUX_Z, KC_VISC_EV, KC_VISC_DIV, KC_RK_PRIMS, KC_EXCH, KC_BC, KC_SENSOR,
+              KC_SPECIES, KC_CHEM, KC_OTHER, KC_NUM };
+const char* kc_names[KC_NUM] = {"flux_x", "flux_y", "flux_z", "visc_ev", "visc_div", "rk_prims", "exchange",
+                                "bc", "sensor", "species", "chem", "other"};
+
+struct Lib {
+  ocfd_params P{};
+  DevConst hc{};
+  int NS = 1;
+  bool sep = false, have_kin = false, flow_ready = false;
+  cudaStream_t st = nullptr;
+  char* arena = nullptr;
+  size_t arena_size = 0, arena_used = 0;
+  double *f = nullptr, *fn = nullptr, *du = nullptr, *d = nullptr, *u = nullptr, *v = nullptr, *w = nullptr,
+         *T = nullptr, *p = nullptr, *Et[2] = {nullptr, nullptr}, *di = nullptr, *din = nullptr, *Rh = nullptr;
+  double *ev[12] = {}, *amu = nullptr, *amk = nullptr, *amd = nullptr, *qp[3] = {}, *ci = nullptr, *se[3] = {};
+  double *X = nullptr, *Y = nullptr, *Z = nullptr, *met[19] = {}, *d1[3] = {}, *partial = nullptr;
+  double *inlet = nullptr, *upper = nullptr, *wall = nullptr, *ht_dev = nullptr;
+  int *nonref = nullptr, *patches = nullptr;
+  int npatch = 0;
+  double** ev_ptrs = nullptr;
+  DevStatus* sdev = nullptr;
+  DevStatus* shost = nullptr;
+  double* ht_host = nullptr;
+  int cur = 0;  // which Et buffer is current
+  Geo geo{};
+  int inlet_kind = 0, upper_kind = 0, outlet = 0;
+  std::vector<double> tm, fait;
+  // graph of one Strang step
+  cudaGraphExec_t gexec = nullptr;
+  double g_dt = 0;
+  int g_ifr = -1, g_nsub = -1, g_par = -1, g_launches = 0;
+  // batched chemistry scratch
+  double *b_di = nullptr, *b_e = nullptr, *b_dt = nullptr;
+  int *b_nsub = nullptr, *b_perm = nullptr, *b_hist = nullptr, *b_counter = nullptr, *b_nfail = nullptr;
+  size_t b_cap = 0;
+  // profiling
+  bool prof = false;
+  double kc_ms[KC_NUM] = {};
+  long long kc_n[KC_NUM] = {};
+  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev_pool;
+  std::vector<std::pair<int, int>> ev_pending;  // (class, pool index)
+  long long launches = 0;
+  // bench support
+  cudaEvent_t uev[16] = {};
+  double* ht_seq = nullptr;
+  double* ht_seq_host = nullptr;
+  int ht_cap = 0;
+};
+Lib* L = nullptr;
+
+template <class T>
+T* alloc(size_t n) {
+  size_t bytes = (n * sizeof(T) + 255) & ~(size_t)255;
+  if (L->arena_used + bytes > L->arena_size) throw std::runtime_error("device arena exhausted");
+  T* p = reinterpret_cast<T*>(L->arena + L->arena_used);
+  L->arena_used += bytes;
+  return p;
+}
+
+// ---------------------------------------------------------------- launch helpers
+struct KTimer {
+  int cls;
+  int idx = -1;
+  KTimer(int c) : cls(c) {
+    L->launches++;
+    if (!L->prof) return;
+    if (L->ev_pending.size() >= L->ev_pool.size()) {
+      cudaEvent_t a, b;
+      CK(cudaEventCreate(&a));
+      CK(cudaEventCreate(&b));
+      L->ev_pool.push_back({a, b});
+    }
+    idx = (int)L->ev_pending.size();
+    CK(cudaEventRecord(L->ev_pool[idx].first, L->st));
+  }
+  ~KTimer() noexcept(false) {
+    if (idx < 0) return;
+    CK(cudaEventRecord(L->ev_pool[idx].second, L->st));
+    L->ev_pending.push_back({cls, idx});
+  }
+};
+void prof_collect() {
+  if (L->ev_pending.empty()) return;
+  CK(cudaStreamSynchronize(L->st));
+  for (auto& pr : L->ev_pending) {
+    float ms = 0;
+    CK(cudaEventElapsedTime(&ms, L->ev_pool[pr.second].first, L->ev_pool[pr.second].second));
+    L->kc_ms[pr.first] += ms;
+    L->kc_n[pr.first] += 1;
+  }
+  L->ev_pending.clear();
+}
+
+inline unsigned nblk(long long n, int b) { return (unsigned)((n + b - 1) / b); }
+
+void exchange(std::initializer_list<double*> fields, int dirmask) {
+  ExchArgs a{};
+  a.nf = 0;
+  for (double* f : fields) a.f[a.nf++] = f;
+  a.dirmask = dirmask;
+  bool any = false;
+  for (int dd = 0; dd < 3; dd++)
+    if ((dirmask >> dd & 1) && L->P.iperiodic[dd]) any = true;
+  if (!any || a.nf == 0) return;
+  const int nx = L->P.nx, ny = L->P.ny, nz = L->P.nz;
+  long long mx = std::max((long long)ny * nz, std::max((long long)nx * nz, (long long)nx * ny)) * OCFD_L;
+  KTimer t(KC_EXCH);
+  k_exchange<<<dim3(nblk(mx, 256), a.nf), 256, 0, L->st>>>(a);
+  LAUNCH_CHECK();
+}
+void exchange_v(const std::vector<double*>& fields, int dirmask) {
+  for (size_t s = 0; s < fields.size(); s += 24) {
+    ExchArgs a{};
+    a.nf = 0;
+    for (size_t m = s; m < fields.size() && m < s + 24; m++) a.f[a.nf++] = fields[m];
+    a.dirmask = dirmask;
+    const int nx = L->P.nx, ny = L->P.ny, nz = L->P.nz;
+    long long mx = std::max((long long)ny * nz, std::max((long long)nx * nz, (long long)nx * ny)) * OCFD_L;
+    KTimer t(KC_EXCH);
+    k_exchange<<<dim3(nblk(mx, 256), a.nf), 256, 0, L->st>>>(a);
+    LAUNCH_CHECK();
+  }
+}
+
+// ---- flux dispatch (kernels compiled in ocfd_flux_{x,y,z}.cu) ----
+void launch_flux(int dir, const FluxArgs& a, bool scalar) {
+  KTimer t(scalar ? KC_SPECIES : KC_FLUX_X + dir);
+  const ocfd_params& P = L->P;
+  if (dir == 0) launch_flux_x(P.scheme_invis, P.flux_splitting, L->sep, scalar, a, P.nx, P.ny, P.nz, L->st);
+  else if (dir == 1) launch_flux_y(P.scheme_invis, P.flux_splitting, L->sep, scalar, a, P.nx, P.ny, P.nz, L->st);
+  else launch_flux_z(P.scheme_invis, P.flux_splitting, L->sep, scalar, a, P.nx, P.ny, P.nz, L->st);
+  LAUNCH_CHECK();
+}
+
+// NS dispatch for the species-templated kernels (N_SPEC 1, 2 and 9 always; 3..8 unless
+// OCFD_FEW_SPECIES is defined, which shortens development builds)
+#ifdef OCFD_FEW_SPECIES
+#define NS_MORE(...)
+#else
+#define NS_MORE(...)                                               \
+    case 3: { constexpr int NSV = 3; __VA_ARGS__; } break;          \
+    case 4: { constexpr int NSV = 4; __VA_ARGS__; } break;          \
+    case 5: { constexpr int NSV = 5; __VA_ARGS__; } break;          \
+    case 6: { constexpr int NSV = 6; __VA_ARGS__; } break;          \
+    case 7: { constexpr int NSV = 7; __VA_ARGS__; } break;          \
+    case 8: { constexpr int NSV = 8; __VA_ARGS__; } break;
+#endif
+#define NS_DISPATCH(ns, ...)                                  \
+  switch (ns) {                                                \
+    case 1: { constexpr int NSV = 1; __VA_ARGS__; } break;            \
+    case 2: { constexpr int NSV = 2; __VA_ARGS__; } break;            \
+    NS_MORE(__VA_ARGS__)                                       \
+    case 9: { constexpr int NSV = 9; __VA_ARGS__; } break;            \
+    default: throw std::runtime_error("N_SPEC must be 1..9"); \
+  }
+
+// ---------------------------------------------------------------- stages
+BcArgs bc_args() {
+  BcArgs a{};
+  a.f = L->f; a.d = L->d; a.u = L->u; a.v = L->v; a.w = L->w; a.T = L->T; a.p = L->p; a.Et = L->Et[L->cur];
+  a.di = L->di;
+  a.inlet = L->inlet; a.upper = L->upper; a.wall_pertb = L->wall; a.nonref = L->nonref;
+  a.inlet_kind = L->inlet_kind; a.upper_kind = L->upper_kind; a.outlet = L->outlet;
+  a.Tw = L->P.bc_para[4]; a.xinit = L->P.bc_para[5]; a.disA = L->P.bc_para[7];
+  a.ht = 0.0;
+  a.X = L->X;
+  a.g = L->geo;
+  return a;
+}
+
+template <int NS>
+void ocfd_bc_t() {
+  BcArgs a = bc_args();
+  const int nx = L->P.nx, ny = L->P.ny, nz = L->P.nz;
+  if (L->P.ibc == OCFD_BC_BOUNDARYLAYER) {
+    KTimer t(KC_BC);
+    k_bc_inlet<NS><<<nblk((long long)ny * nz, 128), 128, 0, L->st>>>(a);
+    LAUNCH_CHECK();
+    if (L->upper_kind >= 0) {
+      k_bc_upper<NS><<<nblk((long long)nx * nz, 128), 128, 0, L->st>>>(a);
+      LAUNCH_CHECK();
+    }
+  }
+  if (L->P.ibc == OCFD_BC_BOUNDARYLAYER) {
+    KTimer t(KC_BC);
+    // the wall disturbance amplitude h(t) is read from device memory so that a captured graph
+    // picks up the current step's value
+    a.ht = 0.0;
+    if (L->sep) k_bc_wall<NS, true><<<nblk((long long)nx * nz, 128), 128, 0, L->st>>>(a, L->ht_dev);
+    else k_bc_wall<NS, false><<<nblk((long long)nx * nz, 128), 128, 0, L->st>>>(a, L->ht_dev);
+    LAUNCH_CHECK();
+    if (L->outlet == 1 || L->outlet == 2) {
+      k_bc_outlet<NS><<<nblk((long long)ny * nz, 128), 128, 0, L->st>>>(a);
+      LAUNCH_CHECK();
+    }
+  }
+  {
+    KTimer t(KC_BC);
+    k_bc_faces<NS><<<nblk(2LL * ny * nz, 128), 128, 0, L->st>>>(a, 0);
+    LAUNCH_CHECK();
+    k_bc_faces<NS><<<nblk(2LL * (nx - 2) * nz, 128), 128, 0, L->st>>>(a, 1);
+    LAUNCH_CHECK();
+    k_bc_faces<NS><<<nblk(2LL * (nx - 2) * (ny - 2), 128), 128, 0, L->st>>>(a, 2);
+    LAUNCH_CHECK();
+  }
+  for (int face = 0; face < 6; face++) {
+    if (!(L->P.ghost_cell[face] == 1 || L->P.ghost_cell[face] == 2)) continue;
+    int dir = face / 2;
+    long long na = dir == 0 ? ny : nx, nb = dir == 2 ? ny : nz;
+    KTimer t(KC_BC);
+    k_bc_ghost<NS><<<nblk(na * nb * OCFD_L, 128), 128, 0, L->st>>>(a, face);
+    LAUNCH_CHECK();
+  }
+}
+
+template <int NS>
+void prims_t(int krk, double dt) {
+  PrimArgs a{};
+  a.f = L->f; a.fn = L->fn; a.du = L->du;
+  a.d = L->d; a.u = L->u; a.v = L->v; a.w = L->w; a.T = L->T; a.p = L->p;
+  a.Et = L->Et[1 - L->cur];
+  a.di = L->di;
+  a.st = L->sdev;
+  a.krk = krk;
+  a.dt = dt;
+  {
+    KTimer t(KC_RK_PRIMS);
+    k_rk_prims<NS><<<nblk(L->hc.N, 256), 256, 0, L->st>>>(a);
+    LAUNCH_CHECK();
+  }
+  {
+    KTimer t(KC_OTHER);
+    k_repair_et<NS><<<1, 32, 0, L->st>>>(L->f, L->Et[1 - L->cur], L->Et[L->cur], L->T, L->p, L->di, L->sdev);
+    LAUNCH_CHECK();
+  }
+  L->cur = 1 - L->cur;
+}
+
+void sensor() {
+  int sensor = (int)std::lround(L->P.hybrid_para[0]);
+  long long N = L->hc.N;
+  KTimer t(KC_SENSOR);
+  if (sensor == 1) {
+    k_sensor1<<<nblk(N, 256), 256, 0, L->st>>>(L->p, L->Rh, L->npatch, L->patches);
+    LAUNCH_CHECK();
+  } else {
+    unsigned nb = nblk(N, 256);
+    if (L->sep) k_sensor2<true><<<nb, 256, 0, L->st>>>(L->p, L->Rh, L->partial, L->geo);
+    else k_sensor2<false><<<nb, 256, 0, L->st>>>(L->p, L->Rh, L->partial, L->geo);
+    LAUNCH_CHECK();
+    k_sensor2_scale<<<nb, 256, 0, L->st>>>(L->Rh, L->partial, (int)nb, L->npatch, L->patches);
+    LAUNCH_CHECK();
+  }
+}
+
+template <int NS>
+void stage_t(int krk, double dt1) {
+  const long long N = L->hc.N, H = L->hc.H;
+  double* Etc = L->Et[L->cur];
+  if (NS > 1) {
+    KTimer t(KC_SPECIES);
+    k_transport<NS><<<nblk(N, 128), 128, 0, L->st>>>(L->d, L->T, L->p, L->di, L->amu, L->amk, L->amd);
+    LAUNCH_CHECK();
+  }
+  {
+    std::vector<double*> fl = {L->d, L->u, L->v, L->w, L->T, L->p, Etc};
+    if (NS > 1)
+      for (int m = 0; m < NS; m++) fl.push_back(L->di + (size_t)m * H);
+    exchange_v(fl, 7);
+  }
+  if (NS == 1) {
+    KTimer t(KC_EXCH);
+    k_copy<<<nblk(H, 256), 256, 0, L->st>>>(L->d, L->di, H);
+    LAUNCH_CHECK();
+  }
+  if (krk == 1 && L->P.scheme_invis == OCFD_SCHEME_HYBRID) {
+    sensor();
+    exchange({L->Rh}, 7);
+  }
+  FluxArgs fa{};
+  fa.d = L->d; fa.u = L->u; fa.v = L->v; fa.w = L->w; fa.p = L->p; fa.Et = Etc; fa.Rh = L->Rh;
+  fa.g = L->geo;
+  if (NS > 1) {
+    for (int m = 0; m < NS; m++) {
+      double* fs = L->di + (size_t)m * H;
+      fa.fs = fs;
+      fa.out = L->du;
+      for (int dd = 0; dd < 3; dd++) launch_flux(dd, fa, true);
+      if (L->P.if_viscous == 1) {
+        KTimer t(KC_SPECIES);
+        k_ci<<<nblk(H, 256), 256, 0, L->st>>>(fs, L->d, L->ci, H);
+        LAUNCH_CHECK();
+        if (L->sep) k_scal_ev<true><<<nblk(N, 256), 256, 0, L->st>>>(m, L->ci, L->d, L->T, L->amd, L->qp[0], L->qp[1], L->qp[2], L->se[0], L->se[1], L->se[2], L->geo);
+        else k_scal_ev<false><<<nblk(N, 256), 256, 0, L->st>>>(m, L->ci, L->d, L->T, L->amd, L->qp[0], L->qp[1], L->qp[2], L->se[0], L->se[1], L->se[2], L->geo);
+        LAUNCH_CHECK();
+      }
+      if (L->P.if_viscous == 1) {
+        exchange({L->se[0]}, 1);
+        exchange({L->se[1]}, 2);
+        exchange({L->se[2]}, 4);
+        KTimer t(KC_SPECIES);
+        if (L->sep) k_scal_div<true><<<nblk(N, 256), 256, 0, L->st>>>(L->se[0], L->se[1], L->se[2], L->du, L->geo);
+        else k_scal_div<false><<<nblk(N, 256), 256, 0, L->st>>>(L->se[0], L->se[1], L->se[2], L->du, L->geo);
+        LAUNCH_CHECK();
+      }
+      {
+        KTimer t(KC_SPECIES);
+        k_scal_rk<<<nblk(N, 256), 256, 0, L->st>>>(krk, dt1, L->du, L->din + (size_t)m * N, fs);
+        LAUNCH_CHECK();
+      }
+    }
+  }
+  fa.fs = nullptr;
+  fa.out = L->du;
+  for (int dd = 0; dd < 3; dd++) launch_flux(dd, fa, false);
+  if (L->P.if_viscous == 1) {
+    ViscArgs va{};
+    va.d = L->d; va.u = L->u; va.v = L->v; va.w = L->w; va.T = L->T; va.di = L->di;
+    if (NS > 1) {
+      va.amu = L->amu; va.amk = L->amk;
+      va.qpx = L->qp[0]; va.qpy = L->qp[1]; va.qpz = L->qp[2];
+    }
+    for (int dd = 0; dd < 3; dd++)
+      for (int m = 0; m < 4; m++) va.ev[dd][m] = L->ev[4 * dd + m];
+    va.g = L->geo;
+    {
+      KTimer t(KC_VISC_EV);
+      if (L->sep) k_visc_ev<NS, true><<<nblk(N, 256), 256, 0, L->st>>>(va);
+      else k_visc_ev<NS, false><<<nblk(N, 256), 256, 0, L->st>>>(va);
+      LAUNCH_CHECK();
+    }
+    exchange({L->ev[0], L->ev[1], L->ev[2], L->ev[3]}, 1);
+    exchange({L->ev[4], L->ev[5], L->ev[6], L->ev[7]}, 2);
+    exchange({L->ev[8], L->ev[9], L->ev[10], L->ev[11]}, 4);
+    {
+      KTimer t(KC_VISC_DIV);
+      if (L->sep) k_visc_div<true><<<nblk(N, 256), 256, 0, L->st>>>(L->ev_ptrs, L->du, L->geo);
+      else k_visc_div<false><<<nblk(N, 256), 256, 0, L->st>>>(L->ev_ptrs, L->du, L->geo);
+      LAUNCH_CHECK();
+    }
+  }
+  prims_t<NS>(krk, dt1);
+  ocfd_bc_t<NS>();
+}
+
+template <int NS>
+void flow_advance_t(double dt1) {
+  const long long N = L->hc.N, H = L->hc.H;
+  CK(cudaMemcpyAsync(L->fn, L->f, sizeof(double) * 5 * N, cudaMemcpyDeviceToDevice, L->st));
+  if (NS > 1) {
+    // din <- di (interior only); a strided 3-D copy per species
+    for (int m = 0; m < NS; m++) {
+      cudaMemcpy3DParms cp{};
+      cp.srcPtr = make_cudaPitchedPtr(L->di + (size_t)m * H + (OCFD_L + L->hc.HX * (OCFD_L + (long long)L->hc.HY * OCFD_L)),
+                                      sizeof(double) * L->hc.HX, L->hc.HX, L->hc.HY);
+      cp.dstPtr = make_cudaPitchedPtr(L->din + (size_t)m * N, sizeof(double) * L->P.nx, L->P.nx, L->P.ny);
+      cp.extent = make_cudaExtent(sizeof(double) * L->P.nx, L->P.ny, L->P.nz);
+      cp.kind = cudaMemcpyDeviceToDevice;
+      CK(cudaMemcpy3DAsync(&cp, L->st));
+    }
+  }
+  for (int krk = 1; krk <= 3; krk++) stage_t<NS>(krk, dt1);
+}
+
+template <int NS>
+void chem_t(double dt2, int nsub) {
+  KTimer t(KC_CHEM);
+  launch_chem_cells(NS, L->hc.N, L->f, L->Et[L->cur], L->T, L->p, L->di, dt2, nsub, &L->sdev->newton_fail, L->st);
+  LAUNCH_CHECK();
+}
+
+double wall_ht(double tt) {
+  // get_ht_multifrequancy (OCFD_BC_Boundarylayers.f90:579-618), evaluated on the host
+  const double PI = 3.14159265358979;
+  double beta = L->P.bc_para[13];
+  if (!(beta > 0.0)) return 1.0;
+  double ht = 0.0;
+  for (size_t m = 0; m < L->tm.size(); m++) ht = ht + L->tm[m] * std::sin((m + 1) * beta * tt * 2.0 * PI + 2.0 * PI * L->fait[m]);
+  return ht;
+}
+
+void set_time(double tt) {
+  *L->ht_host = wall_ht(tt);
+  CK(cudaMemcpyAsync(L->ht_dev, L->ht_host, sizeof(double), cudaMemcpyHostToDevice, L->st));
+}
+
+int check_status() {
+  CK(cudaMemcpyAsync(L->shost, L->sdev, sizeof(DevStatus), cudaMemcpyDeviceToHost, L->st));
+  CK(cudaStreamSynchronize(L->st));
+  prof_collect();
+  if (L->shost->error) {
+    int e = L->shost->error;
+    CK(cudaMemsetAsync(&L->sdev->error, 0, sizeof(int), L->st));
+    g_err = e == OCFD_ERR_NEGATIVE_ET ? "Number of Negative Temperature Points > Limit (10)" : "device error";
+    return e;
+  }
+  if (L->shost->nan_count) {
+    CK(cudaMemsetAsync(&L->sdev->nan_count, 0, sizeof(int), L->st));
+    g_err = "NaN in the internal energy";
+    return OCFD_ERR_NAN;
+  }
+  return 0;
+}
+
+template <class F>
+int guarded(F&& fn) {
+  try {
+    return fn();
+  } catch (CudaError& e) {
+    g_err = e.what();
+    return e.code;
+  } catch (std::exception& e) {
+    g_err = e.what();
+    return OCFD_ERR_PARAM;
+  }
+}
+
+void fill_thermo(DevConst& c, const ocfd_thermo* th, int realgas) {
+  c.realgas = realgas;
+  c.n_tct = th->n_tct;
+  for (int j = 0; j < OCFD_NTCT_MAX; j++) c.tct[j] = th->tct[j];
+  c.tct_max = th->tct_max;
+  for (int k = 0; k < th->n_spec; k++) {
+    c.Mi[k] = th->mi[k];
+    c.Ri[k] = 8.314 / th->mi[k];
+    double ect = 0.0;
+    for (int j = 0; j < th->n_tct; j++) {
+      for (int m = 0; m < 7; m++) c.cf[k][j][m] = th->coef[k][j][m];
+      if (j == 0) {
+        ect = 0.0;
+      } else {  // read_Spec cross-range continuity offset (CHEM_thermdyn.f90:43-47)
+        double t = th->tct[j - 1];
+        const double* a = th->coef[k][j];
+        const double* b = th->coef[k][j - 1];
+        double t2 = t * t, t3 = t2 * t, t4 = t2 * t2, t5 = t2 * t3;
+        double s = (a[0] - b[0]) * t + (a[1] - b[1]) * t2 / 2.0 + (a[2] - b[2]) * t3 / 3.0 +
+                   (a[3] - b[3]) * t4 / 4.0 + (a[4] - b[4]) * t5 / 5.0;
+        ect = -s + ect;
+      }
+      c.cf[k][j][7] = ect;
+    }
+  }
+}
+void fill_kin(DevConst& c, const ocfd_kinetics* kin) {
+  c.nreac = kin->n_reac;
+  c.rereac = kin->rereac;
+  for (int j = 0; j < kin->n_reac; j++) {
+    c.af_type[j] = kin->af_type[j];
+    c.tr_reac[j] = kin->tr_reac[j];
+    c.fc_troe[j] = kin->fc_troe[j];
+    int sg = 0;
+    (void)sg;
+    for (int s = 0; s < 2; s++) { c.af[j][s] = kin->af[j][s]; c.bf[j][s] = kin->bf[j][s]; c.ef[j][s] = kin->ef[j][s]; }
+    c.ar[j] = kin->ar[j]; c.br[j] = kin->br[j]; c.er[j] = kin->er[j];
+    for (int m = 0; m < 5; m++) c.park[j][m] = kin->park[j][m];
+    for (int i = 0; i < kin->n_spec; i++) {
+      c.vf[j][i] = (signed char)kin->vf[j][i];
+      c.vr[j][i] = (signed char)kin->vr[j][i];
+      c.treff[j][i] = kin->treff[j][i];
+      sg += kin->vr[j][i] - kin->vf[j][i];
+    }
+    c.sgm[j] = sg;
+  }
+}
+void fill_trans(DevConst& c, const ocfd_transport* tr, int ns) {
+  c.flag_vis = tr->flag_vis; c.flag_cond = tr->flag_cond; c.flag_diff = tr->flag_diff;
+  c.amu0 = tr->amu0; c.pr = tr->pr; c.sc = tr->sc;
+  for (int k = 0; k < ns; k++)
+    for (int m = 0; m < 4; m++) {
+      c.mu_an[k][m] = tr->mu_an[k][m];
+      c.k_an[k][m] = tr->k_an[k][m];
+      for (int j = 0; j < ns; j++) c.d_an[k][j][m] = tr->d_an[k][j][m];
+    }
+}
+
+void release() {
+  if (!L) return;
+  if (L->gexec) cudaGraphExecDestroy(L->gexec);
+  for (auto& e : L->ev_pool) { cudaEventDestroy(e.first); cudaEventDestroy(e.second); }
+  if (L->arena) cudaFree(L->arena);
+  if (L->shost) cudaFreeHost(L->shost);
+  if (L->ht_host) cudaFreeHost(L->ht_host);
+  if (L->b_di) cudaFree(L->b_di);
+  if (L->ht_seq) cudaFree(L->ht_seq);
+  if (L->ht_seq_host) cudaFreeHost(L->ht_seq_host);
+  for (auto& e : L->uev)
+    if (e) cudaEventDestroy(e);
+  if (L->st) cudaStreamDestroy(L->st);
+  delete L;
+  L = nullptr;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------- setup kernels
+namespace ocfd {
+__global__ void k_fill(double* p, long long n, double v) {
+  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < n) p[t] = v;
+}
+// updata_Axyz_periodic (OCFD_mesh.f90:109-185): shift the coordinates of periodic face halos
+__global__ void k_shift(double* X, double* Y, double* Z, int dir, double sx, double sy, double sz) {
+  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const int L = OCFD_L;
+  int a, b, l, side;
+  long long na = dir == 0 ? cC.ny : cC.nx, nb = dir == 2 ? cC.ny : cC.nz;
+  if (t >= 2 * L * na * nb) return;
+  side = (int)(t & 1);
+  long long r = t >> 1;
+  a = (int)(r % na) + 1;
+  l = (int)((r / na) % L);
+  b = (int)(r / na / L) + 1;
+  int n = dir == 0 ? cC.nx : (dir == 1 ? cC.ny : cC.nz);
+  int s = side == 0 ? 1 - L + l : n + 1 + l;
+  int q = dir == 0 ? hidx(s, a, b) : (dir == 1 ? hidx(a, s, b) : hidx(a, b, s));
+  double sg = side == 0 ? -1.0 : 1.0;
+  if (side == 0) { X[q] = X[q] - sx; Y[q] = Y[q] - sy; Z[q] = Z[q] - sz; }
+  else { X[q] = X[q] + sx; Y[q] = Y[q] + sy; Z[q] = Z[q] + sz; }
+  (void)sg;
+}
+// comput_Jacobian3d (OCFD_mesh.f90:60-107) for general grids
+__global__ void k_jacobian(const double* X, const double* Y, const double* Z, double* const* m) {
+  int i, j, k;
+  if (!cell_of((long long)blockIdx.x * blockDim.x + threadIdx.x, i, j, k)) return;
+  int q = hidx(i, j, k);
+  double xi1 = cdiff(X, q, 0, i, cC.nx), yi1 = cdiff(Y, q, 0, i, cC.nx), zi1 = cdiff(Z, q, 0, i, cC.nx);
+  double xj1 = cdiff(X, q, 1, j, cC.ny), yj1 = cdiff(Y, q, 1, j, cC.ny), zj1 = cdiff(Z, q, 1, j, cC.ny);
+  double xk1 = cdiff(X, q, 2, k, cC.nz), yk1 = cdiff(Y, q, 2, k, cC.nz), zk1 = cdiff(Z, q, 2, k, cC.nz);
+  double jac = 1.0 / (xi1 * yj1 * zk1 + yi1 * zj1 * xk1 + zi1 * xj1 * yk1 - zi1 * yj1 * xk1 - yi1 * xj1 * zk1 -
+                      xi1 * zj1 * yk1);
+  m[G_AJAC][q] = jac;
+  m[G_AKX][q] = jac * (yj1 * zk1 - zj1 * yk1);
+  m[G_AKY][q] = jac * (zj1 * xk1 - xj1 * zk1);
+  m[G_AKZ][q] = jac * (xj1 * yk1 - yj1 * xk1);
+  m[G_AIX][q] = jac * (yk1 * zi1 - zk1 * yi1);
+  m[G_AIY][q] = jac * (zk1 * xi1 - xk1 * zi1);
+  m[G_AIZ][q] = jac * (xk1 * yi1 - yk1 * xi1);
+  m[G_ASX][q] = jac * (yi1 * zj1 - zi1 * yj1);
+  m[G_ASY][q] = jac * (zi1 * xj1 - xi1 * zj1);
+  m[G_ASZ][q] = jac * (xi1 * yj1 - yi1 * xj1);
+}
+// Akx1 = Akx / Ajac ... over the full halo range (OCFD_mesh.f90:40-54)
+__global__ void k_metric_ratio(double* const* m, long long H) {
+  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= H) return;
+  double jac = m[G_AJAC][t];
+  for (int a = 0; a < 9; a++) m[G_AKX1 + a][t] = m[a][t] / jac;
+}
+// tensor-product grids: dx/dxi(i), dy/deta(j), dz/dzeta(k) with the same CD6/CD8 + closures
+__global__ void k_metric1d(const double* X, const double* Y, const double* Z, double* dx, double* dy, double* dz) {
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int L = OCFD_L;
+  if (t < cC.nx) dx[t + L] = cdiff(X, hidx(t + 1, 1, 1), 0, t + 1, cC.nx);
+  if (t < cC.ny) dy[t + L] = cdiff(Y, hidx(1, t + 1, 1), 1, t + 1, cC.ny);
+  if (t < cC.nz) dz[t + L] = cdiff(Z, hidx(1, 1, t + 1), 2, t + 1, cC.nz);
+}
+__global__ void k_metric1d_halo(double* dx, double* dy, double* dz) {
+  int l = threadIdx.x;
+  const int L = OCFD_L;
+  if (l >= L) return;
+  double* a[3] = {dx, dy, dz};
+  int n[3] = {cC.nx, cC.ny, cC.nz};
+  for (int dd = 0; dd < 3; dd++) {
+    if (cC.iper[dd]) {
+      a[dd][l] = a[dd][n[dd] + l];          // index s+L-1 for s = 1-L+l  <-  s = n-L+1+l
+      a[dd][n[dd] + L + l] = a[dd][L + l];  // s = n+1+l  <-  s = 1+l
+    } else {
+      a[dd][l] = 1.0;
+      a[dd][n[dd] + L + l] = 1.0;
+    }
+  }
+}
+// FP64 FMA throughput probe: eight independent chains per thread, registers only
+__global__ void k_fp64_peak(double* out, int iters, double a, double b) {
+  double x0 = threadIdx.x, x1 = x0 + 1, x2 = x0 + 2, x3 = x0 + 3, x4 = x0 + 4, x5 = x0 + 5, x6 = x0 + 6, x7 = x0 + 7;
+  for (int it = 0; it < iters; it++) {
+    x0 = fma(x0, a, b); x1 = fma(x1, a, b); x2 = fma(x2, a, b); x3 = fma(x3, a, b);
+    x4 = fma(x4, a, b); x5 = fma(x5, a, b); x6 = fma(x6, a, b); x7 = fma(x7, a, b);
+  }
+  double s = x0 + x1 + x2 + x3 + x4 + x5 + x6 + x7;
+  if (s == 1234.5678) out[0] = s;  // keeps the chains live
+}
+}  // namespace ocfd
+
+namespace {
+
+int validate(const ocfd_params* p) {
+  auto bad = [](const char* m) { g_err = m; return OCFD_ERR_PARAM; };
+  if (p->lap != 4) return bad("LAP must be 4");
+  if (p->nx < 8 || p->ny < 8 || p->nz < 8) return bad("nx, ny, nz must be >= 8");
+  if (p->n_spec < 1 || p->n_spec > 9) return bad("N_SPEC must be 1..9");
+  int s = p->scheme_invis;
+  if (!(s == 1 || s == 2 || s == 3 || s == 4 || s == 10)) return bad("Scheme_Invis must be WENO5/WENO7/OMP6/UD7L/HYBRID");
+  if (!(p->scheme_vis == OCFD_SCHEME_CD6 || p->scheme_vis == OCFD_SCHEME_CD8)) return bad("Scheme_Vis must be CD6 or CD8");
+  if (!(p->flux_splitting == 1 || p->flux_splitting == 2)) return bad("Flux_Splitting must be 1 or 2");
+  for (int m = 0; m < 6; m++) {
+    if (p->scheme_boundary[m] < -1 || p->scheme_boundary[m] > 1) return bad("Scheme_boundary must be -1, 0 or 1");
+    if (p->ghost_cell[m] < 0 || p->ghost_cell[m] > 2) return bad("Ghost_Cell must be 0, 1 or 2");
+  }
+  if (p->if_scheme_character != 0) { g_err = "IF_Scheme_Character=1 (characteristic flux) is not built"; return OCFD_ERR_UNSUPPORTED; }
+  if (!(p->ibc == OCFD_BC_NONE || p->ibc == OCFD_BC_BOUNDARYLAYER)) { g_err = "boundary condition not built (BC_NONE, BC_BOUNDARYLAYER)"; return OCFD_ERR_UNSUPPORTED; }
+  if (p->wall_catalysis != 0) return bad("only non-catalytic walls");
+  if (!(p->chem_timeadv == 1 || p->chem_timeadv == 2 || p->chem_timeadv == 3 || p->chem_timeadv == -1)) return bad("CHEM_TimeAdv must be 1, 2, 3 or -1");
+  return 0;
+}
+
+bool separable(const ocfd_params* p, const double* coords) {
+  const int L4 = OCFD_L;
+  long long HX = p->nx + 2 * L4, HY = p->ny + 2 * L4;
+  auto ih = [&](int i, int j, int k) { return (long long)(i + L4 - 1) + HX * ((j + L4 - 1) + HY * (long long)(k + L4 - 1)); };
+  long long H = HX * HY * (p->nz + 2 * L4);
+  const double* X = coords;
+  const double* Y = coords + H;
+  const double* Z = coords + 2 * H;
+  for (int k = 1; k <= p->nz; k++)
+    for (int j = 1; j <= p->ny; j++)
+      for (int i = 1; i <= p->nx; i++) {
+        long long q = ih(i, j, k);
+        if (X[q] != X[ih(i, 1, 1)] || Y[q] != Y[ih(1, j, 1)] || Z[q] != Z[ih(1, 1, k)]) return false;
+      }
+  // the periodic shifts must keep the cross coordinates constant too
+  for (int dd = 0; dd < 3; dd++)
+    if (p->iperiodic[dd])
+      for (int c = 0; c < 3; c++)
+        if (c != dd && p->periodic_span[dd][c] != 0.0) return false;
+  return true;
+}
+
+void set_geo_device_ptrs() {
+  Geo& g = L->geo;
+  for (int m = 0; m < 19; m++) g.m[m] = L->met[m];
+  for (int m = 0; m < 3; m++) g.d1[m] = L->d1[m];
+}
+
+}  // namespace
+
+extern "C" {
+
+int ocfd_gpu_init(const ocfd_params* p, const ocfd_thermo* th, const ocfd_kinetics* kin, const ocfd_transport* tr,
+                  const ocfd_bcdata* bc, const double* coords, const double* metrics) {
+  return guarded([&]() -> int {
+    release();
+    if (!p || !th || !tr || !coords) { g_err = "null argument"; return OCFD_ERR_PARAM; }
+    int e = validate(p);
+    if (e) return e;
+    if (th->n_spec != p->n_spec) { g_err = "thermo n_spec differs from N_SPEC"; return OCFD_ERR_PARAM; }
+    if (p->ibc == OCFD_BC_BOUNDARYLAYER && !bc) { g_err = "BC_BOUNDARYLAYER needs boundary data"; return OCFD_ERR_PARAM; }
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) { g_err = "no CUDA device"; return OCFD_ERR_CUDA; }
+    L = new Lib();
+    L->P = *p;
+    L->NS = p->n_spec;
+    CK(cudaStreamCreateWithFlags(&L->st, cudaStreamNonBlocking));
+    DevConst& c = L->hc;
+    c.nx = p->nx; c.ny = p->ny; c.nz = p->nz; c.ns = p->n_spec;
+    c.HX = p->nx + 2 * OCFD_L; c.HY = p->ny + 2 * OCFD_L; c.HZ = p->nz + 2 * OCFD_L;
+    c.H = (long long)c.HX * c.HY * c.HZ;
+    c.N = (long long)p->nx * p->ny * p->nz;
+    if (c.H * p->n_spec >= (1LL << 31)) { g_err = "grid too large for 32-bit halo indexing"; return OCFD_ERR_PARAM; }
+    int nn[3] = {p->nx, p->ny, p->nz};
+    for (int dd = 0; dd < 3; dd++) {
+      c.iper[dd] = p->iperiodic[dd];
+      c.bound[dd][0] = c.bound[dd][1] = p->iperiodic[dd] == 0 ? 1 : 0;
+      double h = 1.0 / (nn[dd] - 1.0);
+      c.h[dd] = h;
+      c.h1[dd] = 1.0 / h;
+      c.cd6[dd][0] = 1.0 / (60.0 * h); c.cd6[dd][1] = -3.0 / (20.0 * h); c.cd6[dd][2] = 3.0 / (4.0 * h);
+      c.cd8[dd][0] = 0.8 / h; c.cd8[dd][1] = -0.2 / h; c.cd8[dd][2] = 3.80952380952380952e-2 / h;
+      c.cd8[dd][3] = -3.571428571428571428e-3 / h;
+      c.h2x[dd] = 2.0 * h; c.h12x[dd] = 12.0 * h;
+    }
+    for (int m = 0; m < 6; m++) { c.sb[m] = p->scheme_boundary[m]; c.ghost[m] = p->ghost_cell[m]; }
+    c.scheme = p->scheme_invis; c.split = p->flux_splitting;
+    switch (c.scheme) {
+      case 1: c.Ka1 = -2; c.Kb1 = 2; c.Ka2 = -1; c.Kb2 = 3; break;
+      case 2: c.Ka1 = -3; c.Kb1 = 3; c.Ka2 = -2; c.Kb2 = 4; break;
+      default: c.Ka1 = -3; c.Kb1 = 4; c.Ka2 = -3; c.Kb2 = 4;
+    }
+    {
+      const double UD7[8] = {-3.0, 25.0, -101.0, 319.0, 214.0, -38.0, 4.0, 0.0};
+      const double CD8[8] = {-3.0, 29.0, -139.0, 533.0, 533.0, -139.0, 29.0, -3.0};
+      for (int k = 0; k < 8; k++) c.UD7L[k] = p->ud7l_diss * UD7[k] / 420.0 + (1.0 - p->ud7l_diss) * CD8[k] / 840.0;
+    }
+    c.theta1 = p->hybrid_para[1];
+    c.theta2 = p->hybrid_para[2];
+    c.cd8_on = p->scheme_vis == OCFD_SCHEME_CD8;
+    c.if_viscous = p->if_viscous;
+    c.if_mass_force = p->if_mass_force;
+    for (int m = 0; m < 3; m++) c.mass_force[m] = p->mass_force[m];
+    fill_thermo(c, th, p->if_realgas);
+    fill_trans(c, tr, p->n_spec);
+    c.timeadv = p->chem_timeadv;
+    if (kin) {
+      if (kin->n_spec != p->n_spec || kin->n_reac > OCFD_MAX_REAC) { g_err = "kinetics size"; return OCFD_ERR_PARAM; }
+      fill_kin(c, kin);
+      L->have_kin = true;
+    }
+    CK(cudaMemcpyToSymbol(cC, &c, sizeof(DevConst)));
+
+    L->sep = separable(p, coords);
+    const long long H = c.H, N = c.N;
+    const int NS = p->n_spec;
+    size_t total = 0;
+    auto add = [&](size_t n, size_t sz) { total += (n * sz + 255) & ~(size_t)255; };
+    add(5 * N, 8); add(5 * N, 8); add(5 * N, 8);
+    for (int m = 0; m < 8; m++) add(H, 8);
+    add(NS * H, 8); add(NS * N, 8); add(H, 8);
+    for (int m = 0; m < 12; m++) add(H, 8);
+    if (NS > 1) { add(N, 8); add(N, 8); add(NS * N, 8); for (int m = 0; m < 3; m++) add(N, 8); add(H, 8); for (int m = 0; m < 3; m++) add(H, 8); }
+    for (int m = 0; m < 3; m++) add(H, 8);
+    if (!L->sep) for (int m = 0; m < 19; m++) add(H, 8);
+    for (int m = 0; m < 3; m++) add(nn[m] + 2 * OCFD_L, 8);
+    add(2 * ((N + 255) / 256) + 2, 8);
+    size_t nv = 5 + NS;
+    add(nv * (size_t)std::max((long long)p->ny * p->nz, (long long)p->nx * p->nz) + nv, 8);
+    add(nv * (size_t)std::max((long long)p->ny * p->nz, (long long)p->nx * p->nz) + nv, 8);
+    add((size_t)p->nx * p->nz, 8); add((size_t)p->nx * p->nz, 4); add(1, 8);
+    add(6 * 20, 4); add(1, sizeof(DevStatus)); add(12, sizeof(double*)); add(19, sizeof(double*));
+    L->arena_size = total + (1 << 20);
+    CK(cudaMalloc(&L->arena, L->arena_size));
+    CK(cudaMallocHost(&L->shost, sizeof(DevStatus)));
+    CK(cudaMallocHost(&L->ht_host, sizeof(double)));
+
+    L->f = alloc<double>(5 * N); L->fn = alloc<double>(5 * N); L->du = alloc<double>(5 * N);
+    L->d = alloc<double>(H); L->u = alloc<double>(H); L->v = alloc<double>(H); L->w = alloc<double>(H);
+    L->T = alloc<double>(H); L->p = alloc<double>(H); L->Et[0] = alloc<double>(H); L->Et[1] = alloc<double>(H);
+    L->di = alloc<double>(NS * H); L->din = alloc<double>(NS * N); L->Rh = alloc<double>(H);
+    for (int m = 0; m < 12; m++) L->ev[m] = alloc<double>(H);
+    if (NS > 1) {
+      L->amu = alloc<double>(N); L->amk = alloc<double>(N); L->amd = alloc<double>(NS * N);
+      for (int m = 0; m < 3; m++) L->qp[m] = alloc<double>(N);
+      L->ci = alloc<double>(H);
+      for (int m = 0; m < 3; m++) L->se[m] = alloc<double>(H);
+    }
+    L->X = alloc<double>(H); L->Y = alloc<double>(H); L->Z = alloc<double>(H);
+    if (!L->sep) for (int m = 0; m < 19; m++) L->met[m] = alloc<double>(H);
+    for (int m = 0; m < 3; m++) L->d1[m] = alloc<double>(nn[m] + 2 * OCFD_L);
+    L->partial = alloc<double>(2 * ((N + 255) / 256) + 2);
+    L->inlet = alloc<double>(nv * (size_t)std::max((long long)p->ny * p->nz, (long long)p->nx * p->nz) + nv);
+    L->upper = alloc<double>(nv * (size_t)std::max((long long)p->ny * p->nz, (long long)p->nx * p->nz) + nv);
+    L->wall = alloc<double>((size_t)p->nx * p->nz);
+    L->nonref = alloc<int>((size_t)p->nx * p->nz);
+    L->ht_dev = alloc<double>(1);
+    L->patches = alloc<int>(6 * 20);
+    L->sdev = alloc<DevStatus>(1);
+    L->ev_ptrs = alloc<double*>(12);
+    double** met_ptrs = alloc<double*>(19);
+    CK(cudaMemcpyAsync(L->ev_ptrs, L->ev, sizeof(double*) * 12, cudaMemcpyHostToDevice, L->st));
+    CK(cudaMemsetAsync(L->sdev, 0, sizeof(DevStatus), L->st));
+
+    // allocate_flow_data initial values (OCFD_allocate_data.f90:53-67)
+    auto fill = [&](double* a, long long n, double val) {
+      k_fill<<<nblk(n, 256), 256, 0, L->st>>>(a, n, val);
+      LAUNCH_CHECK();
+    };
+    fill(L->du, 5 * N, 0.0);
+    fill(L->f, 5 * N, 0.0); fill(L->fn, 5 * N, 0.0);
+    for (double* a : {L->d, L->u, L->v, L->w, L->p, L->Et[0], L->Et[1]}) fill(a, H, 1.0);
+    fill(L->T, H, 300.0);
+    fill(L->di, NS * H, 1.0); fill(L->din, NS * N, 1.0);
+    fill(L->Rh, H, 0.0);
+    for (int m = 0; m < 12; m++) fill(L->ev[m], H, 0.0);
+    if (NS > 1) {
+      fill(L->amu, N, 0.0); fill(L->amk, N, 0.0); fill(L->amd, NS * N, 0.0);
+      for (int m = 0; m < 3; m++) fill(L->qp[m], N, 0.0);
+      fill(L->ci, H, 0.0);
+      for (int m = 0; m < 3; m++) fill(L->se[m], H, 0.0);
+    }
+    // init_mesh
+    CK(cudaMemcpyAsync(L->X, coords, sizeof(double) * H, cudaMemcpyHostToDevice, L->st));
+    CK(cudaMemcpyAsync(L->Y, coords + H, sizeof(double) * H, cudaMemcpyHostToDevice, L->st));
+    CK(cudaMemcpyAsync(L->Z, coords + 2 * H, sizeof(double) * H, cudaMemcpyHostToDevice, L->st));
+    exchange({L->X, L->Y, L->Z}, 7);
+    for (int dd = 0; dd < 3; dd++) {
+      if (!p->iperiodic[dd]) continue;
+      long long na = dd == 0 ? p->ny : p->nx, nb = dd == 2 ? p->ny : p->nz;
+      k_shift<<<nblk(2 * OCFD_L * na * nb, 256), 256, 0, L->st>>>(L->X, L->Y, L->Z, dd, p->periodic_span[dd][0],
+                                                                  p->periodic_span[dd][1], p->periodic_span[dd][2]);
+      LAUNCH_CHECK();
+    }
+    if (L->sep && metrics == nullptr) {
+      int mx = std::max(p->nx, std::max(p->ny, p->nz));
+      k_metric1d<<<nblk(mx, 128), 128, 0, L->st>>>(L->X, L->Y, L->Z, L->d1[0], L->d1[1], L->d1[2]);
+      LAUNCH_CHECK();
+      k_metric1d_halo<<<1, 32, 0, L->st>>>(L->d1[0], L->d1[1], L->d1[2]);
+      LAUNCH_CHECK();
+    } else {
+      L->sep = false;
+      if (!L->met[0]) throw std::runtime_error("metric arrays not allocated");
+      CK(cudaMemcpyAsync(met_ptrs, L->met, sizeof(double*) * 19, cudaMemcpyHostToDevice, L->st));
+      for (int m = 0; m < 19; m++) fill(L->met[m], H, 1.0);
+      if (metrics) {
+        for (int m = 0; m < 10; m++)
+          CK(cudaMemcpyAsync(L->met[m], metrics + (size_t)m * H, sizeof(double) * H, cudaMemcpyHostToDevice, L->st));
+      } else {
+        k_jacobian<<<nblk(N, 256), 256, 0, L->st>>>(L->X, L->Y, L->Z, met_ptrs);
+        LAUNCH_CHECK();
+      }
+      std::vector<double*> ml(L->met, L->met + 10);
+      exchange_v(ml, 7);
+      k_metric_ratio<<<nblk(H, 256), 256, 0, L->st>>>(met_ptrs, H);
+      LAUNCH_CHECK();
+    }
+    set_geo_device_ptrs();
+
+    // boundary-layer data (init_bcdata_boundary / init_bc_nonRef / init_bc_wall_perturbation)
+    if (p->ibc == OCFD_BC_BOUNDARYLAYER) {
+      L->inlet_kind = (int)std::lround(p->bc_para[0]);
+      L->upper_kind = (int)std::lround(p->bc_para[1]);
+      L->outlet = (int)std::lround(p->bc_para[3]);
+      size_t ni = L->inlet_kind == 0 ? nv : (L->inlet_kind == 1 ? nv * p->ny : nv * (size_t)p->ny * p->nz);
+      size_t nu = L->upper_kind == 0 ? nv : (L->upper_kind == 1 ? nv * p->nx : nv * (size_t)p->nx * p->nz);
+      if (L->inlet_kind < 0 || L->inlet_kind > 2 || L->upper_kind > 2) { g_err = "BcData_inlet / BcData_upper"; return OCFD_ERR_PARAM; }
+      CK(cudaMemcpyAsync(L->inlet, bc->inlet, sizeof(double) * ni, cudaMemcpyHostToDevice, L->st));
+      if (L->upper_kind >= 0) CK(cudaMemcpyAsync(L->upper, bc->upper, sizeof(double) * nu, cudaMemcpyHostToDevice, L->st));
+      if (bc->wall_pertb) CK(cudaMemcpyAsync(L->wall, bc->wall_pertb, sizeof(double) * p->nx * p->nz, cudaMemcpyHostToDevice, L->st));
+      else fill(L->wall, (long long)p->nx * p->nz, 0.0);
+      L->tm.assign(bc->tm, bc->tm + bc->n_tm);
+      L->fait.assign(bc->fait, bc->fait + bc->n_tm);
+      std::vector<int> nr((size_t)p->nx * p->nz, 0);
+      int mode = (int)std::lround(p->bc_para[2]);
+      double sy0 = std::tan(p->aoa);
+      const int L4 = OCFD_L;
+      long long HX = c.HX, HY = c.HY;
+      auto ih = [&](int i, int j, int k) { return (long long)(i + L4 - 1) + HX * ((j + L4 - 1) + HY * (long long)(k + L4 - 1)); };
+      const double* Xh = coords;
+      const double* Yh = coords + H;
+      for (int k = 1; k <= p->nz; k++)
+        for (int i = 1; i <= p->nx; i++) {
+          int val = 0;
+          if (mode == 1) val = 1;
+          else if (mode == 0) {
+            double sy;
+            if (i == 1) sy = (Yh[ih(i + 1, p->ny, k)] - Yh[ih(i, p->ny, k)]) / (Xh[ih(i + 1, p->ny, k)] - Xh[ih(i, p->ny, k)]);
+            else sy = (Yh[ih(i, p->ny, k)] - Yh[ih(i - 1, p->ny, k)]) / (Xh[ih(i, p->ny, k)] - Xh[ih(i - 1, p->ny, k)]);
+            val = (sy >= sy0 + 1.0e-6) ? 0 : 1;
+          }
+          nr[(i - 1) + (size_t)p->nx * (k - 1)] = val;
+        }
+      CK(cudaMemcpy(L->nonref, nr.data(), sizeof(int) * nr.size(), cudaMemcpyHostToDevice));
+    }
+    // hybrid forced patches (Hybrid_para(4..), OCFD_SetHybrid.f90:80-102)
+    if (p->scheme_invis == OCFD_SCHEME_HYBRID) {
+      int mp = (int)std::lround(p->hybrid_para[3]);
+      if (mp < 0 || mp > 15) { g_err = "Hybrid_para(4): at most 15 patches"; return OCFD_ERR_PARAM; }
+      std::vector<int> pb(6 * 20, 0);
+      for (int m = 0; m < mp; m++) {
+        const double* h = p->hybrid_para + 4 + 6 * m;
+        pb[6 * m + 0] = std::max((int)std::lround(h[0]), 1);
+        pb[6 * m + 1] = std::min((int)std::lround(h[1]), p->nx);
+        pb[6 * m + 2] = std::max((int)std::lround(h[2]), 1);
+        pb[6 * m + 3] = std::min((int)std::lround(h[3]), p->ny);
+        pb[6 * m + 4] = std::max((int)std::lround(h[4]), 1);
+        pb[6 * m + 5] = std::min((int)std::lround(h[5]), p->nz);
+      }
+      L->npatch = mp;
+      CK(cudaMemcpy(L->patches, pb.data(), sizeof(int) * pb.size(), cudaMemcpyHostToDevice));
+    }
+    CK(cudaStreamSynchronize(L->st));
+    return 0;
+  });
+}
+
+int ocfd_gpu_init_state(const double* prim5, const double* di, double tt) {
+  return guarded([&]() -> int {
+    if (!L || !L->d) { g_err = "ocfd_gpu_init first"; return OCFD_ERR_STATE; }
+    const long long N = L->hc.N;
+    const int NS = L->NS;
+    double *dp, *ddi;
+    CK(cudaMallocAsync(&dp, sizeof(double) * 5 * N, L->st));
+    CK(cudaMallocAsync(&ddi, sizeof(double) * NS * N, L->st));
+    CK(cudaMemcpyAsync(dp, prim5, sizeof(double) * 5 * N, cudaMemcpyHostToDevice, L->st));
+    CK(cudaMemcpyAsync(ddi, di, sizeof(double) * NS * N, cudaMemcpyHostToDevice, L->st));
+    NS_DISPATCH(NS, {
+      k_init_state<NSV><<<nblk(N, 256), 256, 0, L->st>>>(dp, ddi, L->f, L->d, L->u, L->v, L->w, L->T, L->di);
+      LAUNCH_CHECK();
+      set_time(tt);
+      prims_t<NSV>(0, 0.0);
+      ocfd_bc_t<NSV>();
+    });
+    CK(cudaFreeAsync(dp, L->st));
+    CK(cudaFreeAsync(ddi, L->st));
+    L->flow_ready = true;
+    return check_status();
+  });
+}
+
+int ocfd_gpu_upload_state(const double* f, const double* di, const double* prims) {
+  return guarded([&]() -> int {
+    if (!L || !L->d) { g_err = "ocfd_gpu_init first"; return OCFD_ERR_STATE; }
+    const long long N = L->hc.N, H = L->hc.H;
+    CK(cudaMemcpyAsync(L->f, f, sizeof(double) * 5 * N, cudaMemcpyHostToDevice, L->st));
+    CK(cudaMemcpyAsync(L->di, di, sizeof(double) * L->NS * H, cudaMemcpyHostToDevice, L->st));
+    double* pr[7] = {L->d, L->u, L->v, L->w, L->T, L->p, L->Et[L->cur]};
+    for (int m = 0; m < 7; m++)
+      CK(cudaMemcpyAsync(pr[m], prims + (size_t)m * H, sizeof(double) * H, cudaMemcpyHostToDevice, L->st));
+    CK(cudaMemcpyAsync(L->Et[1 - L->cur], prims + (size_t)6 * H, sizeof(double) * H, cudaMemcpyHostToDevice, L->st));
+    CK(cudaStreamSynchronize(L->st));
+    L->flow_ready = true;
+    return 0;
+  });
+}
+
+int ocfd_gpu_flow_advance(double dt1, double tt) {
+  return guarded([&]() -> int {
+    if (!L || !L->flow_ready) { g_err = "state not initialised"; return OCFD_ERR_STATE; }
+    set_time(tt);
+    NS_DISPATCH(L->NS, flow_advance_t<NSV>(dt1));
+    return check_status();
+  });
+}
+
+int ocfd_gpu_chem_advance(double dt2, int nsub) {
+  return guarded([&]() -> int {
+    if (!L || !L->flow_ready) { g_err = "state not initialised"; return OCFD_ERR_STATE; }
+    if (!L->have_kin) { g_err = "no reaction mechanism given to ocfd_gpu_init"; return OCFD_ERR_PARAM; }
+    NS_DISPATCH(L->NS, chem_t<NSV>(dt2, nsub));
+    return check_status();
+  });
+}
+
+}  // extern "C"
+
+namespace {
+// (re)captures the Strang step as a CUDA graph when dt, the chemistry switch or the Et buffer
+// parity changed since the last capture
+void ensure_graph(double dt, int if_reaction, int nsub) {
+  if (L->gexec && L->g_dt == dt && L->g_ifr == if_reaction && L->g_nsub == nsub && L->g_par == L->cur) return;
+  if (L->gexec) { CK(cudaGraphExecDestroy(L->gexec)); L->gexec = nullptr; }
+  int cur0 = L->cur;
+  long long l0 = L->launches;
+  cudaGraph_t graph;
+  CK(cudaStreamBeginCapture(L->st, cudaStreamCaptureModeThreadLocal));
+  try {
+    NS_DISPATCH(L->NS, {
+      flow_advance_t<NSV>(0.5 * dt);
+      if (if_reaction) chem_t<NSV>(dt / nsub, nsub);
+      flow_advance_t<NSV>(0.5 * dt);
+    });
+  } catch (...) {
+    cudaStreamEndCapture(L->st, &graph);
+    L->cur = cur0;
+    throw;
+  }
+  CK(cudaStreamEndCapture(L->st, &graph));
+  CK(cudaGraphInstantiate(&L->gexec, graph, 0));
+  CK(cudaGraphDestroy(graph));
+  L->g_dt = dt; L->g_ifr = if_reaction; L->g_nsub = nsub; L->g_par = cur0;
+  L->g_launches = (int)(L->launches - l0);
+  L->launches = l0;
+  L->cur = cur0;  // six stages: the Et buffer parity returns to its start value
+}
+}  // namespace
+
+extern "C" {
+
+int ocfd_gpu_step(double dt, double tt, int if_reaction, int nsub) {
+  return guarded([&]() -> int {
+    if (!L || !L->flow_ready) { g_err = "state not initialised"; return OCFD_ERR_STATE; }
+    if (if_reaction && !L->have_kin) { g_err = "no reaction mechanism given to ocfd_gpu_init"; return OCFD_ERR_PARAM; }
+    if (nsub < 1) nsub = 1;
+    set_time(tt);
+    if (L->prof) {  // timed per kernel: plain launches
+      NS_DISPATCH(L->NS, {
+        flow_advance_t<NSV>(0.5 * dt);
+        if (if_reaction) chem_t<NSV>(dt / nsub, nsub);
+        flow_advance_t<NSV>(0.5 * dt);
+      });
+      return check_status();
+    }
+    ensure_graph(dt, if_reaction, nsub);
+    CK(cudaGraphLaunch(L->gexec, L->st));
+    L->launches += L->g_launches;
+    return check_status();
+  });
+}
+
+int ocfd_gpu_run(double dt, double tt0, int nsteps, int if_reaction, int nsub) {
+  return guarded([&]() -> int {
+    if (!L || !L->flow_ready) { g_err = "state not initialised"; return OCFD_ERR_STATE; }
+    if (if_reaction && !L->have_kin) { g_err = "no reaction mechanism given to ocfd_gpu_init"; return OCFD_ERR_PARAM; }
+    if (nsteps <= 0) return 0;
+    if (nsub < 1) nsub = 1;
+    if (nsteps > L->ht_cap) {
+      if (L->ht_seq) cudaFree(L->ht_seq);
+      if (L->ht_seq_host) cudaFreeHost(L->ht_seq_host);
+      CK(cudaMalloc(&L->ht_seq, sizeof(double) * nsteps));
+      CK(cudaMallocHost(&L->ht_seq_host, sizeof(double) * nsteps));
+      L->ht_cap = nsteps;
+    }
+    CK(cudaStreamSynchronize(L->st));
+    for (int s = 0; s < nsteps; s++) L->ht_seq_host[s] = wall_ht(tt0 + s * dt);
+    CK(cudaMemcpyAsync(L->ht_seq, L->ht_seq_host, sizeof(double) * nsteps, cudaMemcpyHostToDevice, L->st));
+    ensure_graph(dt, if_reaction, nsub);
+    for (int s = 0; s < nsteps; s++) {
+      CK(cudaMemcpyAsync(L->ht_dev, L->ht_seq + s, sizeof(double), cudaMemcpyDeviceToDevice, L->st));
+      CK(cudaGraphLaunch(L->gexec, L->st));
+      L->launches += L->g_launches;
+    }
+    return check_status();
+  });
+}
+
+int ocfd_gpu_event_record(int slot) {
+  return guarded([&]() -> int {
+    if (!L || slot < 0 || slot >= 16) { g_err = "event slot"; return OCFD_ERR_PARAM; }
+    if (!L->uev[slot]) CK(cudaEventCreate(&L->uev[slot]));
+    CK(cudaEventRecord(L->uev[slot], L->st));
+    return 0;
+  });
+}
+
+int ocfd_gpu_event_elapsed(int a, int b, double* ms) {
+  return guarded([&]() -> int {
+    if (!L || a < 0 || b < 0 || a >= 16 || b >= 16 || !L->uev[a] || !L->uev[b]) { g_err = "event slot"; return OCFD_ERR_PARAM; }
+    CK(cudaEventSynchronize(L->uev[b]));
+    float f = 0;
+    CK(cudaEventElapsedTime(&f, L->uev[a], L->uev[b]));
+    *ms = f;
+    return 0;
+  });
+}
+
+int ocfd_gpu_pinned_alloc(size_t bytes, void** ptr) {
+  return guarded([&]() -> int {
+    CK(cudaMallocHost(ptr, bytes));
+    return 0;
+  });
+}
+
+int ocfd_gpu_pinned_free(void* ptr) {
+  return guarded([&]() -> int {
+    CK(cudaFreeHost(ptr));
+    return 0;
+  });
+}
+
+int ocfd_gpu_step_launches(void) { return L ? L->g_launches : 0; }
+
+int ocfd_gpu_download_state(double* f, double* di, double* prims) {
+  return guarded([&]() -> int {
+    if (!L || !L->d) { g_err = "ocfd_gpu_init first"; return OCFD_ERR_STATE; }
+    const long long N = L->hc.N, H = L->hc.H;
+    if (f) CK(cudaMemcpyAsync(f, L->f, sizeof(double) * 5 * N, cudaMemcpyDeviceToHost, L->st));
+    if (di) CK(cudaMemcpyAsync(di, L->di, sizeof(double) * L->NS * H, cudaMemcpyDeviceToHost, L->st));
+    if (prims) {
+      double* pr[7] = {L->d, L->u, L->v, L->w, L->T, L->p, L->Et[L->cur]};
+      for (int m = 0; m < 7; m++)
+        CK(cudaMemcpyAsync(prims + (size_t)m * H, pr[m], sizeof(double) * H, cudaMemcpyDeviceToHost, L->st));
+    }
+    CK(cudaStreamSynchronize(L->st));
+    return 0;
+  });
+}
+
+int ocfd_gpu_diag(double* e_mean, double* k_mean) {
+  return guarded([&]() -> int {
+    if (!L || !L->flow_ready) { g_err = "state not initialised"; return OCFD_ERR_STATE; }
+    const long long N = L->hc.N;
+    unsigned nb = nblk(N, 256);
+    if (L->sep) k_diag<true><<<nb, 256, 0, L->st>>>(L->f, L->d, L->u, L->v, L->w, L->partial, L->geo);
+    else k_diag<false><<<nb, 256, 0, L->st>>>(L->f, L->d, L->u, L->v, L->w, L->partial, L->geo);
+    LAUNCH_CHECK();
+    std::vector<double> h(2 * nb);
+    CK(cudaMemcpyAsync(h.data(), L->partial, sizeof(double) * 2 * nb, cudaMemcpyDeviceToHost, L->st));
+    CK(cudaStreamSynchronize(L->st));
+    double e = 0.0, k = 0.0;
+    for (unsigned b = 0; b < nb; b++) { e = e + h[2 * b]; k = k + h[2 * b + 1]; }
+    double nn = (double)L->P.nx * L->P.ny * L->P.nz;
+    *e_mean = e / nn;
+    *k_mean = k / nn;
+    return 0;
+  });
+}
+
+int ocfd_gpu_download_rhybrid(double* r) {
+  return guarded([&]() -> int {
+    if (!L || !L->d) { g_err = "ocfd_gpu_init first"; return OCFD_ERR_STATE; }
+    CK(cudaMemcpyAsync(r, L->Rh, sizeof(double) * L->hc.H, cudaMemcpyDeviceToHost, L->st));
+    CK(cudaStreamSynchronize(L->st));
+    return 0;
+  });
+}
+
+int ocfd_gpu_download_metrics(double* m) {
+  return guarded([&]() -> int {
+    if (!L || !L->d) { g_err = "ocfd_gpu_init first"; return OCFD_ERR_STATE; }
+    const long long H = L->hc.H;
+    if (L->sep) {
+      // expand the separable metrics to the reference's ten 3-D arrays (interior + periodic halo)
+      int nn[3] = {L->P.nx, L->P.ny, L->P.nz};
+      std::vector<double> d1[3];
+      for (int dd = 0; dd < 3; dd++) {
+        d1[dd].resize(nn[dd] + 2 * OCFD_L);
+        CK(cudaMemcpy(d1[dd].data(), L->d1[dd], sizeof(double) * d1[dd].size(), cudaMemcpyDeviceToHost));
+      }
+      const int L4 = OCFD_L;
+      long long HX = L->hc.HX, HY = L->hc.HY;
+      for (int mm = 0; mm < 10; mm++) std::fill(m + mm * H, m + (mm + 1) * H, 1.0);
+      for (int k = 1 - L4; k <= nn[2] + L4; k++)
+        for (int j = 1 - L4; j <= nn[1] + L4; j++)
+          for (int i = 1 - L4; i <= nn[0] + L4; i++) {
+            int outside = (i < 1 || i > nn[0]) + (j < 1 || j > nn[1]) + (k < 1 || k > nn[2]);
+            if (outside > 1) continue;
+            if ((i < 1 || i > nn[0]) && !L->P.iperiodic[0]) continue;
+            if ((j < 1 || j > nn[1]) && !L->P.iperiodic[1]) continue;
+            if ((k < 1 || k > nn[2]) && !L->P.iperiodic[2]) continue;
+            long long q = (i + L4 - 1) + HX * ((j + L4 - 1) + HY * (long long)(k + L4 - 1));
+            double xi = d1[0][i + L4 - 1], yj = d1[1][j + L4 - 1], zk = d1[2][k + L4 - 1];
+            double jac = 1.0 / (xi * yj * zk);
+            for (int mm = 0; mm < 9; mm++) m[mm * H + q] = 0.0;
+            m[0 * H + q] = jac * (yj * zk);
+            m[4 * H + q] = jac * (zk * xi);
+            m[8 * H + q] = jac * (xi * yj);
+            m[9 * H + q] = jac;
+          }
+      return 0;
+    }
+    for (int mm = 0; mm < 10; mm++) CK(cudaMemcpy(m + mm * H, L->met[mm], sizeof(double) * H, cudaMemcpyDeviceToHost));
+    return 0;
+  });
+}
+
+int ocfd_gpu_chem_setup(const ocfd_thermo* th, const ocfd_kinetics* kin, int realgas, int timeadv) {
+  return guarded([&]() -> int {
+    if (!th || !kin) { g_err = "null argument"; return OCFD_ERR_PARAM; }
+    if (th->n_spec < 1 || th->n_spec > 9 || kin->n_spec != th->n_spec || kin->n_reac > OCFD_MAX_REAC) {
+      g_err = "N_SPEC must be 1..9 and match the mechanism";
+      return OCFD_ERR_PARAM;
+    }
+    if (!(timeadv == 1 || timeadv == 2 || timeadv == 3 || timeadv == -1)) { g_err = "CHEM_TimeAdv"; return OCFD_ERR_PARAM; }
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) { g_err = "no CUDA device"; return OCFD_ERR_CUDA; }
+    if (!L) {
+      L = new Lib();
+      CK(cudaStreamCreateWithFlags(&L->st, cudaStreamNonBlocking));
+      CK(cudaMallocHost(&L->shost, sizeof(DevStatus)));
+      CK(cudaMallocHost(&L->ht_host, sizeof(double)));
+    }
+    L->NS = th->n_spec;
+    fill_thermo(L->hc, th, realgas);
+    fill_kin(L->hc, kin);
+    L->hc.timeadv = timeadv;
+    L->hc.ns = th->n_spec;
+    L->have_kin = true;
+    CK(cudaMemcpyToSymbol(cC, &L->hc, sizeof(DevConst)));
+    return 0;
+  });
+}
+
+int ocfd_gpu_chem_batch_device(int n, double* d_di, double* d_e, const double* d_dt, const int* d_nsub) {
+  return guarded([&]() -> int {
+    if (!L || !L->have_kin) { g_err = "ocfd_gpu_init or ocfd_gpu_chem_setup with a mechanism first"; return OCFD_ERR_STATE; }
+    if (n <= 0) return 0;
+    const int nbins = 1024;
+    if ((size_t)n > L->b_cap) {
+      if (L->b_di) cudaFree(L->b_di);
+      size_t bytes = sizeof(int) * ((size_t)n + nbins + 64);
+      CK(cudaMalloc(&L->b_di, bytes));
+      L->b_perm = reinterpret_cast<int*>(L->b_di);
+      L->b_hist = L->b_perm + n;
+      L->b_counter = L->b_hist + nbins;
+      L->b_nfail = L->b_counter + 32;
+      L->b_cap = n;
+    }
+    CK(cudaMemsetAsync(L->b_hist, 0, sizeof(int) * (nbins + 64), L->st));
+    {
+      KTimer t(KC_CHEM);
+      k_nsub_hist<<<nblk(n, 256), 256, 0, L->st>>>(n, d_nsub, L->b_hist, nbins);
+      k_nsub_scan<<<1, 32, 0, L->st>>>(L->b_hist, nbins);
+      k_nsub_scatter<<<nblk(n, 256), 256, 0, L->st>>>(n, d_nsub, L->b_hist, nbins, L->b_perm);
+      LAUNCH_CHECK();
+    }
+    int dev = 0, sms = 148;
+    CK(cudaGetDevice(&dev));
+    CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    {
+      KTimer t(KC_CHEM);
+      launch_chem_batch(L->NS, sms, n, d_di, d_e, d_dt, d_nsub, L->b_perm, L->b_counter, L->b_nfail, L->st);
+      LAUNCH_CHECK();
+    }
+    CK(cudaStreamSynchronize(L->st));
+    prof_collect();
+    return 0;
+  });
+}
+
+int ocfd_gpu_chem_batch(int n, double* di, double* e, const double* dt, const int* nsub) {
+  return guarded([&]() -> int {
+    if (!L || !L->have_kin) { g_err = "ocfd_gpu_init or ocfd_gpu_chem_setup with a mechanism first"; return OCFD_ERR_STATE; }
+    if (n <= 0) return 0;
+    const int NS = L->NS;
+    double *ddi, *de, *ddt;
+    int* dns = nullptr;
+    CK(cudaMallocAsync(&ddi, sizeof(double) * (size_t)n * NS, L->st));
+    CK(cudaMallocAsync(&de, sizeof(double) * n, L->st));
+    CK(cudaMallocAsync(&ddt, sizeof(double) * n, L->st));
+    if (nsub) CK(cudaMallocAsync(&dns, sizeof(int) * n, L->st));
+    CK(cudaMemcpyAsync(ddi, di, sizeof(double) * (size_t)n * NS, cudaMemcpyHostToDevice, L->st));
+    CK(cudaMemcpyAsync(de, e, sizeof(double) * n, cudaMemcpyHostToDevice, L->st));
+    CK(cudaMemcpyAsync(ddt, dt, sizeof(double) * n, cudaMemcpyHostToDevice, L->st));
+    if (nsub) CK(cudaMemcpyAsync(dns, nsub, sizeof(int) * n, cudaMemcpyHostToDevice, L->st));
+    int rc = ocfd_gpu_chem_batch_device(n, ddi, de, ddt, dns);
+    if (rc) return rc;
+    CK(cudaMemcpyAsync(di, ddi, sizeof(double) * (size_t)n * NS, cudaMemcpyDeviceToHost, L->st));
+    CK(cudaMemcpyAsync(e, de, sizeof(double) * n, cudaMemcpyDeviceToHost, L->st));
+    CK(cudaFreeAsync(ddi, L->st));
+    CK(cudaFreeAsync(de, L->st));
+    CK(cudaFreeAsync(ddt, L->st));
+    if (dns) CK(cudaFreeAsync(dns, L->st));
+    CK(cudaStreamSynchronize(L->st));
+    return 0;
+  });
+}
+
+int ocfd_gpu_stats(long long* neg_et, long long* newton_fail) {
+  return guarded([&]() -> int {
+    if (!L || !L->sdev) { g_err = "not initialised"; return OCFD_ERR_STATE; }
+    CK(cudaMemcpyAsync(L->shost, L->sdev, sizeof(DevStatus), cudaMemcpyDeviceToHost, L->st));
+    CK(cudaStreamSynchronize(L->st));
+    if (neg_et) *neg_et = (long long)L->shost->neg_total;
+    if (newton_fail) *newton_fail = L->shost->newton_fail;
+    return 0;
+  });
+}
+
+int ocfd_gpu_profile(int enable) {
+  if (!L) return OCFD_ERR_STATE;
+  L->prof = enable != 0;
+  for (int c = 0; c < KC_NUM; c++) { L->kc_ms[c] = 0; L->kc_n[c] = 0; }
+  return 0;
+}
+int ocfd_gpu_profile_read(int cls, double* ms, long long* count) {
+  if (!L || cls < 0 || cls >= KC_NUM) return OCFD_ERR_PARAM;
+  *ms = L->kc_ms[cls];
+  *count = L->kc_n[cls];
+  return 0;
+}
+const char* ocfd_gpu_profile_name(int cls) { return (cls >= 0 && cls < KC_NUM) ? kc_names[cls] : ""; }
+int ocfd_gpu_profile_nclass(void) { return KC_NUM; }
+void* ocfd_gpu_stream(void) { return L ? (void*)L->st : nullptr; }
+long long ocfd_gpu_launch_count(void) { return L ? (long long)L->launches : 0; }
+int ocfd_gpu_is_separable(void) { return L && L->sep ? 1 : 0; }
+
+double ocfd_gpu_fp64_peak_gflops(void) {
+  double r = -1.0;
+  guarded([&]() -> int {
+    int dev = 0, sms = 0;
+    CK(cudaGetDevice(&dev));
+    CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    double* out;
+    CK(cudaMalloc(&out, sizeof(double)));
+    cudaEvent_t a, b;
+    CK(cudaEventCreate(&a));
+    CK(cudaEventCreate(&b));
+    const int iters = 1 << 14, blocks = sms * 8, threads = 256;
+    k_fp64_peak<<<blocks, threads>>>(out, 64, 1.0000001, 1e-9);  // warm-up
+    CK(cudaEventRecord(a));
+    k_fp64_peak<<<blocks, threads>>>(out, iters, 1.0000001, 1e-9);
+    CK(cudaEventRecord(b));
+    CK(cudaEventSynchronize(b));
+    float ms = 0;
+    CK(cudaEventElapsedTime(&ms, a, b));
+    r = 2.0 * 8.0 * (double)iters * blocks * threads / (ms * 1e-3) / 1e9;
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    cudaFree(out);
+    return 0;
+  });
+  return r;
+}
+
+const char* ocfd_gpu_last_error(void) { return g_err.c_str(); }
+
+int ocfd_gpu_finalize(void) {
+  release();
+  return 0;
+}
+
+}  // extern "C"

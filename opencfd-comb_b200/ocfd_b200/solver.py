@@ -1,0 +1,174 @@
+"""Host-side mirror of the reference's hot-path interface, backed by libocfd_gpu.so.
+
+The reference's Fortran driver (code/flow-solver/OCFD_NS_Solver.f90) calls, per time step,
+flow_time_advance(dt/2), Chemical_time_advance(dt/Chemical_sub_step) x Chemical_sub_step +
+comput_T_P, and flow_time_advance(dt/2); show_flow_msg reduces mean energies. This class
+offers the same calls (same names, argument meaning and error behaviour: a failing call raises,
+as the reference stops) over the C ABI of include/ocfd_gpu.h. There is no CPU fallback: if the
+CUDA library or a device is missing, construction fails.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+from . import abi
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIBPATH = os.path.join(HERE, "libocfd_gpu.so")
+
+_lib = None
+
+
+class OcfdError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__("OpenCFD-Comb GPU error %d: %s" % (code, msg))
+        self.code = code
+
+
+def lib():
+    """Loads libocfd_gpu.so (built by `make -C opencfd-comb_b200`)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIBPATH):
+            raise OcfdError(abi.ERR_CUDA, "libocfd_gpu.so is not built (run make -C opencfd-comb_b200)")
+        L = C.CDLL(LIBPATH)
+        for name, (res, args) in abi.GPU_SIGNATURES.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        extra = {
+            "ocfd_gpu_init_state": (C.c_int, [abi.PD, abi.PD, C.c_double]),
+            "ocfd_gpu_chem_setup": (C.c_int, [C.POINTER(abi.Thermo), C.POINTER(abi.Kinetics), C.c_int, C.c_int]),
+            "ocfd_gpu_profile": (C.c_int, [C.c_int]),
+            "ocfd_gpu_profile_read": (C.c_int, [C.c_int, abi.PD, C.POINTER(C.c_longlong)]),
+            "ocfd_gpu_profile_name": (C.c_char_p, [C.c_int]),
+            "ocfd_gpu_profile_nclass": (C.c_int, []),
+            "ocfd_gpu_stream": (C.c_void_p, []),
+            "ocfd_gpu_launch_count": (C.c_longlong, []),
+            "ocfd_gpu_is_separable": (C.c_int, []),
+        }
+        for name, (res, args) in extra.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+def _chk(rc):
+    if rc != 0:
+        raise OcfdError(rc, lib().ocfd_gpu_last_error().decode())
+
+
+class Solver:
+    """One grid, one GPU, one stream (the reference's single MPI rank)."""
+
+    def __init__(self, case, metrics=None):
+        L = lib()
+        self.case = case
+        bc = case.bcdata()
+        _chk(L.ocfd_gpu_init(C.byref(case.params), C.byref(case.thermo),
+                             C.byref(case.kin) if case.kin is not None else None, C.byref(case.trans),
+                             C.byref(bc) if bc is not None else None, abi.dptr(case.coords), abi.dptr(metrics)))
+        self.tt = 0.0
+        self.istep = 0
+
+    # ---- start-up (OCFD_NS_Solver.f90:15-18) ----
+    def init_state(self, tt=0.0):
+        c = self.case
+        _chk(lib().ocfd_gpu_init_state(abi.dptr(c.prim5), abi.dptr(c.di), tt))
+        self.tt = tt
+
+    def upload_state(self, f, di, prims):
+        _chk(lib().ocfd_gpu_upload_state(abi.dptr(f), abi.dptr(di), abi.dptr(prims)))
+
+    # ---- the hot path ----
+    def flow_time_advance(self, dt1, tt=None):
+        _chk(lib().ocfd_gpu_flow_advance(dt1, self.tt if tt is None else tt))
+
+    def chemical_time_advance(self, dt2, nsub=1):
+        """nsub x Chemical_time_advance(dt2) followed by comput_T_P."""
+        _chk(lib().ocfd_gpu_chem_advance(dt2, nsub))
+
+    def step(self, dt, if_reaction=0, nsub=1):
+        """One NS_solver time step (OCFD_NS_Solver.f90:28-46) as a replayed CUDA graph."""
+        _chk(lib().ocfd_gpu_step(dt, self.tt, if_reaction, nsub))
+        self.istep += 1
+        self.tt += dt
+
+    def show_flow_msg(self):
+        """Mean total energy and kinetic energy (OCFD_Time_Adv.f90:210-223)."""
+        e, k = C.c_double(), C.c_double()
+        _chk(lib().ocfd_gpu_diag(C.byref(e), C.byref(k)))
+        return e.value, k.value
+
+    # ---- state transfer ----
+    def download_state(self):
+        c = self.case
+        nx, ny, nz = c.shape
+        hs = c.halo_shape()
+        f = np.empty((5, nz, ny, nx))
+        di = np.empty((c.params.n_spec,) + hs)
+        prims = np.empty((7,) + hs)
+        _chk(lib().ocfd_gpu_download_state(abi.dptr(f), abi.dptr(di), abi.dptr(prims)))
+        return f, di, prims
+
+    def rhybrid(self):
+        r = np.empty(self.case.halo_shape())
+        _chk(lib().ocfd_gpu_download_rhybrid(abi.dptr(r)))
+        return r
+
+    def metrics(self):
+        m = np.empty((10,) + self.case.halo_shape())
+        _chk(lib().ocfd_gpu_download_metrics(abi.dptr(m)))
+        return m
+
+    def stats(self):
+        a, b = C.c_longlong(), C.c_longlong()
+        _chk(lib().ocfd_gpu_stats(C.byref(a), C.byref(b)))
+        return a.value, b.value
+
+    # ---- measurement helpers ----
+    @staticmethod
+    def profile(enable):
+        lib().ocfd_gpu_profile(1 if enable else 0)
+
+    @staticmethod
+    def profile_read():
+        L = lib()
+        out = {}
+        for c in range(L.ocfd_gpu_profile_nclass()):
+            ms, n = C.c_double(), C.c_longlong()
+            L.ocfd_gpu_profile_read(c, C.byref(ms), C.byref(n))
+            out[L.ocfd_gpu_profile_name(c).decode()] = (ms.value, n.value)
+        return out
+
+    @staticmethod
+    def stream():
+        return lib().ocfd_gpu_stream()
+
+    @staticmethod
+    def launch_count():
+        return lib().ocfd_gpu_launch_count()
+
+    def close(self):
+        lib().ocfd_gpu_finalize()
+
+
+def chem_setup(thermo, kin, realgas=1, timeadv=abi.CHEM_IMPLICIT):
+    _chk(lib().ocfd_gpu_chem_setup(C.byref(thermo), C.byref(kin), realgas, timeadv))
+
+
+def chem_batch(di, e, dt, nsub=None):
+    """Batched 0-D reactors (host arrays, updated in place): di (n, Ns), e (n), dt (n), nsub (n) int32."""
+    _chk(lib().ocfd_gpu_chem_batch(len(e), abi.dptr(di), abi.dptr(e), abi.dptr(dt), abi.iptr(nsub)))
+
+
+def chem_batch_device(n, di_ptr, e_ptr, dt_ptr, nsub_ptr):
+    """Same on device pointers (e.g. torch tensors' data_ptr())."""
+    _chk(lib().ocfd_gpu_chem_batch_device(n, di_ptr, e_ptr, dt_ptr, nsub_ptr))
+
+
+def fp64_peak_gflops():
+    return lib().ocfd_gpu_fp64_peak_gflops()
