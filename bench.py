@@ -44,6 +44,7 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=5)
+    ap.add_argument("--nz", type=int, default=128, help="spanwise cells of the flat-plate workload (128 = full)")
     return ap.parse_args()
 
 
@@ -197,7 +198,7 @@ def main_ours(a):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item())
 
-    c, name = make_case(a.workload)
+    c, name = make_case(a.workload, nz=a.nz)
     g = solver.Solver(c)
     g.init_state()
     dt = c.dt

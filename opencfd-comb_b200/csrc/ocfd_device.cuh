@@ -62,12 +62,17 @@ __constant__ DevConst cC;
 extern __constant__ DevConst cC;
 #endif
 
-// geometry: either 19 full metric arrays or three 1-D derivative arrays (tensor-product grids)
+// geometry: either 19 full metric arrays or, for tensor-product grids, three 1-D derivative
+// arrays plus the cross derivatives that the one-sided closures of OCFD_dx0/dy0/dz0 leave at the
+// non-periodic end planes (e.g. (-3y+4y-y)/(2h) at i = 1 is a rounding residue, not zero).
 struct Geo {
   const double* m[19];   // Akx,Aky,Akz,Aix,Aiy,Aiz,Asx,Asy,Asz,Ajac,Akx1..Asz1 (halo layout)
   const double* d1[3];   // dx/dxi(i), dy/deta(j), dz/dzeta(k), halo-inclusive, index s+L-1
+  const double* e[6];    // cross terms at the end planes, [side][index+L-1]:
+                         //   yi(j), zi(k) at i=1|nx; xj(i), zj(k) at j=1|ny; xk(i), yk(j) at k=1|nz
 };
 enum { G_AKX = 0, G_AKY, G_AKZ, G_AIX, G_AIY, G_AIZ, G_ASX, G_ASY, G_ASZ, G_AJAC, G_AKX1 };
+enum { E_YI = 0, E_ZI, E_XJ, E_ZJ, E_XK, E_YK };
 
 __device__ __forceinline__ int hidx(int i, int j, int k) {
   return (i + OCFD_L - 1) + cC.HX * ((j + OCFD_L - 1) + cC.HY * (k + OCFD_L - 1));
@@ -93,19 +98,84 @@ __device__ __forceinline__ double powi_rt(double x, int m) {
 __device__ __forceinline__ double fsgn(double x) { return signbit(x) ? -1.0 : 1.0; }
 
 // ---------------------------------------------------------------- metrics
-// Separable (1-D grid) metrics: the Jacobian formula of comput_Jacobian3d with all cross
-// derivatives exactly zero reduces to these products (OCFD_mesh.f90:88-98).
+// comput_Jacobian3d (OCFD_mesh.f90:88-98) from the nine coordinate derivatives; for a separable
+// grid the cross derivatives are zero except on the non-periodic end planes, where the closure
+// residues are looked up, so every point reproduces the reference's 3-D arrays exactly.
+__device__ __forceinline__ void sep_derivs(const Geo& g, int i, int j, int k, double& xi, double& yi, double& zi,
+                                           double& xj, double& yj, double& zj, double& xk, double& yk, double& zk,
+                                           bool& cross) {
+  const int L = OCFD_L;
+  xi = g.d1[0][i + L - 1];
+  yj = g.d1[1][j + L - 1];
+  zk = g.d1[2][k + L - 1];
+  yi = zi = xj = zj = xk = yk = 0.0;
+  const bool bx = !cC.iper[0] && (i == 1 || i == cC.nx);
+  const bool by = !cC.iper[1] && (j == 1 || j == cC.ny);
+  const bool bz = !cC.iper[2] && (k == 1 || k == cC.nz);
+  cross = bx || by || bz;
+  if (bx) {
+    int s = i == 1 ? 0 : 1;
+    yi = g.e[E_YI][s * (cC.ny + 2 * L) + j + L - 1];
+    zi = g.e[E_ZI][s * (cC.nz + 2 * L) + k + L - 1];
+  }
+  if (by) {
+    int s = j == 1 ? 0 : 1;
+    xj = g.e[E_XJ][s * (cC.nx + 2 * L) + i + L - 1];
+    zj = g.e[E_ZJ][s * (cC.nz + 2 * L) + k + L - 1];
+  }
+  if (bz) {
+    int s = k == 1 ? 0 : 1;
+    xk = g.e[E_XK][s * (cC.nx + 2 * L) + i + L - 1];
+    yk = g.e[E_YK][s * (cC.ny + 2 * L) + j + L - 1];
+  }
+}
+// halo points the reference never fills (non-periodic face halos, edges, corners) keep
+// allocate_flow_data's 1.0 in every metric array; they enter the split flux when a face uses
+// Scheme_boundary = -1 or 1
+__device__ __forceinline__ bool metric_unfilled(int i, int j, int k) {
+  const bool ox = i < 1 || i > cC.nx, oy = j < 1 || j > cC.ny, oz = k < 1 || k > cC.nz;
+  const int n = (int)ox + (int)oy + (int)oz;
+  return n > 1 || (ox && !cC.iper[0]) || (oy && !cC.iper[1]) || (oz && !cC.iper[2]);
+}
+__device__ __forceinline__ void jac_full(double xi1, double yi1, double zi1, double xj1, double yj1, double zj1,
+                                         double xk1, double yk1, double zk1, double* a, double& jac) {
+  jac = 1.0 / (xi1 * yj1 * zk1 + yi1 * zj1 * xk1 + zi1 * xj1 * yk1 - zi1 * yj1 * xk1 - yi1 * xj1 * zk1 -
+               xi1 * zj1 * yk1);
+  a[0] = jac * (yj1 * zk1 - zj1 * yk1);
+  a[1] = jac * (zj1 * xk1 - xj1 * zk1);
+  a[2] = jac * (xj1 * yk1 - yj1 * xk1);
+  a[3] = jac * (yk1 * zi1 - zk1 * yi1);
+  a[4] = jac * (zk1 * xi1 - xk1 * zi1);
+  a[5] = jac * (xk1 * yi1 - yk1 * xi1);
+  a[6] = jac * (yi1 * zj1 - zi1 * yj1);
+  a[7] = jac * (zi1 * xj1 - xi1 * zj1);
+  a[8] = jac * (xi1 * yj1 - yi1 * xj1);
+}
 template <bool SEP>
 __device__ __forceinline__ void metric_dir(const Geo& g, int dir, int i, int j, int k, int q, double& A1, double& A2,
                                            double& A3) {
   if (SEP) {
-    double xi = g.d1[0][i + OCFD_L - 1], yj = g.d1[1][j + OCFD_L - 1], zk = g.d1[2][k + OCFD_L - 1];
-    double jac = 1.0 / (xi * yj * zk);
-    double a = dir == 0 ? jac * (yj * zk) : (dir == 1 ? jac * (zk * xi) : jac * (xi * yj));
-    double d = a / jac;
-    A1 = dir == 0 ? d : 0.0;
-    A2 = dir == 1 ? d : 0.0;
-    A3 = dir == 2 ? d : 0.0;
+    if (metric_unfilled(i, j, k)) {
+      A1 = A2 = A3 = 1.0;
+      return;
+    }
+    double xi, yi, zi, xj, yj, zj, xk, yk, zk;
+    bool cross;
+    sep_derivs(g, i, j, k, xi, yi, zi, xj, yj, zj, xk, yk, zk, cross);
+    if (!cross) {
+      double jac = 1.0 / (xi * yj * zk);
+      double a = dir == 0 ? jac * (yj * zk) : (dir == 1 ? jac * (zk * xi) : jac * (xi * yj));
+      double d = a / jac;
+      A1 = dir == 0 ? d : 0.0;
+      A2 = dir == 1 ? d : 0.0;
+      A3 = dir == 2 ? d : 0.0;
+    } else {
+      double a[9], jac;
+      jac_full(xi, yi, zi, xj, yj, zj, xk, yk, zk, a, jac);
+      A1 = a[3 * dir] / jac;
+      A2 = a[3 * dir + 1] / jac;
+      A3 = a[3 * dir + 2] / jac;
+    }
   } else {
     A1 = __ldg(g.m[G_AKX1 + 3 * dir] + q);
     A2 = __ldg(g.m[G_AKX1 + 3 * dir + 1] + q);
@@ -115,8 +185,14 @@ __device__ __forceinline__ void metric_dir(const Geo& g, int dir, int i, int j, 
 template <bool SEP>
 __device__ __forceinline__ double metric_jac(const Geo& g, int i, int j, int k, int q) {
   if (SEP) {
-    double xi = g.d1[0][i + OCFD_L - 1], yj = g.d1[1][j + OCFD_L - 1], zk = g.d1[2][k + OCFD_L - 1];
-    return 1.0 / (xi * yj * zk);
+    if (metric_unfilled(i, j, k)) return 1.0;
+    double xi, yi, zi, xj, yj, zj, xk, yk, zk;
+    bool cross;
+    sep_derivs(g, i, j, k, xi, yi, zi, xj, yj, zj, xk, yk, zk, cross);
+    if (!cross) return 1.0 / (xi * yj * zk);
+    double a[9], jac;
+    jac_full(xi, yi, zi, xj, yj, zj, xk, yk, zk, a, jac);
+    return jac;
   }
   return __ldg(g.m[G_AJAC] + q);
 }
@@ -124,13 +200,27 @@ __device__ __forceinline__ double metric_jac(const Geo& g, int i, int j, int k, 
 template <bool SEP>
 __device__ __forceinline__ void metric_all(const Geo& g, int i, int j, int k, int q, double* a, double* a1) {
   if (SEP) {
-    double xi = g.d1[0][i + OCFD_L - 1], yj = g.d1[1][j + OCFD_L - 1], zk = g.d1[2][k + OCFD_L - 1];
-    double jac = 1.0 / (xi * yj * zk);
-    double akx = jac * (yj * zk), aiy = jac * (zk * xi), asz = jac * (xi * yj);
+    if (metric_unfilled(i, j, k)) {
 #pragma unroll
-    for (int m = 0; m < 9; m++) { a[m] = 0.0; a1[m] = 0.0; }
-    a[0] = akx; a[4] = aiy; a[8] = asz;
-    a1[0] = akx / jac; a1[4] = aiy / jac; a1[8] = asz / jac;
+      for (int m = 0; m < 9; m++) { a[m] = 1.0; a1[m] = 1.0; }
+      return;
+    }
+    double xi, yi, zi, xj, yj, zj, xk, yk, zk;
+    bool cross;
+    sep_derivs(g, i, j, k, xi, yi, zi, xj, yj, zj, xk, yk, zk, cross);
+    if (!cross) {
+      double jac = 1.0 / (xi * yj * zk);
+      double akx = jac * (yj * zk), aiy = jac * (zk * xi), asz = jac * (xi * yj);
+#pragma unroll
+      for (int m = 0; m < 9; m++) { a[m] = 0.0; a1[m] = 0.0; }
+      a[0] = akx; a[4] = aiy; a[8] = asz;
+      a1[0] = akx / jac; a1[4] = aiy / jac; a1[8] = asz / jac;
+    } else {
+      double jac;
+      jac_full(xi, yi, zi, xj, yj, zj, xk, yk, zk, a, jac);
+#pragma unroll
+      for (int m = 0; m < 9; m++) a1[m] = a[m] / jac;
+    }
   } else {
 #pragma unroll
     for (int m = 0; m < 9; m++) {

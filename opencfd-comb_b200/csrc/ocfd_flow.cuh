@@ -643,7 +643,7 @@ struct BcArgs {
   double *f, *d, *u, *v, *w, *T, *p, *Et, *di;
   const double *inlet, *upper, *wall_pertb;
   const int* nonref;
-  int inlet_kind, upper_kind, outlet;
+  int inlet_kind, upper_kind, outlet, jet_iflag;
   double ht, Tw, xinit, disA;
   const double* X;  // Axx (halo array) for the wall start
   Geo g;
@@ -738,6 +738,51 @@ __global__ void k_bc_outlet(BcArgs a) {
       a.di[(size_t)m * cC.H + q] = 2.0 * a.di[(size_t)m * cC.H + q1] - a.di[(size_t)m * cC.H + q2];
   }
 }
+// ocfd_bc_jet inlet (OCFD_BC_jet.f90:21-75): 2-D table; Iflag_inlet 0 = Dirichlet, 1 = keep the
+// interior pressure where the inflow is subsonic (u < c)
+template <int NS>
+__global__ void k_bc_jet_inlet(BcArgs a) {
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= cC.ny * cC.nz) return;
+  int j = t % cC.ny + 1, k = t / cC.ny + 1;
+  int q = hidx(1, j, k);
+  double vals[5 + NS];
+  for (int c = 0; c < 5 + NS; c++) vals[c] = a.inlet[((size_t)c * cC.nz + (k - 1)) * cC.ny + (j - 1)];
+  if (a.jet_iflag == 0) {
+    set_point<NS>(a, q, vals);
+    return;
+  }
+  a.u[q] = vals[1]; a.v[q] = vals[2]; a.w[q] = vals[3]; a.T[q] = vals[4];
+  double T1 = vals[4], d1 = vals[0], di1[NS], ai1[NS], d0 = 0.0;
+  for (int m = 0; m < NS; m++) { di1[m] = vals[5 + m]; d0 = d0 + di1[m]; }
+  for (int m = 0; m < NS; m++) ai1[m] = di1[m] / d0;
+  double p1 = dev_P<NS>(di1, T1);
+  double Et1 = dev_E<NS>(di1, T1);
+  double gamma = p1 / Et1 + 1.0;
+  double c1 = sqrt(gamma * p1 / d1);
+  if (vals[1] < c1) {
+    double pp = a.p[hidx(2, j, k)];
+    a.p[q] = pp;
+    double dn = dev_dens<NS>(ai1, T1, pp);
+    a.d[q] = dn;
+    for (int m = 0; m < NS; m++) a.di[(size_t)m * cC.H + q] = dn * ai1[m];
+  } else {
+    a.d[q] = d1;
+    for (int m = 0; m < NS; m++) a.di[(size_t)m * cC.H + q] = di1[m];
+  }
+}
+// ocfd_bc_jet outlet (:77-93): zeroth-order extrapolation of every primitive
+template <int NS>
+__global__ void k_bc_jet_outlet(BcArgs a) {
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= cC.ny * cC.nz) return;
+  int j = t % cC.ny + 1, k = t / cC.ny + 1;
+  int q = hidx(cC.nx, j, k), q1 = hidx(cC.nx - 1, j, k);
+  a.d[q] = a.d[q1]; a.u[q] = a.u[q1]; a.v[q] = a.v[q1]; a.w[q] = a.w[q1]; a.T[q] = a.T[q1];
+  a.p[q] = a.p[q1]; a.Et[q] = a.Et[q1];
+  for (int m = 0; m < NS; m++) a.di[(size_t)m * cC.H + q] = a.di[(size_t)m * cC.H + q1];
+}
+
 // OCFD_bc lines 33-184: every domain-face cell gets di re-scaled, Et and p re-derived from T and
 // f rebuilt, once per face it lies on (edges twice, corners three times, as the sequential face
 // loops of the reference do). group 0: i faces; 1: j faces without i faces; 2: k faces only.

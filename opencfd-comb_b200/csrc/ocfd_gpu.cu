@@ -53,7 +53,7 @@ struct Lib {
   double *f = nullptr, *fn = nullptr, *du = nullptr, *d = nullptr, *u = nullptr, *v = nullptr, *w = nullptr,
          *T = nullptr, *p = nullptr, *Et[2] = {nullptr, nullptr}, *di = nullptr, *din = nullptr, *Rh = nullptr;
   double *ev[12] = {}, *amu = nullptr, *amk = nullptr, *amd = nullptr, *qp[3] = {}, *ci = nullptr, *se[3] = {};
-  double *X = nullptr, *Y = nullptr, *Z = nullptr, *met[19] = {}, *d1[3] = {}, *partial = nullptr;
+  double *X = nullptr, *Y = nullptr, *Z = nullptr, *met[19] = {}, *d1[3] = {}, *edge[6] = {}, *partial = nullptr;
   double *inlet = nullptr, *upper = nullptr, *wall = nullptr, *ht_dev = nullptr;
   int *nonref = nullptr, *patches = nullptr;
   int npatch = 0;
@@ -201,6 +201,7 @@ BcArgs bc_args() {
   a.di = L->di;
   a.inlet = L->inlet; a.upper = L->upper; a.wall_pertb = L->wall; a.nonref = L->nonref;
   a.inlet_kind = L->inlet_kind; a.upper_kind = L->upper_kind; a.outlet = L->outlet;
+  a.jet_iflag = (int)std::lround(L->P.bc_para[0]);
   a.Tw = L->P.bc_para[4]; a.xinit = L->P.bc_para[5]; a.disA = L->P.bc_para[7];
   a.ht = 0.0;
   a.X = L->X;
@@ -233,6 +234,13 @@ void ocfd_bc_t() {
       k_bc_outlet<NS><<<nblk((long long)ny * nz, 128), 128, 0, L->st>>>(a);
       LAUNCH_CHECK();
     }
+  }
+  if (L->P.ibc == OCFD_BC_JET) {
+    KTimer t(KC_BC);
+    k_bc_jet_inlet<NS><<<nblk((long long)ny * nz, 128), 128, 0, L->st>>>(a);
+    LAUNCH_CHECK();
+    k_bc_jet_outlet<NS><<<nblk((long long)ny * nz, 128), 128, 0, L->st>>>(a);
+    LAUNCH_CHECK();
   }
   {
     KTimer t(KC_BC);
@@ -610,6 +618,58 @@ __global__ void k_metric1d_halo(double* dx, double* dy, double* dz) {
     }
   }
 }
+// cross derivatives of the coordinates on the non-periodic end planes (closure residues)
+__global__ void k_metric_edges(const double* X, const double* Y, const double* Z, double* const* e) {
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int L = OCFD_L, nx = cC.nx, ny = cC.ny, nz = cC.nz;
+  for (int s = 0; s < 2; s++) {
+    int is = s ? nx : 1, js = s ? ny : 1, ks = s ? nz : 1;
+    if (t < ny) e[E_YI][s * (ny + 2 * L) + t + L] = cdiff(Y, hidx(is, t + 1, 1), 0, is, nx);
+    if (t < nz) e[E_ZI][s * (nz + 2 * L) + t + L] = cdiff(Z, hidx(is, 1, t + 1), 0, is, nx);
+    if (t < nx) e[E_XJ][s * (nx + 2 * L) + t + L] = cdiff(X, hidx(t + 1, js, 1), 1, js, ny);
+    if (t < nz) e[E_ZJ][s * (nz + 2 * L) + t + L] = cdiff(Z, hidx(1, js, t + 1), 1, js, ny);
+    if (t < nx) e[E_XK][s * (nx + 2 * L) + t + L] = cdiff(X, hidx(t + 1, 1, ks), 2, ks, nz);
+    if (t < ny) e[E_YK][s * (ny + 2 * L) + t + L] = cdiff(Y, hidx(1, t + 1, ks), 2, ks, nz);
+  }
+}
+__global__ void k_metric_edges_halo(double* const* e) {
+  int l = threadIdx.x;
+  const int L = OCFD_L;
+  if (l >= L) return;
+  const int dir[6] = {1, 2, 0, 2, 0, 1};  // the index direction of each end-plane array
+  const int n[3] = {cC.nx, cC.ny, cC.nz};
+  for (int m = 0; m < 6; m++)
+    for (int s = 0; s < 2; s++) {
+      int d = dir[m], nn = n[d];
+      double* a = e[m] + s * (nn + 2 * L);
+      if (cC.iper[d]) {
+        a[l] = a[nn + l];
+        a[nn + L + l] = a[L + l];
+      } else {
+        a[l] = 0.0;
+        a[nn + L + l] = 0.0;
+      }
+    }
+}
+// the ten reference metric arrays from the separable representation (for downloads); halo
+// points the reference never fills keep allocate_flow_data's 1.0
+__global__ void k_expand_metrics(Geo g, double* out, long long H) {
+  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= H) return;
+  int i = (int)(t % cC.HX) - OCFD_L + 1;
+  int j = (int)((t / cC.HX) % cC.HY) - OCFD_L + 1;
+  int k = (int)(t / cC.HX / cC.HY) - OCFD_L + 1;
+  bool ox = i < 1 || i > cC.nx, oy = j < 1 || j > cC.ny, oz = k < 1 || k > cC.nz;
+  (void)ox; (void)oy; (void)oz;
+  if (metric_unfilled(i, j, k)) {
+    for (int m = 0; m < 10; m++) out[m * H + t] = 1.0;
+    return;
+  }
+  double a[9], a1[9];
+  metric_all<true>(g, i, j, k, (int)t, a, a1);
+  for (int m = 0; m < 9; m++) out[m * H + t] = a[m];
+  out[9 * H + t] = metric_jac<true>(g, i, j, k, (int)t);
+}
 // FP64 FMA throughput probe: eight independent chains per thread, registers only
 __global__ void k_fp64_peak(double* out, int iters, double a, double b) {
   double x0 = threadIdx.x, x1 = x0 + 1, x2 = x0 + 2, x3 = x0 + 3, x4 = x0 + 4, x5 = x0 + 5, x6 = x0 + 6, x7 = x0 + 7;
@@ -635,10 +695,15 @@ int validate(const ocfd_params* p) {
   if (!(p->flux_splitting == 1 || p->flux_splitting == 2)) return bad("Flux_Splitting must be 1 or 2");
   for (int m = 0; m < 6; m++) {
     if (p->scheme_boundary[m] < -1 || p->scheme_boundary[m] > 1) return bad("Scheme_boundary must be -1, 0 or 1");
-    if (p->ghost_cell[m] < 0 || p->ghost_cell[m] > 2) return bad("Ghost_Cell must be 0, 1 or 2");
+    if (p->ghost_cell[m] != 0) {
+      // ghost cells need the Jacobian ghost extension of init_mesh (Jac_Ghost_boundary,
+      // OCFD_GhostCell.f90:1-160, 366-580) as well as the flow extrapolation; not built
+      g_err = "Ghost_Cell != 0 is not built";
+      return OCFD_ERR_UNSUPPORTED;
+    }
   }
   if (p->if_scheme_character != 0) { g_err = "IF_Scheme_Character=1 (characteristic flux) is not built"; return OCFD_ERR_UNSUPPORTED; }
-  if (!(p->ibc == OCFD_BC_NONE || p->ibc == OCFD_BC_BOUNDARYLAYER)) { g_err = "boundary condition not built (BC_NONE, BC_BOUNDARYLAYER)"; return OCFD_ERR_UNSUPPORTED; }
+  if (!(p->ibc == OCFD_BC_NONE || p->ibc == OCFD_BC_BOUNDARYLAYER || p->ibc == OCFD_BC_JET)) { g_err = "boundary condition not built (BC_NONE, BC_BOUNDARYLAYER, BC_JET)"; return OCFD_ERR_UNSUPPORTED; }
   if (p->wall_catalysis != 0) return bad("only non-catalytic walls");
   if (!(p->chem_timeadv == 1 || p->chem_timeadv == 2 || p->chem_timeadv == 3 || p->chem_timeadv == -1)) return bad("CHEM_TimeAdv must be 1, 2, 3 or -1");
   return 0;
@@ -670,6 +735,7 @@ void set_geo_device_ptrs() {
   Geo& g = L->geo;
   for (int m = 0; m < 19; m++) g.m[m] = L->met[m];
   for (int m = 0; m < 3; m++) g.d1[m] = L->d1[m];
+  for (int m = 0; m < 6; m++) g.e[m] = L->edge[m];
 }
 
 }  // namespace
@@ -684,7 +750,7 @@ int ocfd_gpu_init(const ocfd_params* p, const ocfd_thermo* th, const ocfd_kineti
     int e = validate(p);
     if (e) return e;
     if (th->n_spec != p->n_spec) { g_err = "thermo n_spec differs from N_SPEC"; return OCFD_ERR_PARAM; }
-    if (p->ibc == OCFD_BC_BOUNDARYLAYER && !bc) { g_err = "BC_BOUNDARYLAYER needs boundary data"; return OCFD_ERR_PARAM; }
+    if ((p->ibc == OCFD_BC_BOUNDARYLAYER || p->ibc == OCFD_BC_JET) && !bc) { g_err = "BC_BOUNDARYLAYER / BC_JET need boundary data"; return OCFD_ERR_PARAM; }
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) { g_err = "no CUDA device"; return OCFD_ERR_CUDA; }
     L = new Lib();
@@ -750,6 +816,8 @@ int ocfd_gpu_init(const ocfd_params* p, const ocfd_thermo* th, const ocfd_kineti
     for (int m = 0; m < 3; m++) add(H, 8);
     if (!L->sep) for (int m = 0; m < 19; m++) add(H, 8);
     for (int m = 0; m < 3; m++) add(nn[m] + 2 * OCFD_L, 8);
+    for (int m = 0; m < 6; m++) add(2 * (std::max(nn[0], std::max(nn[1], nn[2])) + 2 * OCFD_L), 8);
+    add(6, sizeof(double*));
     add(2 * ((N + 255) / 256) + 2, 8);
     size_t nv = 5 + NS;
     add(nv * (size_t)std::max((long long)p->ny * p->nz, (long long)p->nx * p->nz) + nv, 8);
@@ -775,6 +843,9 @@ int ocfd_gpu_init(const ocfd_params* p, const ocfd_thermo* th, const ocfd_kineti
     L->X = alloc<double>(H); L->Y = alloc<double>(H); L->Z = alloc<double>(H);
     if (!L->sep) for (int m = 0; m < 19; m++) L->met[m] = alloc<double>(H);
     for (int m = 0; m < 3; m++) L->d1[m] = alloc<double>(nn[m] + 2 * OCFD_L);
+    const int emax = std::max(nn[0], std::max(nn[1], nn[2])) + 2 * OCFD_L;
+    for (int m = 0; m < 6; m++) L->edge[m] = alloc<double>(2 * emax);
+    double** edge_ptrs = alloc<double*>(6);
     L->partial = alloc<double>(2 * ((N + 255) / 256) + 2);
     L->inlet = alloc<double>(nv * (size_t)std::max((long long)p->ny * p->nz, (long long)p->nx * p->nz) + nv);
     L->upper = alloc<double>(nv * (size_t)std::max((long long)p->ny * p->nz, (long long)p->nx * p->nz) + nv);
@@ -823,6 +894,11 @@ int ocfd_gpu_init(const ocfd_params* p, const ocfd_thermo* th, const ocfd_kineti
       k_metric1d<<<nblk(mx, 128), 128, 0, L->st>>>(L->X, L->Y, L->Z, L->d1[0], L->d1[1], L->d1[2]);
       LAUNCH_CHECK();
       k_metric1d_halo<<<1, 32, 0, L->st>>>(L->d1[0], L->d1[1], L->d1[2]);
+      LAUNCH_CHECK();
+      CK(cudaMemcpyAsync(edge_ptrs, L->edge, sizeof(double*) * 6, cudaMemcpyHostToDevice, L->st));
+      k_metric_edges<<<nblk(mx, 128), 128, 0, L->st>>>(L->X, L->Y, L->Z, edge_ptrs);
+      LAUNCH_CHECK();
+      k_metric_edges_halo<<<1, 32, 0, L->st>>>(edge_ptrs);
       LAUNCH_CHECK();
     } else {
       L->sep = false;
@@ -878,6 +954,11 @@ int ocfd_gpu_init(const ocfd_params* p, const ocfd_thermo* th, const ocfd_kineti
           nr[(i - 1) + (size_t)p->nx * (k - 1)] = val;
         }
       CK(cudaMemcpy(L->nonref, nr.data(), sizeof(int) * nr.size(), cudaMemcpyHostToDevice));
+    }
+    if (p->ibc == OCFD_BC_JET) {  // ocfd_bc_jet: BcData_inlet = 2, no upper data
+      L->inlet_kind = 2;
+      L->upper_kind = -1;
+      CK(cudaMemcpyAsync(L->inlet, bc->inlet, sizeof(double) * nv * p->ny * p->nz, cudaMemcpyHostToDevice, L->st));
     }
     // hybrid forced patches (Hybrid_para(4..), OCFD_SetHybrid.f90:80-102)
     if (p->scheme_invis == OCFD_SCHEME_HYBRID) {
@@ -1127,33 +1208,13 @@ int ocfd_gpu_download_metrics(double* m) {
     if (!L || !L->d) { g_err = "ocfd_gpu_init first"; return OCFD_ERR_STATE; }
     const long long H = L->hc.H;
     if (L->sep) {
-      // expand the separable metrics to the reference's ten 3-D arrays (interior + periodic halo)
-      int nn[3] = {L->P.nx, L->P.ny, L->P.nz};
-      std::vector<double> d1[3];
-      for (int dd = 0; dd < 3; dd++) {
-        d1[dd].resize(nn[dd] + 2 * OCFD_L);
-        CK(cudaMemcpy(d1[dd].data(), L->d1[dd], sizeof(double) * d1[dd].size(), cudaMemcpyDeviceToHost));
-      }
-      const int L4 = OCFD_L;
-      long long HX = L->hc.HX, HY = L->hc.HY;
-      for (int mm = 0; mm < 10; mm++) std::fill(m + mm * H, m + (mm + 1) * H, 1.0);
-      for (int k = 1 - L4; k <= nn[2] + L4; k++)
-        for (int j = 1 - L4; j <= nn[1] + L4; j++)
-          for (int i = 1 - L4; i <= nn[0] + L4; i++) {
-            int outside = (i < 1 || i > nn[0]) + (j < 1 || j > nn[1]) + (k < 1 || k > nn[2]);
-            if (outside > 1) continue;
-            if ((i < 1 || i > nn[0]) && !L->P.iperiodic[0]) continue;
-            if ((j < 1 || j > nn[1]) && !L->P.iperiodic[1]) continue;
-            if ((k < 1 || k > nn[2]) && !L->P.iperiodic[2]) continue;
-            long long q = (i + L4 - 1) + HX * ((j + L4 - 1) + HY * (long long)(k + L4 - 1));
-            double xi = d1[0][i + L4 - 1], yj = d1[1][j + L4 - 1], zk = d1[2][k + L4 - 1];
-            double jac = 1.0 / (xi * yj * zk);
-            for (int mm = 0; mm < 9; mm++) m[mm * H + q] = 0.0;
-            m[0 * H + q] = jac * (yj * zk);
-            m[4 * H + q] = jac * (zk * xi);
-            m[8 * H + q] = jac * (xi * yj);
-            m[9 * H + q] = jac;
-          }
+      double* tmp;
+      CK(cudaMalloc(&tmp, sizeof(double) * 10 * H));
+      k_expand_metrics<<<nblk(H, 256), 256, 0, L->st>>>(L->geo, tmp, H);
+      LAUNCH_CHECK();
+      CK(cudaMemcpyAsync(m, tmp, sizeof(double) * 10 * H, cudaMemcpyDeviceToHost, L->st));
+      CK(cudaStreamSynchronize(L->st));
+      CK(cudaFree(tmp));
       return 0;
     }
     for (int mm = 0; mm < 10; mm++) CK(cudaMemcpy(m + mm * H, L->met[mm], sizeof(double) * H, cudaMemcpyDeviceToHost));

@@ -124,4 +124,19 @@ GPU_SIGNATURES = {
     "ocfd_gpu_last_error": (C.c_char_p, []),
     "ocfd_gpu_finalize": (I, []),
     "ocfd_gpu_fp64_peak_gflops": (D, []),
+    "ocfd_gpu_init_state": (I, [PD, PD, D]),
+    "ocfd_gpu_run": (I, [D, D, I, I, I]),
+    "ocfd_gpu_chem_setup": (I, [C.POINTER(Thermo), C.POINTER(Kinetics), I, I]),
+    "ocfd_gpu_profile": (I, [I]),
+    "ocfd_gpu_profile_read": (I, [I, PD, C.POINTER(C.c_longlong)]),
+    "ocfd_gpu_profile_name": (C.c_char_p, [I]),
+    "ocfd_gpu_profile_nclass": (I, []),
+    "ocfd_gpu_stream": (C.c_void_p, []),
+    "ocfd_gpu_launch_count": (C.c_longlong, []),
+    "ocfd_gpu_is_separable": (I, []),
+    "ocfd_gpu_event_record": (I, [I]),
+    "ocfd_gpu_event_elapsed": (I, [I, I, PD]),
+    "ocfd_gpu_pinned_alloc": (I, [C.c_size_t, C.POINTER(C.c_void_p)]),
+    "ocfd_gpu_pinned_free": (I, [C.c_void_p]),
+    "ocfd_gpu_step_launches": (I, []),
 }

@@ -454,3 +454,74 @@ def reactors(n=2 ** 20, seed=0, dt_sub_max=1.0e-8, nsub_max=100):
     E = energy_realgas(thermo, di.T.copy(), T)
     nsub = np.clip(np.ceil(dt / dt_sub_max), 1, nsub_max).astype(np.int32)
     return names, thermo, kin, di, np.ascontiguousarray(E), np.ascontiguousarray(dt), nsub, T
+
+
+# ---------------------------------------------------------------- C5: reacting H2 jet
+
+def _mole_to_mass(names, mi, X):
+    X = np.asarray(X, dtype=float)
+    X = X / X.sum()
+    Y = X * mi
+    return Y / Y.sum()
+
+
+def jet(nx=384, ny=256, nz=256, seed=0, D=1.0e-3, Uj=200.0, Tj=300.0, Uc=10.0, Tc=1100.0, pert=0.02,
+        lx_d=30.0, ly_d=10.0, nsteps=200, timeadv=abi.CHEM_IMPLICIT, nsub=1, iflag_inlet=1):
+    """Round H2/N2 jet (70/30 by volume, 300 K, 200 m/s, D = 1 mm, tanh-smoothed top hat) into an
+    air coflow (1100 K, 10 m/s, 1 atm); x stretched, y/z tanh-clustered toward the jet axis;
+    9-species H2-air chemistry, Wilke transport, BC_JET inflow with seeded 2 % velocity noise."""
+    names, th, kin, tr = h2air_structs()
+    ns = len(names)
+    case = Case("jet-%dx%dx%d" % (nx, ny, nz))
+    p = base_params(nx, ny, nz, ns)
+    p.ibc = abi.BC_JET
+    p.bc_para[0] = iflag_inlet
+    p.if_realgas = 1
+    p.chem_timeadv = timeadv
+    case.params = p
+    case.thermo, case.kin, case.trans = th, kin, tr
+    mi = np.array([th.mi[k] for k in range(ns)])
+    Xj = np.zeros(ns); Xj[names.index("H2")] = 0.7; Xj[names.index("N2")] = 0.3
+    Xc = np.zeros(ns); Xc[names.index("O2")] = 0.21; Xc[names.index("N2")] = 0.79
+    Yj, Yc = _mole_to_mass(names, mi, Xj), _mole_to_mass(names, mi, Xc)
+    # grids
+    s = np.arange(nx) / (nx - 1)
+    x = lx_d * D * (np.expm1(2.0 * s) / np.expm1(2.0))
+    def clustered(n, half):
+        t = np.linspace(-1.0, 1.0, n)
+        b = 1.5
+        return half * np.sinh(b * t) / np.sinh(b)
+    y = clustered(ny, 0.5 * ly_d * D)
+    z = clustered(nz, 0.5 * ly_d * D)
+    case.coords = coords_1d(x, y, z)
+    # inlet table (BcData_inlet = 2): [comp][k][j]
+    Y2, Z2 = np.meshgrid(y, z)  # (nz, ny)
+    r = np.sqrt(Y2 ** 2 + Z2 ** 2)
+    fr = 0.5 * (1.0 - np.tanh((r - 0.5 * D) / (0.05 * D)))  # 1 in the jet, 0 in the coflow
+    rng = np.random.default_rng(seed)
+    U = Uc + (Uj - Uc) * fr
+    U = U * (1.0 + pert * rng.uniform(-1.0, 1.0, U.shape))
+    T = Tc + (Tj - Tc) * fr
+    Yk = Yc[:, None, None] + (Yj - Yc)[:, None, None] * fr[None]
+    Rmix = (Yk * (R0 / mi)[:, None, None]).sum(axis=0)
+    rho = ATM / (Rmix * T)
+    inlet = np.zeros((5 + ns, nz, ny))
+    inlet[0], inlet[1], inlet[4] = rho, U, T
+    inlet[5:] = Yk * rho[None]
+    case.bc = dict(inlet=np.ascontiguousarray(inlet), upper=np.zeros(5 + ns), wall_pertb=None, tm=np.zeros(0),
+                   fait=np.zeros(0))
+    # initial field: the inflow plane extended downstream
+    d3 = np.broadcast_to(rho[:, :, None], (nz, ny, nx)).copy()
+    u3 = np.broadcast_to(U[:, :, None], (nz, ny, nx)).copy()
+    T3 = np.broadcast_to(T[:, :, None], (nz, ny, nx)).copy()
+    zero = np.zeros((nz, ny, nx))
+    case.prim5 = np.ascontiguousarray(np.stack([d3, u3, zero, zero.copy(), T3]))
+    case.di = np.ascontiguousarray(np.broadcast_to((Yk * rho[None])[:, :, :, None], (ns, nz, ny, nx)).copy())
+    cmax = math.sqrt(1.4 * R0 / 0.029 * Tc)
+    dmin = min(np.diff(x).min(), np.diff(y).min(), np.diff(z).min())
+    case.dt = 0.5 * dmin / (Uj * (1 + pert) + cmax)
+    case.nsteps = nsteps
+    case.if_reaction = 1
+    case.nsub = nsub
+    case.info = dict(D=D, dmin=dmin)
+    return case

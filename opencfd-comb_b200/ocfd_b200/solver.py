@@ -37,21 +37,6 @@ def lib():
             fn = getattr(L, name)
             fn.restype = res
             fn.argtypes = args
-        extra = {
-            "ocfd_gpu_init_state": (C.c_int, [abi.PD, abi.PD, C.c_double]),
-            "ocfd_gpu_chem_setup": (C.c_int, [C.POINTER(abi.Thermo), C.POINTER(abi.Kinetics), C.c_int, C.c_int]),
-            "ocfd_gpu_profile": (C.c_int, [C.c_int]),
-            "ocfd_gpu_profile_read": (C.c_int, [C.c_int, abi.PD, C.POINTER(C.c_longlong)]),
-            "ocfd_gpu_profile_name": (C.c_char_p, [C.c_int]),
-            "ocfd_gpu_profile_nclass": (C.c_int, []),
-            "ocfd_gpu_stream": (C.c_void_p, []),
-            "ocfd_gpu_launch_count": (C.c_longlong, []),
-            "ocfd_gpu_is_separable": (C.c_int, []),
-        }
-        for name, (res, args) in extra.items():
-            fn = getattr(L, name)
-            fn.restype = res
-            fn.argtypes = args
         _lib = L
     return _lib
 

@@ -145,6 +145,8 @@ struct Oracle {
     P = *pp;
     nx = P.nx; ny = P.ny; nz = P.nz; L = P.lap; NS = P.n_spec;
     if (L != 4 || NS < 1 || NS > OCFD_MAX_SPEC || nx < 8 || ny < 8 || nz < 8) { err = "bad sizes"; return OCFD_ERR_PARAM; }
+    for (int m = 0; m < 6; m++)
+      if (P.ghost_cell[m] != 0) { err = "Ghost_Cell != 0 (needs Jac_Ghost_boundary) is not restated"; return OCFD_ERR_UNSUPPORTED; }
     HX = nx + 2 * L; HY = ny + 2 * L; HZ = nz + 2 * L; H = HX * HY * HZ; N = (long)nx * ny * nz;
     hx = 1.0 / (nx - 1.0); hy = 1.0 / (ny - 1.0); hz = 1.0 / (nz - 1.0);
     for (int dd = 0; dd < 3; dd++) bound[dd][0] = bound[dd][1] = P.iperiodic[dd] == 0 ? 1 : 0;
@@ -198,6 +200,13 @@ struct Oracle {
       for (int m = 0; m < 9; m++) M[M_AKX1 + m][q] = M[M_AKX + m][q] / jac;
     }
 
+    /* jet inflow data: a 2-D inlet table (ocfd_bc_jet forces BcData_inlet = 2, no upper data) */
+    if (P.ibc == OCFD_BC_JET) {
+      if (!bc) { err = "bcdata"; return OCFD_ERR_PARAM; }
+      bcdata_inlet = 2;
+      bcdata_upper = -1;
+      inlet.assign(bc->inlet, bc->inlet + (long)(5 + NS) * ny * nz);
+    }
     /* boundary-layer data */
     if (P.ibc == OCFD_BC_BOUNDARYLAYER) {
       if (!bc) { err = "bcdata"; return OCFD_ERR_PARAM; }
@@ -807,6 +816,46 @@ struct Oracle {
     }
   }
 
+  /* ocfd_bc_jet (OCFD_BC_jet.f90:2-96): 2-D inlet table, Dirichlet (Iflag_inlet = 0) or
+   * subsonic / supersonic switch on the inlet Mach number (1); zeroth-order outlet */
+  void bc_jet() {
+    int iflag = (int)std::lround(P.bc_para[0]);
+    for (int k = 1; k <= nz; k++)
+      for (int j = 1; j <= ny; j++) {
+        long q = ih(1, j, k);
+        double vals[5 + OCFD_MAX_SPEC];
+        for (int c = 0; c < 5 + NS; c++) vals[c] = inlet[((long)c * nz + (k - 1)) * ny + (j - 1)];
+        if (iflag == 0) {
+          d[q] = vals[0]; u[q] = vals[1]; v[q] = vals[2]; w[q] = vals[3]; T[q] = vals[4];
+          for (int m = 0; m < NS; m++) di[(long)m * H + q] = vals[5 + m];
+        } else {
+          u[q] = vals[1]; v[q] = vals[2]; w[q] = vals[3]; T[q] = vals[4];
+          double d1 = vals[0], di1[OCFD_MAX_SPEC], ai1[OCFD_MAX_SPEC], d0 = 0.0;
+          for (int m = 0; m < NS; m++) { di1[m] = vals[5 + m]; d0 = d0 + di1[m]; }
+          for (int m = 0; m < NS; m++) ai1[m] = di1[m] / d0;
+          double p1 = ch.P(di1, T[q]);
+          double Et1 = ch.E_of_T(di1, T[q]);
+          double gamma = p1 / Et1 + 1.0;
+          double c1 = std::sqrt(gamma * p1 / d1);  /* comput_soundspeed (CHEM_thermdyn.f90:412-418) */
+          if (u[q] < c1) {
+            p[q] = p[ih(2, j, k)];
+            double dn = ch.Dens(ai1, T[q], p[q]);
+            d[q] = dn;
+            for (int m = 0; m < NS; m++) di[(long)m * H + q] = dn * ai1[m];
+          } else {
+            d[q] = d1;
+            for (int m = 0; m < NS; m++) di[(long)m * H + q] = di1[m];
+          }
+        }
+      }
+    for (int k = 1; k <= nz; k++)
+      for (int j = 1; j <= ny; j++) {
+        long q = ih(nx, j, k), q1 = ih(nx - 1, j, k);
+        d[q] = d[q1]; u[q] = u[q1]; v[q] = v[q1]; w[q] = w[q1]; T[q] = T[q1]; p[q] = p[q1]; Et[q] = Et[q1];
+        for (int m = 0; m < NS; m++) di[(long)m * H + q] = di[(long)m * H + q1];
+      }
+  }
+
   /* Flow_Ghost_Extent_2nd (OCFD_GhostCell.f90:166-364) */
   void ghost() {
     const double s1 = 0.8, s2 = 1.2;
@@ -844,6 +893,7 @@ struct Oracle {
 
   void ocfd_bc(double tt) {
     if (P.ibc == OCFD_BC_BOUNDARYLAYER) bc_boundary_layer(tt);
+    if (P.ibc == OCFD_BC_JET) bc_jet();
     for (int k = 1; k <= nz; k++)
       for (int j = 1; j <= ny; j++) { face_cell(1, j, k); }
     for (int k = 1; k <= nz; k++)

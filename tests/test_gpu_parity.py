@@ -101,14 +101,21 @@ def test_flatplate_bitwise(oracle, gpu, scheme):
         assert len(np.unique(sel)) >= 2  # the case exercises more than one scheme
 
 
-def test_flatplate_boundary_variants_bitwise(oracle, gpu):
-    """Scheme_boundary = 1 / -1 faces and second-order ghost cells at the outlet and upper face."""
+def _variant(p, name):
+    if name in ("sb_iplus_weno5", "all"):
+        p.scheme_boundary[1] = 1   # i+: full WENO5 at the closure interfaces (ghost-cell type)
+    if name in ("sb_jplus_none", "all"):
+        p.scheme_boundary[3] = -1  # j+: interior scheme up to the face
+    if name in ("outlet2", "all"):
+        p.bc_para[3] = 2           # second-order outlet extrapolation
+
+
+@pytest.mark.parametrize("name", ["sb_iplus_weno5", "sb_jplus_none", "outlet2", "all"])
+def test_flatplate_boundary_variants_bitwise(oracle, gpu, name):
+    """Scheme_boundary = 1 / -1 faces (their closures read the halo, whose metrics are the
+    reference's unfilled 1.0) and the second-order outlet."""
     c = cases.flatplate(nx=40, ny=24, nz=12, scheme="WENO5", lx=0.01, ly=0.004, y1=2e-5)
-    c.params.scheme_boundary[1] = 1   # i+: WENO5 with ghost cells
-    c.params.scheme_boundary[3] = -1  # j+: interior scheme up to the face
-    c.params.ghost_cell[1] = 1
-    c.params.ghost_cell[3] = 2
-    c.params.bc_para[3] = 2           # second-order outlet extrapolation
+    _variant(c.params, name)
     so, sg, *_ = run_pair(oracle, gpu, c, 2)
     assert_bitwise(so, sg)
 
@@ -167,6 +174,19 @@ def test_reacting_nine_species(oracle, gpu):
     assert rel_linf(interior(pro[4]), interior(prg[4])) <= tol
 
 
+@pytest.mark.parametrize("iflag", [0, 1])
+def test_reacting_jet(oracle, gpu, iflag):
+    """BC_JET inflow (Dirichlet / subsonic switch), zeroth-order outlet, 9 species, Wilke, chemistry."""
+    c = cases.jet(nx=24, ny=16, nz=16, iflag_inlet=iflag)
+    so, sg, *_ = run_pair(oracle, gpu, c, 2, if_reaction=1, nsub=1)
+    fo, dio, pro = so
+    fg, dig, prg = sg
+    for m in range(5):
+        assert rel_linf(fo[m], fg[m]) <= 1e-10, (m, rel_linf(fo[m], fg[m]))
+    for m in range(9):
+        assert rel_linf(interior(dio[m]), interior(dig[m])) <= 1e-10
+
+
 @pytest.mark.parametrize("mode", [abi.CHEM_IMPLICIT, abi.CHEM_EULER, abi.CHEM_RK2, abi.CHEM_RK3])
 def test_chem_batch(oracle, gpu, mode):
     """Batched 0-D reactors (persistent work queue) against the oracle integrator."""
@@ -211,6 +231,11 @@ def test_negative_energy_repair_bitwise(oracle, gpu):
 
 
 def test_bad_parameters_rejected(gpu):
+    c = cases.isotropic(n=12)
+    c.params.ghost_cell[0] = 1
+    with pytest.raises(gpu.OcfdError) as ei:
+        gpu.Solver(c)
+    assert ei.value.code == abi.ERR_UNSUPPORTED
     c = cases.isotropic(n=12)
     c.params.scheme_invis = 7
     with pytest.raises(gpu.OcfdError) as ei:
