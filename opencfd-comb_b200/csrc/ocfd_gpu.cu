@@ -316,11 +316,6 @@ void stage_t(int krk, double dt1) {
       for (int m = 0; m < NS; m++) fl.push_back(L->di + (size_t)m * H);
     exchange_v(fl, 7);
   }
-  if (NS == 1) {
-    KTimer t(KC_EXCH);
-    k_copy<<<nblk(H, 256), 256, 0, L->st>>>(L->d, L->di, H);
-    LAUNCH_CHECK();
-  }
   if (krk == 1 && L->P.scheme_invis == OCFD_SCHEME_HYBRID) {
     sensor();
     exchange({L->Rh}, 7);
@@ -386,6 +381,14 @@ void stage_t(int krk, double dt1) {
       else k_visc_div<false><<<nblk(N, 256), 256, 0, L->st>>>(L->ev_ptrs, L->du, L->geo);
       LAUNCH_CHECK();
     }
+  }
+  // N_SPEC = 1: di = d over the whole array (OCFD_Time_Adv.f90:45-52). Nothing between the stage
+  // start and here reads di, and the inline transport of k_visc_ev must see the previous stage's
+  // di (comput_Amu_Amk_AMD runs before the copy in the reference), so the copy happens here.
+  if (NS == 1) {
+    KTimer t(KC_EXCH);
+    k_copy<<<nblk(H, 256), 256, 0, L->st>>>(L->d, L->di, H);
+    LAUNCH_CHECK();
   }
   prims_t<NS>(krk, dt1);
   ocfd_bc_t<NS>();
