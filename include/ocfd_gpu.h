@@ -222,8 +222,19 @@ int ocfd_gpu_pinned_free(void* ptr);
 int ocfd_gpu_step_launches(void);
 /* Kernels launched by the library since init (graph replays count their kernels). */
 long long ocfd_gpu_launch_count(void);
+/* Bytes of the device arena in use (state, metrics, work arrays). */
+long long ocfd_gpu_device_bytes(void);
 /* 1 when the grid is a tensor product and metrics are kept as three 1-D arrays. */
 int ocfd_gpu_is_separable(void);
+
+/* ocfd_gpu_chem_batch_device for callers that cannot allocate device memory: it allocates
+ * nothing and keeps its scratch (reactor ordering, sub-step histogram, work-queue counter) in a
+ * fixed array of the library sized for at most 1048576 reactors (about 4 MB, held on every GPU
+ * that loads the library until exit). Larger n returns OCFD_ERR_PARAM. The first call on a device
+ * looks up the array's device address, so make that first call before any stream capture. All
+ * calls share the one array: calls that overlap on the GPU (other threads, other streams) race.
+ * No counterpart in the reference (its chemistry loop runs on the CPU and allocates nothing). */
+int ocfd_gpu_chem_batch_noalloc(int n, double* d_di, double* d_e, const double* d_dt, const int* d_nsub);
 
 /* Statistics of the last advance: number of Et<=0 repairs, Newton non-converged cells. */
 int ocfd_gpu_stats(long long* neg_et, long long* newton_fail);

@@ -1289,6 +1289,80 @@ int ocfd_gpu_chem_batch_device(int n, double* d_di, double* d_e, const double* d
   });
 }
 
+}  // extern "C"
+
+// ---------------------------------------------------------------- batched chemistry, no allocation
+// Some callers cannot let a library allocate device memory: a host application that owns the
+// whole device memory budget through its own pool (the usual situation when the chemistry is
+// embedded in a larger solver or a serving process), or code that must not allocate between its
+// setup and its launches. ocfd_gpu_chem_batch_device gets its scratch (the sub-step ordering of
+// the reactors, the histogram of sub-step counts and the work-queue counter) from cudaMalloc the
+// first time and whenever n grows; this variant takes it from a fixed array of the library
+// instead, so it allocates nothing. The array is sized for OCFD_NOALLOC_MAX_REACTORS reactors and
+// lives on every GPU that loads the library until the process exits.
+#define OCFD_NOALLOC_MAX_REACTORS (1 << 20)
+#define OCFD_NOALLOC_BINS 1024
+#define OCFD_NOALLOC_WORDS (OCFD_NOALLOC_MAX_REACTORS + OCFD_NOALLOC_BINS + 64)
+static __device__ __align__(256) int g_noalloc_scratch[OCFD_NOALLOC_WORDS];
+
+namespace {
+// device address of g_noalloc_scratch per device, looked up once per device with that device
+// current (in host code the array's name is only a host-side stand-in)
+int* g_noalloc_ptr[64] = {};
+
+int* noalloc_scratch() {
+  int dev = 0;
+  CK(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 64) throw std::runtime_error("device index out of range");
+  if (!g_noalloc_ptr[dev]) {
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess || p == nullptr)
+      throw CudaError(std::string("cudaGetSymbolAddress(g_noalloc_scratch): ") + cudaGetErrorString(e), OCFD_ERR_CUDA);
+    g_noalloc_ptr[dev] = static_cast<int*>(p);
+  }
+  return g_noalloc_ptr[dev];
+}
+}  // namespace
+
+extern "C" {
+
+int ocfd_gpu_chem_batch_noalloc(int n, double* d_di, double* d_e, const double* d_dt, const int* d_nsub) {
+  return guarded([&]() -> int {
+    if (!L || !L->have_kin) { g_err = "ocfd_gpu_init or ocfd_gpu_chem_setup with a mechanism first"; return OCFD_ERR_STATE; }
+    if (n < 0 || n > OCFD_NOALLOC_MAX_REACTORS) {
+      g_err = "ocfd_gpu_chem_batch_noalloc: n = " + std::to_string(n) + " exceeds the fixed scratch of " +
+              std::to_string(OCFD_NOALLOC_MAX_REACTORS) + " reactors (use ocfd_gpu_chem_batch_device)";
+      return OCFD_ERR_PARAM;
+    }
+    if (n == 0) return 0;
+    int* perm = noalloc_scratch();
+    int* hist = perm + OCFD_NOALLOC_MAX_REACTORS;
+    int* counter = hist + OCFD_NOALLOC_BINS;
+    int* nfail = counter + 32;
+    // the array keeps the previous call's contents: the histogram and the counters restart at 0
+    CK(cudaMemsetAsync(hist, 0, sizeof(int) * (OCFD_NOALLOC_BINS + 64), L->st));
+    {
+      KTimer t(KC_CHEM);
+      k_nsub_hist<<<nblk(n, 256), 256, 0, L->st>>>(n, d_nsub, hist, OCFD_NOALLOC_BINS);
+      k_nsub_scan<<<1, 32, 0, L->st>>>(hist, OCFD_NOALLOC_BINS);
+      k_nsub_scatter<<<nblk(n, 256), 256, 0, L->st>>>(n, d_nsub, hist, OCFD_NOALLOC_BINS, perm);
+      LAUNCH_CHECK();
+    }
+    int dev = 0, sms = 148;
+    CK(cudaGetDevice(&dev));
+    CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    {
+      KTimer t(KC_CHEM);
+      launch_chem_batch(L->NS, sms, n, d_di, d_e, d_dt, d_nsub, perm, counter, nfail, L->st);
+      LAUNCH_CHECK();
+    }
+    CK(cudaStreamSynchronize(L->st));
+    prof_collect();
+    return 0;
+  });
+}
+
 int ocfd_gpu_chem_batch(int n, double* di, double* e, const double* dt, const int* nsub) {
   return guarded([&]() -> int {
     if (!L || !L->have_kin) { g_err = "ocfd_gpu_init or ocfd_gpu_chem_setup with a mechanism first"; return OCFD_ERR_STATE; }
@@ -1345,6 +1419,7 @@ int ocfd_gpu_profile_nclass(void) { return KC_NUM; }
 void* ocfd_gpu_stream(void) { return L ? (void*)L->st : nullptr; }
 long long ocfd_gpu_launch_count(void) { return L ? (long long)L->launches : 0; }
 int ocfd_gpu_is_separable(void) { return L && L->sep ? 1 : 0; }
+long long ocfd_gpu_device_bytes(void) { return L ? (long long)L->arena_used : 0; }
 
 double ocfd_gpu_fp64_peak_gflops(void) {
   double r = -1.0;

@@ -134,9 +134,11 @@ GPU_SIGNATURES = {
     "ocfd_gpu_stream": (C.c_void_p, []),
     "ocfd_gpu_launch_count": (C.c_longlong, []),
     "ocfd_gpu_is_separable": (I, []),
+    "ocfd_gpu_device_bytes": (C.c_longlong, []),
     "ocfd_gpu_event_record": (I, [I]),
     "ocfd_gpu_event_elapsed": (I, [I, I, PD]),
     "ocfd_gpu_pinned_alloc": (I, [C.c_size_t, C.POINTER(C.c_void_p)]),
     "ocfd_gpu_pinned_free": (I, [C.c_void_p]),
     "ocfd_gpu_step_launches": (I, []),
+    "ocfd_gpu_chem_batch_noalloc": (I, [I, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
 }
