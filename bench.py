@@ -200,6 +200,7 @@ def main_ours(a):
 
     c, name = make_case(a.workload, nz=a.nz)
     g = solver.Solver(c)
+    state_gb = L.ocfd_gpu_device_bytes() / 1e9
     g.init_state()
     dt = c.dt
     tt = 0.0
@@ -318,8 +319,7 @@ def main_ours(a):
                "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
                "config": {"workload": name, "cells_per_gpu": c.ncell, "dt": dt, "chemistry": "off (non-reacting air)",
                           "parallelism": "replicas x%d (no data-path collective)" % world,
-                          "l2": "state %.1f GB per GPU >> 126 MB L2; no flush" % (L.ocfd_gpu_launch_count() and 0 or
-                                                                                   (8 * (20 * c.ncell) / 1e9))},
+                          "l2": "device state %.1f GB per GPU >> 126 MB L2; no flush between steps" % state_gb},
                "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches),
                "clocks": clk.summary()}
         print(json.dumps(out))

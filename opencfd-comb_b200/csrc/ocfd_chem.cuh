@@ -245,9 +245,9 @@ __device__ void chem_step(double* di, double& E, double dt, int* nfail) {
 template <int NS>
 __global__ void __launch_bounds__(128) k_chem_cells(double* f, double* Et, double* T, double* p, double* di,
                                                     double dt2, int nsub, int* nfail) {
-  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= cC.N) return;
-  int i = (int)(t % cC.nx) + 1, j = (int)((t / cC.nx) % cC.ny) + 1, k = (int)(t / cC.nx / cC.ny) + 1;
+  int i = t % cC.nx + 1, j = (t / cC.nx) % cC.ny + 1, k = t / cC.nx / cC.ny + 1;
   const int q = hidx(i, j, k);
   double d1[NS];
 #pragma unroll

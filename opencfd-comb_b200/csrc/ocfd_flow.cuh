@@ -250,12 +250,16 @@ __device__ __forceinline__ double cdiff(const double* __restrict__ f, int q, int
          c[3] * (f[q + 4 * s] - f[q - 4 * s]);
 }
 
-__device__ __forceinline__ bool cell_of(long long t, int& i, int& j, int& k) {
-  if (t >= cC.N) return false;
-  i = (int)(t % cC.nx) + 1;
-  long long r = t / cC.nx;
-  j = (int)(r % cC.ny) + 1;
-  k = (int)(r / cC.ny) + 1;
+// interior cell of a linear thread index (32-bit arithmetic: the library rejects grids whose
+// halo arrays reach 2^31 elements, and 64-bit division is emulated in software on the GPU)
+__device__ __forceinline__ bool cell_of(long long t64, int& i, int& j, int& k) {
+  if (t64 >= cC.N) return false;
+  const unsigned t = (unsigned)t64, nx = (unsigned)cC.nx, ny = (unsigned)cC.ny;
+  const unsigned r = t / nx;
+  i = (int)(t - r * nx) + 1;
+  const unsigned s = r / ny;
+  j = (int)(r - s * ny) + 1;
+  k = (int)s + 1;
   return true;
 }
 
@@ -447,21 +451,20 @@ static __global__ void k_exchange(ExchArgs a) {
   if (fidx >= a.nf) return;
   double* f = a.f[fidx];
   const int L = OCFD_L;
-  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  const long long nxz = (long long)L * cC.ny * cC.nz, nyz = (long long)L * cC.nx * cC.nz,
-                  nzz = (long long)L * cC.nx * cC.ny;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int nxz = L * cC.ny * cC.nz, nyz = L * cC.nx * cC.nz, nzz = L * cC.nx * cC.ny;
   if ((a.dirmask & 1) && cC.iper[0] && t < nxz) {
-    int l = (int)(t % L), j = (int)((t / L) % cC.ny) + 1, k = (int)(t / L / cC.ny) + 1;
+    int l = t % L, j = (t / L) % cC.ny + 1, k = t / L / cC.ny + 1;
     f[hidx(cC.nx + 1 + l, j, k)] = f[hidx(1 + l, j, k)];
     f[hidx(1 - L + l, j, k)] = f[hidx(cC.nx + 1 - L + l, j, k)];
   }
   if ((a.dirmask & 2) && cC.iper[1] && t < nyz) {
-    int i = (int)(t % cC.nx) + 1, l = (int)((t / cC.nx) % L), k = (int)(t / cC.nx / L) + 1;
+    int i = t % cC.nx + 1, l = (t / cC.nx) % L, k = t / cC.nx / L + 1;
     f[hidx(i, cC.ny + 1 + l, k)] = f[hidx(i, 1 + l, k)];
     f[hidx(i, 1 - L + l, k)] = f[hidx(i, cC.ny + 1 - L + l, k)];
   }
   if ((a.dirmask & 4) && cC.iper[2] && t < nzz) {
-    int i = (int)(t % cC.nx) + 1, j = (int)((t / cC.nx) % cC.ny) + 1, l = (int)(t / cC.nx / cC.ny);
+    int i = t % cC.nx + 1, j = (t / cC.nx) % cC.ny + 1, l = t / cC.nx / cC.ny;
     f[hidx(i, j, cC.nz + 1 + l)] = f[hidx(i, j, 1 + l)];
     f[hidx(i, j, 1 - L + l)] = f[hidx(i, j, cC.nz + 1 - L + l)];
   }
