@@ -77,11 +77,13 @@ __device__ __forceinline__ void split_point(double Et1, double p1, double c1, do
   }
 }
 
-// tile shapes: x sweeps run along the contiguous index, so a tile is a long chunk of few
-// lines; y / z sweeps put 32 contiguous i-lines across the warp and a short chunk along j / k.
+// Tile shapes. x sweeps run along the contiguous index, so a tile is a long chunk of few lines;
+// y / z sweeps put 32 contiguous i-lines across the warp and a short chunk along j / k. Each
+// shape makes the split phase (C + 8 points of NL pencils) a whole number of 256-thread rounds.
+constexpr int FLUX_THREADS = 256;
 template <int DIR>
 struct Tile {
-  static constexpr int C = 64, NL = 4;
+  static constexpr int C = 56, NL = 4;
 };
 template <>
 struct Tile<1> {
@@ -92,6 +94,15 @@ struct Tile<2> {
   static constexpr int C = 16, NL = 32;
 };
 
+template <int DIR, bool SCALAR>
+struct FluxTile {
+  static constexpr int C = Tile<DIR>::C, NL = Tile<DIR>::NL, P = C + 8, NC = SCALAR ? 1 : 5;
+  static constexpr int NCS = 2 * NC;        // (component, sign) pairs: plus components, then minus
+  static constexpr int NI = (C + 1) * NL;   // interfaces of a tile
+  static_assert((P * NL) % FLUX_THREADS == 0, "split phase must fill whole rounds");
+  static constexpr size_t smem = sizeof(double) * (size_t)(NCS * P * NL + NCS * NI) + sizeof(int) * (2 * NI + 4);
+};
+
 struct FluxArgs {
   const double *d, *u, *v, *w, *p, *Et;  // halo arrays
   const double* fs;                      // scalar (species density) for SCALAR sweeps
@@ -100,17 +111,48 @@ struct FluxArgs {
   Geo g;
 };
 
+// interface i of a pencil of n cells lies where a boundary closure of OCFD2d_flux1/2 may apply
+// to the positive or the negative flux (OCFD_inviscous.f90:209-362)
+__device__ __forceinline__ bool closure_zone(int i, int n, int dir) {
+  const int ka = max(-cC.Ka1, -cC.Ka2), kb = max(cC.Kb1, cC.Kb2);
+  return (cC.bound[dir][0] == 1 && cC.sb[2 * dir] != -1 && i <= ka) ||
+         (cC.bound[dir][1] == 1 && cC.sb[2 * dir + 1] != -1 && i >= n - kb + 1);
+}
+
+// UD7L for either sign with one code path: the negative flux reads the stencil mirrored, and
+// both sums keep the reference's term order (OCFD_Schemes_1.f90 UD7L P / M)
+template <int VS>
+__device__ __forceinline__ double ud7l_signed(const double* v, bool plus) {
+  const double* U = cC.UD7L;
+  const double* w = plus ? v - 3 * VS : v + 4 * VS;
+  const int s = plus ? VS : -VS;
+  return U[0] * w[0] + U[1] * w[s] + U[2] * w[2 * s] + U[3] * w[3 * s] + U[4] * w[4 * s] + U[5] * w[5 * s] +
+         U[6] * w[6 * s] + U[7] * w[7 * s];
+}
+
+// One sweep direction of the inviscid flux for a tile of NL pencils x C cells, in three phases:
+//  1. split fluxes of the C + 8 points of every pencil into shared memory (one point per thread);
+//     for HYBRID the same threads classify the tile's interfaces: those that take UD7L away from
+//     a boundary closure are marked fast, the rest go to a shared-memory work list;
+//  2. interface fluxes, one (component, sign, interface) item per thread: fast interfaces run
+//     UD7L, then the listed ones run the general reconstruction (closures, WENO5/7, OMP6), so a
+//     warp never carries the WENO branches for the lanes that need only UD7L;
+//  3. flux difference (hh(i) - hh(i-1)) / d, combined into du as the reference does per sweep.
 template <int DIR, int SCHEME, int SPLIT, bool SEP, bool SCALAR>
-__global__ void __launch_bounds__(256) k_flux(FluxArgs a) {
-  constexpr int C = Tile<DIR>::C, NL = Tile<DIR>::NL, P = C + 8, NC = SCALAR ? 1 : 5;
+__global__ void __launch_bounds__(FLUX_THREADS, 2) k_flux(FluxArgs a) {
+  using T = FluxTile<DIR, SCALAR>;
+  constexpr int C = T::C, NL = T::NL, P = T::P, NC = T::NC, NCS = T::NCS, NI = T::NI;
+  constexpr bool HYB = SCHEME == OCFD_SCHEME_HYBRID;
   constexpr int VS = DIR == 0 ? 1 : NL;  // stride of consecutive sweep points in shared memory
   extern __shared__ double smem[];
-  double* sfp = smem;                // [NC][..]
-  double* sfm = smem + NC * P * NL;  // [NC][..]
-  double* sh1 = sfm + NC * P * NL;   // [NC][(C+1) x NL]
-  double* sh2 = sh1 + NC * (C + 1) * NL;
-  auto sidx = [&](int c, int p, int l) { return DIR == 0 ? (c * NL + l) * P + p : (c * P + p) * NL + l; };
-  auto hidx2 = [&](int c, int t, int l) { return DIR == 0 ? (c * NL + l) * (C + 1) + t : (c * (C + 1) + t) * NL + l; };
+  double* sf = smem;               // [NCS][P x NL] split fluxes
+  double* sh = sf + NCS * P * NL;  // [NCS][NI] interface fluxes
+  int* squeue = reinterpret_cast<int*>(sh + NCS * NI);  // listed interfaces: scm << 16 | interface
+  int* sfast = squeue + NI;                             // 1 = UD7L fast path
+  int* sqn = sfast + NI;                                // list length
+  // point p of pencil l, interface t of pencil l
+  auto sidx = [&](int cs, int p, int l) { return DIR == 0 ? (cs * NL + l) * P + p : (cs * P + p) * NL + l; };
+  auto iidx = [&](int t, int l) { return DIR == 0 ? l * (C + 1) + t : t * NL + l; };
 
   const int n = DIR == 0 ? cC.nx : (DIR == 1 ? cC.ny : cC.nz);
   const int s0 = (DIR == 0 ? blockIdx.x : blockIdx.y) * C + 1;  // first cell of the chunk
@@ -124,18 +166,24 @@ __global__ void __launch_bounds__(256) k_flux(FluxArgs a) {
     else if (DIR == 1) { i = l0 + l; j = s; k = bz; }
     else { i = l0 + l; j = bz; k = s; }
   };
+  if (HYB) {
+    if (threadIdx.x == 0) *sqn = 0;
+    __syncthreads();
+  }
 
-  // phase 1: split fluxes of every point of the tile (cells plus 4 on each side)
-  for (int idx = threadIdx.x; idx < P * NL; idx += blockDim.x) {
+  // phase 1 (uniform trip count: the warp-wide ballot below needs every lane)
+  for (int base = 0; base < P * NL; base += FLUX_THREADS) {
+    const int idx = base + threadIdx.x;
     int p, l;
     if (DIR == 0) { p = idx % P; l = idx / P; }
     else { l = idx % NL; p = idx / NL; }
-    int s = s0 - 4 + p;
+    const int s = s0 - 4 + p;
+    const bool line_ok = l0 + l <= nl_max;
     double fp[5], fm[5];
-    if (l0 + l <= nl_max && p < ncell + 8) {
+    if (line_ok && p < ncell + 8) {
       int i, j, k;
       coords(s, l, i, j, k);
-      int q = hidx(i, j, k);
+      const int q = hidx(i, j, k);
       double A1, A2, A3;
       metric_dir<SEP>(a.g, DIR, i, j, k, q, A1, A2, A3);
       if (SCALAR) {
@@ -155,52 +203,89 @@ __global__ void __launch_bounds__(256) k_flux(FluxArgs a) {
     }
 #pragma unroll
     for (int c = 0; c < NC; c++) {
-      sfp[sidx(c, p, l)] = fp[c];
-      sfm[sidx(c, p, l)] = fm[c];
+      sf[sidx(c, p, l)] = fp[c];
+      sf[sidx(NC + c, p, l)] = fm[c];
+    }
+    if (HYB) {
+      // interface t = p - 3 lies between this point's cell and the next one
+      const int t = p - 3;
+      bool listed = false;
+      int scm = 1;
+      if (line_ok && t >= 0 && t <= ncell) {
+        const int ig = s0 - 1 + t;
+        int i, j, k;
+        coords(ig, l, i, j, k);
+        const int q = hidx(i, j, k);
+        scm = hybrid_index(fmax(__ldg(a.Rh + q), __ldg(a.Rh + q + stride)));
+        listed = scm != 1 || closure_zone(ig, n, DIR);
+        sfast[iidx(t, l)] = listed ? 0 : 1;
+      }
+      const unsigned m = __ballot_sync(0xffffffffu, listed);
+      if (m) {
+        const int lane = threadIdx.x & 31, leader = __ffs(m) - 1;
+        int pos = 0;
+        if (lane == leader) pos = atomicAdd(sqn, __popc(m));
+        pos = __shfl_sync(0xffffffffu, pos, leader);
+        if (listed) squeue[pos + __popc(m & ((1u << lane) - 1u))] = (scm << 16) | iidx(t, l);
+      }
     }
   }
   __syncthreads();
 
   // phase 2: numerical fluxes at interfaces s0-1 .. s0-1+ncell
-  for (int idx = threadIdx.x; idx < (C + 1) * NL; idx += blockDim.x) {
+  const int nq = HYB ? *sqn : 0;
+  const int nfast = NCS * NI;
+  for (int idx = threadIdx.x; idx < nfast + NCS * nq; idx += FLUX_THREADS) {
+    int cs, it, scm = 0;
+    if (idx < nfast) {
+      cs = idx / NI;
+      it = idx - cs * NI;
+    } else {
+      const int r = idx - nfast;
+      cs = r / nq;
+      const int e = squeue[r - cs * nq];
+      it = e & 0xffff;
+      scm = e >> 16;
+    }
     int t, l;
-    if (DIR == 0) { t = idx % (C + 1); l = idx / (C + 1); }
-    else { l = idx % NL; t = idx / NL; }
-    if (l0 + l > nl_max || t > ncell) continue;
-    int ig = s0 - 1 + t;  // reference interface index hh(ig), between cells ig and ig+1
-    int scm = 0;
-    if (SCHEME == OCFD_SCHEME_HYBRID) {
-      int i, j, k;
-      coords(ig, l, i, j, k);
-      int q = hidx(i, j, k);
-      scm = hybrid_index(fmax(__ldg(a.Rh + q), __ldg(a.Rh + q + stride)));
+    if (DIR == 0) { t = it % (C + 1); l = it / (C + 1); }
+    else { l = it % NL; t = it / NL; }
+    if (idx < nfast) {
+      if (l0 + l > nl_max || t > ncell) continue;
+      if (HYB && !sfast[it]) continue;
     }
-#pragma unroll
-    for (int c = 0; c < NC; c++) {
-      const double* vp = sfp + sidx(c, t + 3, l);
-      const double* vm = sfm + sidx(c, t + 3, l);
-      sh1[hidx2(c, t, l)] = interface_flux<SCHEME, true, VS>(vp, ig, n, DIR, scm);
-      sh2[hidx2(c, t, l)] = interface_flux<SCHEME, false, VS>(vm, ig, n, DIR, scm);
+    const double* v = sf + sidx(cs, t + 3, l);
+    const bool plus = cs < NC;
+    double h;
+    if (HYB && idx < nfast) {
+      h = ud7l_signed<VS>(v, plus);
+    } else {
+      const int ig = s0 - 1 + t;  // reference interface index hh(ig), between cells ig and ig+1
+      h = plus ? interface_flux<SCHEME, true, VS>(v, ig, n, DIR, scm) : interface_flux<SCHEME, false, VS>(v, ig, n, DIR, scm);
     }
+    sh[cs * NI + it] = h;
   }
   __syncthreads();
 
   // phase 3: flux difference into du
   const double h1 = cC.h1[DIR];
   const long long N = cC.N;
-  for (int idx = threadIdx.x; idx < C * NL; idx += blockDim.x) {
+  for (int idx = threadIdx.x; idx < C * NL; idx += FLUX_THREADS) {
     int t, l;
     if (DIR == 0) { t = idx % C; l = idx / C; }
     else { l = idx % NL; t = idx / NL; }
     if (l0 + l > nl_max || t >= ncell) continue;
     int i, j, k;
     coords(s0 + t, l, i, j, k);
-    int nn = nidx(i, j, k);
+    const int nn = nidx(i, j, k);
     double ajac = 0.0;
     if (DIR == 2) ajac = metric_jac<SEP>(a.g, i, j, k, hidx(i, j, k));
+    const int i0 = iidx(t, l), i1 = iidx(t + 1, l);
 #pragma unroll
     for (int c = 0; c < NC; c++) {
-      double val = (sh1[hidx2(c, t + 1, l)] - sh1[hidx2(c, t, l)] + sh2[hidx2(c, t + 1, l)] - sh2[hidx2(c, t, l)]) * h1;
+      const double* hp = sh + c * NI;
+      const double* hm = sh + (NC + c) * NI;
+      double val = (hp[i1] - hp[i0] + hm[i1] - hm[i0]) * h1;
       double* o = a.out + (size_t)c * N + nn;
       if (DIR == 0) *o = val;
       else if (DIR == 1) *o = *o + val;
@@ -220,8 +305,7 @@ __global__ void __launch_bounds__(256) k_flux(FluxArgs a) {
 
 template <int DIR, bool SCALAR>
 constexpr size_t flux_smem() {
-  constexpr int C = Tile<DIR>::C, NL = Tile<DIR>::NL, P = C + 8, NC = SCALAR ? 1 : 5;
-  return sizeof(double) * (size_t)(2 * NC * P * NL + 2 * NC * (C + 1) * NL);
+  return FluxTile<DIR, SCALAR>::smem;
 }
 
 // ---------------------------------------------------------------- CD6 / CD8 derivative
