@@ -78,20 +78,22 @@ __device__ __forceinline__ void split_point(double Et1, double p1, double c1, do
 }
 
 // Tile shapes. x sweeps run along the contiguous index, so a tile is a long chunk of few lines;
-// y / z sweeps put 32 contiguous i-lines across the warp and a short chunk along j / k. Each
+// y / z sweeps put 16 contiguous i-lines across a half-warp and a chunk along j / k. Each
 // shape makes the split phase (C + 8 points of NL pencils) a whole number of 256-thread rounds.
 constexpr int FLUX_THREADS = 256;
+// MINB is the resident-block target given to the register allocator (3 x 256 threads per SM;
+// the shared memory of one tile, 40 KB for x and 73 KB for y / z, also fits 3 times).
 template <int DIR>
 struct Tile {
-  static constexpr int C = 56, NL = 4;
+  static constexpr int C = 56, NL = 4, MINB = 3;
 };
 template <>
 struct Tile<1> {
-  static constexpr int C = 16, NL = 32;
+  static constexpr int C = 24, NL = 16, MINB = 3;
 };
 template <>
 struct Tile<2> {
-  static constexpr int C = 16, NL = 32;
+  static constexpr int C = 24, NL = 16, MINB = 3;
 };
 
 template <int DIR, bool SCALAR>
@@ -139,7 +141,7 @@ __device__ __forceinline__ double ud7l_signed(const double* v, bool plus) {
 //     warp never carries the WENO branches for the lanes that need only UD7L;
 //  3. flux difference (hh(i) - hh(i-1)) / d, combined into du as the reference does per sweep.
 template <int DIR, int SCHEME, int SPLIT, bool SEP, bool SCALAR>
-__global__ void __launch_bounds__(FLUX_THREADS, 2) k_flux(FluxArgs a) {
+__global__ void __launch_bounds__(FLUX_THREADS, Tile<DIR>::MINB) k_flux(FluxArgs a) {
   using T = FluxTile<DIR, SCALAR>;
   constexpr int C = T::C, NL = T::NL, P = T::P, NC = T::NC, NCS = T::NCS, NI = T::NI;
   constexpr bool HYB = SCHEME == OCFD_SCHEME_HYBRID;
@@ -309,29 +311,38 @@ constexpr size_t flux_smem() {
 }
 
 // ---------------------------------------------------------------- CD6 / CD8 derivative
-// OCFD_dx0/dy0/dz0 (OCFD_dxyz_viscous.f90) at one interior point q, sweep index ii of n.
-__device__ __forceinline__ double cdiff(const double* __restrict__ f, int q, int dir, int ii, int n) {
-  const int s = hstride(dir);
+// OCFD_dx0/dy0/dz0 (OCFD_dxyz_viscous.f90) at sweep index ii of n; f(m) is the value m points
+// away along the direction. CD = 6 or 8 fixes the interior scheme at compile time, CD = 0 reads
+// it from the constant block; every variant evaluates the same expressions.
+template <int CD, class F>
+__device__ __forceinline__ double cdiff_g(F f, int dir, int ii, int n) {
+  const bool cd8 = CD == 8 || (CD == 0 && cC.cd8_on);
   if (!cC.iper[dir]) {
     const double h2 = cC.h2x[dir], h12 = cC.h12x[dir];
-    if (ii == 1) return (-3.0 * f[q] + 4.0 * f[q + s] - f[q + 2 * s]) / h2;
-    if (ii == 2) return (f[q + s] - f[q - s]) / h2;
-    if (ii == 3) return (8.0 * (f[q + s] - f[q - s]) - (f[q + 2 * s] - f[q - 2 * s])) / h12;
-    if (ii == n) return (f[q - 2 * s] - 4.0 * f[q - s] + 3.0 * f[q]) / h2;
-    if (ii == n - 1) return (f[q + s] - f[q - s]) / h2;
-    if (ii == n - 2) return (8.0 * (f[q + s] - f[q - s]) - (f[q + 2 * s] - f[q - 2 * s])) / h12;
-    if (cC.cd8_on && (ii == 4 || ii == n - 3)) {
+    if (ii == 1) return (-3.0 * f(0) + 4.0 * f(1) - f(2)) / h2;
+    if (ii == 2) return (f(1) - f(-1)) / h2;
+    if (ii == 3) return (8.0 * (f(1) - f(-1)) - (f(2) - f(-2))) / h12;
+    if (ii == n) return (f(-2) - 4.0 * f(-1) + 3.0 * f(0)) / h2;
+    if (ii == n - 1) return (f(1) - f(-1)) / h2;
+    if (ii == n - 2) return (8.0 * (f(1) - f(-1)) - (f(2) - f(-2))) / h12;
+    if (cd8 && (ii == 4 || ii == n - 3)) {
       const double* a = cC.cd6[dir];
-      return a[0] * (f[q + 3 * s] - f[q - 3 * s]) + a[1] * (f[q + 2 * s] - f[q - 2 * s]) + a[2] * (f[q + s] - f[q - s]);
+      return a[0] * (f(3) - f(-3)) + a[1] * (f(2) - f(-2)) + a[2] * (f(1) - f(-1));
     }
   }
-  if (!cC.cd8_on) {
+  if (CD == 6 || !cd8) {
     const double* a = cC.cd6[dir];
-    return a[0] * (f[q + 3 * s] - f[q - 3 * s]) + a[1] * (f[q + 2 * s] - f[q - 2 * s]) + a[2] * (f[q + s] - f[q - s]);
+    return a[0] * (f(3) - f(-3)) + a[1] * (f(2) - f(-2)) + a[2] * (f(1) - f(-1));
   }
-  const double* c = cC.cd8[dir];
-  return c[0] * (f[q + s] - f[q - s]) + c[1] * (f[q + 2 * s] - f[q - 2 * s]) + c[2] * (f[q + 3 * s] - f[q - 3 * s]) +
-         c[3] * (f[q + 4 * s] - f[q - 4 * s]);
+  if constexpr (CD != 6) {
+    const double* c = cC.cd8[dir];
+    return c[0] * (f(1) - f(-1)) + c[1] * (f(2) - f(-2)) + c[2] * (f(3) - f(-3)) + c[3] * (f(4) - f(-4));
+  }
+  return 0.0;
+}
+__device__ __forceinline__ double cdiff(const double* __restrict__ f, int q, int dir, int ii, int n) {
+  const int s = hstride(dir);
+  return cdiff_g<0>([&](int m) { return f[q + m * s]; }, dir, ii, n);
 }
 
 // interior cell of a linear thread index (32-bit arithmetic: the library rejects grids whose
@@ -355,19 +366,12 @@ struct ViscArgs {
   Geo g;
 };
 
+// stresses, heat flux and Ev1..Ev3 at one cell from its twelve derivatives g[m][dir] of
+// (u, v, w, T) along (xi, eta, zeta) (OCFD_viscous.f90:60-108)
 template <int NS, bool SEP>
-__global__ void __launch_bounds__(256) k_visc_ev(ViscArgs a) {
-  int i, j, k;
-  if (!cell_of((long long)blockIdx.x * blockDim.x + threadIdx.x, i, j, k)) return;
+__device__ __forceinline__ void visc_point(const ViscArgs& a, int i, int j, int k, const double (&g)[4][3], double uq,
+                                           double vq, double wq, double Tq) {
   const int q = hidx(i, j, k), nn = nidx(i, j, k);
-  double g[4][3];  // d(u,v,w,T)/d(xi,eta,zeta)
-  const double* fl[4] = {a.u, a.v, a.w, a.T};
-  const int ii[3] = {i, j, k};
-  const int nd[3] = {cC.nx, cC.ny, cC.nz};
-#pragma unroll
-  for (int m = 0; m < 4; m++)
-#pragma unroll
-    for (int dd = 0; dd < 3; dd++) g[m][dd] = cdiff(fl[m], q, dd, ii[dd], nd[dd]);
   double A[9], A1[9];
   metric_all<SEP>(a.g, i, j, k, q, A, A1);
   // A: Akx Aky Akz Aix Aiy Aiz Asx Asy Asz
@@ -385,7 +389,7 @@ __global__ void __launch_bounds__(256) k_visc_ev(ViscArgs a) {
   double Tz = g[3][0] * A[2] + g[3][1] * A[5] + g[3][2] * A[8];
   double div = ux + vy + wz;
   double amu1, amuk;
-  if (a.amu) {
+  if constexpr (NS > 1) {  // from k_transport
     amu1 = a.amu[nn];
     amuk = a.amk[nn];
   } else {  // comput_Amu_Amk_AMD inline (Comput_flow_variables.f90:69-98)
@@ -398,10 +402,9 @@ __global__ void __launch_bounds__(256) k_visc_ev(ViscArgs a) {
     }
 #pragma unroll
     for (int m = 0; m < NS; m++) Xi[m] = Xi[m] / X0;
-    double T = a.T[q];
-    amu1 = dev_viscosity<NS>(T, Xi);
-    double cp = dev_Cp<NS>(a.d[q], d0, T);
-    amuk = dev_conductivity<NS>(amu1, cp, T, Xi);
+    amu1 = dev_viscosity<NS>(Tq, Xi);
+    double cp = dev_Cp<NS>(a.d[q], d0, Tq);
+    amuk = dev_conductivity<NS>(amu1, cp, Tq, Xi);
   }
   const double tmp2_3 = 2.0 / 3.0;
   double s11 = (2.0 * ux - tmp2_3 * div) * amu1;
@@ -409,8 +412,7 @@ __global__ void __launch_bounds__(256) k_visc_ev(ViscArgs a) {
   double s33 = (2.0 * wz - tmp2_3 * div) * amu1;
   double s12 = (uy + vx) * amu1, s13 = (uz + wx) * amu1, s23 = (vz + wy) * amu1;
   double qx = 0.0, qy = 0.0, qz = 0.0;
-  if (a.qpx) { qx = a.qpx[nn]; qy = a.qpy[nn]; qz = a.qpz[nn]; }
-  double uq = a.u[q], vq = a.v[q], wq = a.w[q];
+  if constexpr (NS > 1) { qx = a.qpx[nn]; qy = a.qpy[nn]; qz = a.qpz[nn]; }
   double E1 = uq * s11 + vq * s12 + wq * s13 + amuk * Tx + qx;
   double E2 = uq * s12 + vq * s22 + wq * s23 + amuk * Ty + qy;
   double E3 = uq * s13 + vq * s23 + wq * s33 + amuk * Tz + qz;
@@ -424,19 +426,215 @@ __global__ void __launch_bounds__(256) k_visc_ev(ViscArgs a) {
   }
 }
 
-template <bool SEP>
-__global__ void __launch_bounds__(256) k_visc_div(const double* const* ev, double* du, Geo g) {
-  int i, j, k;
-  if (!cell_of((long long)blockIdx.x * blockDim.x + threadIdx.x, i, j, k)) return;
-  const int q = hidx(i, j, k), nn = nidx(i, j, k);
-  double ajac = metric_jac<SEP>(g, i, j, k, q);
+// asynchronous 8-byte global -> shared copies (cp.async, completed per thread by commit/wait
+// groups); an invalid source fills the destination with zeros and reads nothing
+__device__ __forceinline__ void cp_async8(double* dst, const double* src, bool valid) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(d), "l"(src), "r"(valid ? 8 : 0) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+// k_visc_ev as a 2.5-D stencil: a VE_TX x VE_TY tile of (i, j) columns marches along a chunk of
+// VE_KC planes in k. The x / y neighbours of (u, v, w, T) come from a shared-memory copy of the
+// current plane with an HZ-point halo, the z neighbours from a ring of the tile's own columns, so
+// each value is read from global memory about twice per sweep instead of once per stencil use.
+// The copies of plane k+1 (and ring plane k+HZ+1) are in flight while plane k is computed: the
+// halo plane is double-buffered and the ring has 2 HZ + 2 slots. HZ = 3 for CD6, 4 for CD8.
+#ifndef OCFD_VE_MINB
+#define OCFD_VE_MINB 2  // resident blocks per SM given to the register allocator
+#endif
+constexpr int VE_TX = 32, VE_TY = 8, VE_KC = 16, VE_THREADS = VE_TX * VE_TY;
+template <int HZ>
+struct VeTile {
+  static constexpr int W = VE_TX + 2 * HZ, HH = VE_TY + 2 * HZ, PL = W * HH;  // halo plane
+  static constexpr int RS = 2 * HZ + 2;                                         // ring slots
+  static constexpr size_t smem = sizeof(double) * (size_t)(2 * 4 * PL + RS * 4 * VE_THREADS);
+};
+
+template <int NS, bool SEP, int HZ>
+__global__ void __launch_bounds__(VE_THREADS, OCFD_VE_MINB) k_visc_ev(ViscArgs a) {
+  using TT = VeTile<HZ>;
+  constexpr int W = TT::W, PL = TT::PL, RS = TT::RS, CD = HZ == 3 ? 6 : 8;
+  extern __shared__ double smem[];
+  double* pl = smem;                 // [2][4][HH][W]: u, v, w, T of planes k, k+1 with the halo
+  double* ring = smem + 2 * 4 * PL;  // [RS][4][VE_THREADS]: planes k-HZ .. k+HZ+1, own columns
+  const int tid = threadIdx.x, tx = tid % VE_TX, ty = tid / VE_TX;
+  const int i0 = blockIdx.x * VE_TX + 1, j0 = blockIdx.y * VE_TY + 1, k0 = blockIdx.z * VE_KC + 1;
+  const int i = i0 + tx, j = j0 + ty;
+  const int k1 = min(k0 + VE_KC - 1, cC.nz);
+  const int imax = cC.nx + OCFD_L, jmax = cC.ny + OCFD_L;  // last index of the halo arrays
+  const bool in_array = i <= imax && j <= jmax;
+  const bool active = i <= cC.nx && j <= cC.ny;
+  const double* fl[4] = {a.u, a.v, a.w, a.T};
+  auto ring_issue = [&](int kk) {  // kk >= 1 - HZ
+    double* r = ring + ((kk + 4 * RS) % RS) * 4 * VE_THREADS + tid;
+    const int q = in_array ? hidx(i, j, kk) : 0;
 #pragma unroll
-  for (int m = 0; m < 4; m++) {
-    double uk = cdiff(ev[m], q, 0, i, cC.nx);
-    double ui = cdiff(ev[4 + m], q, 1, j, cC.ny);
-    double us = cdiff(ev[8 + m], q, 2, k, cC.nz);
-    double* o = du + (size_t)(m + 1) * cC.N + nn;
-    *o = *o + (uk + ui + us) * ajac;
+    for (int f = 0; f < 4; f++) cp_async8(r + f * VE_THREADS, fl[f] + q, in_array);
+  };
+  auto plane_issue = [&](int k, int b) {
+    double* dst = pl + b * 4 * PL;
+#pragma unroll
+    for (int it = 0; it < (PL + VE_THREADS - 1) / VE_THREADS; it++) {
+      const int r = tid + it * VE_THREADS;
+      if (r < PL) {
+        const int yy = r / W, xx = r - yy * W;
+        const int ii = i0 - HZ + xx, jj = j0 - HZ + yy;
+        const bool ok = ii <= imax && jj <= jmax;
+        const int q = ok ? hidx(ii, jj, k) : 0;
+#pragma unroll
+        for (int f = 0; f < 4; f++) cp_async8(dst + f * PL + r, fl[f] + q, ok);
+      }
+    }
+  };
+  for (int kk = k0 - HZ; kk <= k0 + HZ; kk++) ring_issue(kk);
+  plane_issue(k0, 0);
+  cp_async_commit();
+
+  for (int k = k0; k <= k1; k++) {
+    const int b = (k - k0) & 1;
+    if (k < k1) {  // prefetch the next plane
+      ring_issue(k + HZ + 1);
+      plane_issue(k + 1, b ^ 1);
+    }
+    cp_async_commit();
+    cp_async_wait<1>();  // everything but the prefetch has landed
+    __syncthreads();
+    if (active) {
+      int sl[2 * HZ + 1];  // ring slot of plane k + m at sl[m + HZ]
+      {
+        int c = (k - HZ + 4 * RS) % RS;
+#pragma unroll
+        for (int m = 0; m <= 2 * HZ; m++) {
+          sl[m] = c;
+          c = c + 1 == RS ? 0 : c + 1;
+        }
+      }
+      const double* cur = pl + b * 4 * PL;
+      double g[4][3];
+#pragma unroll
+      for (int f = 0; f < 4; f++) {
+        const double* row = cur + f * PL + (ty + HZ) * W + tx + HZ;
+        g[f][0] = cdiff_g<CD>([&](int m) { return row[m]; }, 0, i, cC.nx);
+        g[f][1] = cdiff_g<CD>([&](int m) { return row[m * W]; }, 1, j, cC.ny);
+        g[f][2] = cdiff_g<CD>([&](int m) { return ring[(sl[m + HZ] * 4 + f) * VE_THREADS + tid]; }, 2, k, cC.nz);
+      }
+      const double* c0 = cur + (ty + HZ) * W + tx + HZ;
+      visc_point<NS, SEP>(a, i, j, k, g, c0[0], c0[PL], c0[2 * PL], c0[3 * PL]);
+    }
+    __syncthreads();  // plane buffer b and ring slot k-HZ are refilled next
+  }
+}
+
+struct DivArgs {
+  const double* ev[12];  // Ev1 (4), Ev2 (4), Ev3 (4) halo arrays, periodic halos exchanged
+  double* du;
+  Geo g;
+};
+
+// k_visc_div on the same marching tiles as k_visc_ev: Ev1 is differentiated along x from a
+// plane copy with an x halo, Ev2 along y from a plane copy with a y halo, Ev3 along z from a
+// ring of the tile's columns (double-buffered planes, 2 HZ + 2 ring slots, next plane in flight);
+// du(2..5) += (dEv1/dxi + dEv2/deta + dEv3/dzeta) * Jac (OCFD_viscous.f90:114-129).
+template <int HZ>
+struct VdTile {
+  static constexpr int W = VE_TX + 2 * HZ, HH = VE_TY + 2 * HZ;
+  static constexpr int PX = VE_TY * W, PY = HH * VE_TX, RS = 2 * HZ + 2;
+  static constexpr size_t smem = sizeof(double) * (size_t)(2 * 4 * (PX + PY) + RS * 4 * VE_THREADS);
+};
+
+template <bool SEP, int HZ>
+__global__ void __launch_bounds__(VE_THREADS, 2) k_visc_div(DivArgs a) {
+  using TT = VdTile<HZ>;
+  constexpr int W = TT::W, PX = TT::PX, PY = TT::PY, RS = TT::RS, CD = HZ == 3 ? 6 : 8;
+  extern __shared__ double smem[];
+  double* pb = smem;                        // [2][ [4][VE_TY][W] Ev1 | [4][HH][VE_TX] Ev2 ]
+  double* ring = smem + 2 * 4 * (PX + PY);  // [RS][4][VE_THREADS]: Ev3 of planes k-HZ .. k+HZ+1
+  const int tid = threadIdx.x, tx = tid % VE_TX, ty = tid / VE_TX;
+  const int i0 = blockIdx.x * VE_TX + 1, j0 = blockIdx.y * VE_TY + 1, k0 = blockIdx.z * VE_KC + 1;
+  const int i = i0 + tx, j = j0 + ty;
+  const int k1 = min(k0 + VE_KC - 1, cC.nz);
+  const int imax = cC.nx + OCFD_L, jmax = cC.ny + OCFD_L;
+  const bool in_array = i <= imax && j <= jmax;
+  const bool active = i <= cC.nx && j <= cC.ny;
+  auto ring_issue = [&](int kk) {
+    double* r = ring + ((kk + 4 * RS) % RS) * 4 * VE_THREADS + tid;
+    const int q = in_array ? hidx(i, j, kk) : 0;
+#pragma unroll
+    for (int m = 0; m < 4; m++) cp_async8(r + m * VE_THREADS, a.ev[8 + m] + q, in_array);
+  };
+  auto plane_issue = [&](int k, int b) {
+    double* px = pb + b * 4 * (PX + PY);
+    double* py = px + 4 * PX;
+#pragma unroll
+    for (int it = 0; it < (PX + VE_THREADS - 1) / VE_THREADS; it++) {
+      const int r = tid + it * VE_THREADS;
+      if (r < PX) {
+        const int yy = r / W, xx = r - yy * W;
+        const int ii = i0 - HZ + xx, jj = j0 + yy;
+        const bool ok = ii <= imax && jj <= jmax;
+        const int q = ok ? hidx(ii, jj, k) : 0;
+#pragma unroll
+        for (int m = 0; m < 4; m++) cp_async8(px + m * PX + r, a.ev[m] + q, ok);
+      }
+    }
+#pragma unroll
+    for (int it = 0; it < (PY + VE_THREADS - 1) / VE_THREADS; it++) {
+      const int r = tid + it * VE_THREADS;
+      if (r < PY) {
+        const int yy = r / VE_TX, xx = r - yy * VE_TX;
+        const int ii = i0 + xx, jj = j0 - HZ + yy;
+        const bool ok = ii <= imax && jj <= jmax;
+        const int q = ok ? hidx(ii, jj, k) : 0;
+#pragma unroll
+        for (int m = 0; m < 4; m++) cp_async8(py + m * PY + r, a.ev[4 + m] + q, ok);
+      }
+    }
+  };
+  for (int kk = k0 - HZ; kk <= k0 + HZ; kk++) ring_issue(kk);
+  plane_issue(k0, 0);
+  cp_async_commit();
+
+  const long long N = cC.N;
+  for (int k = k0; k <= k1; k++) {
+    const int b = (k - k0) & 1;
+    if (k < k1) {
+      ring_issue(k + HZ + 1);
+      plane_issue(k + 1, b ^ 1);
+    }
+    cp_async_commit();
+    cp_async_wait<1>();
+    __syncthreads();
+    if (active) {
+      int sl[2 * HZ + 1];
+      {
+        int c = (k - HZ + 4 * RS) % RS;
+#pragma unroll
+        for (int m = 0; m <= 2 * HZ; m++) {
+          sl[m] = c;
+          c = c + 1 == RS ? 0 : c + 1;
+        }
+      }
+      const double* px = pb + b * 4 * (PX + PY);
+      const double* py = px + 4 * PX;
+      const double ajac = metric_jac<SEP>(a.g, i, j, k, hidx(i, j, k));
+      const int nn = nidx(i, j, k);
+#pragma unroll
+      for (int m = 0; m < 4; m++) {
+        const double* rx = px + m * PX + ty * W + tx + HZ;
+        const double* ry = py + m * PY + (ty + HZ) * VE_TX + tx;
+        double uk = cdiff_g<CD>([&](int o) { return rx[o]; }, 0, i, cC.nx);
+        double ui = cdiff_g<CD>([&](int o) { return ry[o * VE_TX]; }, 1, j, cC.ny);
+        double us = cdiff_g<CD>([&](int o) { return ring[(sl[o + HZ] * 4 + m) * VE_THREADS + tid]; }, 2, k, cC.nz);
+        double* o = a.du + (size_t)(m + 1) * N + nn;
+        *o = *o + (uk + ui + us) * ajac;
+      }
+    }
+    __syncthreads();
   }
 }
 

@@ -57,7 +57,6 @@ struct Lib {
   double *inlet = nullptr, *upper = nullptr, *wall = nullptr, *ht_dev = nullptr;
   int *nonref = nullptr, *patches = nullptr;
   int npatch = 0;
-  double** ev_ptrs = nullptr;
   DevStatus* sdev = nullptr;
   DevStatus* shost = nullptr;
   double* ht_host = nullptr;
@@ -301,6 +300,33 @@ void sensor() {
   }
 }
 
+// k_visc_ev over (i, j) tiles and k chunks; HZ = the CD6 / CD8 stencil half-width
+template <int NS, bool SEP, int HZ>
+void visc_ev_go(const ViscArgs& va) {
+  constexpr size_t sm = VeTile<HZ>::smem;
+  static bool attr = false;
+  if (!attr) {
+    CK(cudaFuncSetAttribute(k_visc_ev<NS, SEP, HZ>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    attr = true;
+  }
+  const ocfd_params& P = L->P;
+  dim3 grid(nblk(P.nx, VE_TX), nblk(P.ny, VE_TY), nblk(P.nz, VE_KC));
+  k_visc_ev<NS, SEP, HZ><<<grid, VE_THREADS, sm, L->st>>>(va);
+}
+
+template <bool SEP, int HZ>
+void visc_div_go(const DivArgs& da) {
+  constexpr size_t sm = VdTile<HZ>::smem;
+  static bool attr = false;
+  if (!attr) {
+    CK(cudaFuncSetAttribute(k_visc_div<SEP, HZ>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    attr = true;
+  }
+  const ocfd_params& P = L->P;
+  dim3 grid(nblk(P.nx, VE_TX), nblk(P.ny, VE_TY), nblk(P.nz, VE_KC));
+  k_visc_div<SEP, HZ><<<grid, VE_THREADS, sm, L->st>>>(da);
+}
+
 template <int NS>
 void stage_t(int krk, double dt1) {
   const long long N = L->hc.N, H = L->hc.H;
@@ -368,8 +394,9 @@ void stage_t(int krk, double dt1) {
     va.g = L->geo;
     {
       KTimer t(KC_VISC_EV);
-      if (L->sep) k_visc_ev<NS, true><<<nblk(N, 256), 256, 0, L->st>>>(va);
-      else k_visc_ev<NS, false><<<nblk(N, 256), 256, 0, L->st>>>(va);
+      const bool cd8 = L->P.scheme_vis == OCFD_SCHEME_CD8;
+      if (L->sep) cd8 ? visc_ev_go<NS, true, 4>(va) : visc_ev_go<NS, true, 3>(va);
+      else cd8 ? visc_ev_go<NS, false, 4>(va) : visc_ev_go<NS, false, 3>(va);
       LAUNCH_CHECK();
     }
     exchange({L->ev[0], L->ev[1], L->ev[2], L->ev[3]}, 1);
@@ -377,8 +404,13 @@ void stage_t(int krk, double dt1) {
     exchange({L->ev[8], L->ev[9], L->ev[10], L->ev[11]}, 4);
     {
       KTimer t(KC_VISC_DIV);
-      if (L->sep) k_visc_div<true><<<nblk(N, 256), 256, 0, L->st>>>(L->ev_ptrs, L->du, L->geo);
-      else k_visc_div<false><<<nblk(N, 256), 256, 0, L->st>>>(L->ev_ptrs, L->du, L->geo);
+      DivArgs da{};
+      for (int m = 0; m < 12; m++) da.ev[m] = L->ev[m];
+      da.du = L->du;
+      da.g = L->geo;
+      const bool cd8 = L->P.scheme_vis == OCFD_SCHEME_CD8;
+      if (L->sep) cd8 ? visc_div_go<true, 4>(da) : visc_div_go<true, 3>(da);
+      else cd8 ? visc_div_go<false, 4>(da) : visc_div_go<false, 3>(da);
       LAUNCH_CHECK();
     }
   }
@@ -857,9 +889,7 @@ int ocfd_gpu_init(const ocfd_params* p, const ocfd_thermo* th, const ocfd_kineti
     L->ht_dev = alloc<double>(1);
     L->patches = alloc<int>(6 * 20);
     L->sdev = alloc<DevStatus>(1);
-    L->ev_ptrs = alloc<double*>(12);
     double** met_ptrs = alloc<double*>(19);
-    CK(cudaMemcpyAsync(L->ev_ptrs, L->ev, sizeof(double*) * 12, cudaMemcpyHostToDevice, L->st));
     CK(cudaMemsetAsync(L->sdev, 0, sizeof(DevStatus), L->st));
 
     // allocate_flow_data initial values (OCFD_allocate_data.f90:53-67)
