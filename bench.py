@@ -120,6 +120,16 @@ class Clocks:
 ALG_BYTES_PER_CELL = {"flux_x": 88, "flux_y": 128, "flux_z": 128, "visc_ev": 144, "visc_div": 160,
                       "rk_prims": 240}
 
+# algorithmic FP64 operations per cell of one launch on the flat-plate workload (hand count of the
+# kernels' arithmetic; a division or a square root counts as one operation; UD7L interfaces: the
+# ~2 % of interfaces that take WENO5 are not counted):
+#  split (Steger-Warming + sound speed + separable metric) ~160 per point, (C + 8) / C points per
+#  cell (C = 56 for x, 24 for y / z); UD7L 15 per component and sign, 150 per interface,
+#  (C + 1) / C interfaces per cell; flux difference 4-6 per component.
+#  visc_ev: 12 CD6 derivatives (8 each), metrics 12, chain rule 60, Sutherland + Cp + conductivity
+#  ~30, stresses and heat flux 48, Ev 60.  visc_div: 12 CD6 derivatives, sum and Jacobian 16.
+ALG_FLOPS_PER_CELL = {"flux_x": 356, "flux_y": 394, "flux_z": 402, "visc_ev": 305, "visc_div": 115}
+
 
 def main_reference(a):
     """The reference's algorithm on the host cores: the C++ restatement of the Fortran (no
@@ -245,10 +255,20 @@ def main_ours(a):
         if dom in tr:
             traffic = tr[dom] * c.ncell
     fp64 = solver.fp64_peak_gflops()
+    # the build keeps multiplies and adds separate (no FMA), so the FP64 operation peak is half
+    # the measured FMA flop rate
+    fp64_ops_peak = fp64 / 2.0
+    fp64_roof = None
+    if a.workload == "flatplate" and dom in ALG_FLOPS_PER_CELL:
+        ops = ALG_FLOPS_PER_CELL[dom] * c.ncell
+        ach = ops / (dom_ms * 1e-3) / 1e9
+        fp64_roof = {"achieved": ach, "peak": fp64_ops_peak, "unit": "GFLOP/s", "frac": ach / fp64_ops_peak,
+                     "alg_flops_per_launch": ops, "peak_kind": "measured FP64 FMA rate / 2 (no-FMA build)"}
     roof = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm, "unit": "GB/s",
             "frac": achieved / hbm, "traffic": traffic, "peak_kind": hbm_kind,
             "alg_bytes_per_launch": alg, "avg_launch_ms": dom_ms,
             "share_of_step": prof[dom][0] / 2.0 / step_ms if step_ms > 0 else None,
+            "fp64": fp64_roof,
             "fp64_fma_peak_gflops_measured": fp64,
             "kernel_shares": {k: round(v[0] / 2.0 / step_ms, 4) for k, v in prof.items() if v[1] > 0}}
 

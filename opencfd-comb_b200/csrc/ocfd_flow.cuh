@@ -234,6 +234,28 @@ __global__ void __launch_bounds__(FLUX_THREADS, Tile<DIR>::MINB) k_flux(FluxArgs
   }
   __syncthreads();
 
+  // the y / z sweeps add into du: load this thread's phase-3 cells now, so the loads are in
+  // flight during phase 2
+  constexpr int R3 = (C * NL + FLUX_THREADS - 1) / FLUX_THREADS;
+  const long long N = cC.N;
+  double pre[R3][NC];
+  if (DIR != 0) {
+#pragma unroll
+    for (int r = 0; r < R3; r++) {
+      const int idx = threadIdx.x + r * FLUX_THREADS;
+      int t, l;
+      if (DIR == 0) { t = idx % C; l = idx / C; }
+      else { l = idx % NL; t = idx / NL; }
+      if (idx < C * NL && l0 + l <= nl_max && t < ncell) {
+        int i, j, k;
+        coords(s0 + t, l, i, j, k);
+        const int nn = nidx(i, j, k);
+#pragma unroll
+        for (int c = 0; c < NC; c++) pre[r][c] = a.out[(size_t)c * N + nn];
+      }
+    }
+  }
+
   // phase 2: numerical fluxes at interfaces s0-1 .. s0-1+ncell
   const int nq = HYB ? *sqn : 0;
   const int nfast = NCS * NI;
@@ -271,12 +293,13 @@ __global__ void __launch_bounds__(FLUX_THREADS, Tile<DIR>::MINB) k_flux(FluxArgs
 
   // phase 3: flux difference into du
   const double h1 = cC.h1[DIR];
-  const long long N = cC.N;
-  for (int idx = threadIdx.x; idx < C * NL; idx += FLUX_THREADS) {
+#pragma unroll
+  for (int r = 0; r < R3; r++) {
+    const int idx = threadIdx.x + r * FLUX_THREADS;
     int t, l;
     if (DIR == 0) { t = idx % C; l = idx / C; }
     else { l = idx % NL; t = idx / NL; }
-    if (l0 + l > nl_max || t >= ncell) continue;
+    if (idx >= C * NL || l0 + l > nl_max || t >= ncell) continue;
     int i, j, k;
     coords(s0 + t, l, i, j, k);
     const int nn = nidx(i, j, k);
@@ -290,8 +313,8 @@ __global__ void __launch_bounds__(FLUX_THREADS, Tile<DIR>::MINB) k_flux(FluxArgs
       double val = (hp[i1] - hp[i0] + hm[i1] - hm[i0]) * h1;
       double* o = a.out + (size_t)c * N + nn;
       if (DIR == 0) *o = val;
-      else if (DIR == 1) *o = *o + val;
-      else *o = -(*o + val) * ajac;
+      else if (DIR == 1) *o = pre[r][c] + val;
+      else *o = -(pre[r][c] + val) * ajac;
     }
     if (DIR == 2 && !SCALAR && cC.if_mass_force == 1) {
       int q = hidx(i, j, k);
@@ -600,11 +623,24 @@ __global__ void __launch_bounds__(VE_THREADS, 2) k_visc_div(DivArgs a) {
   cp_async_commit();
 
   const long long N = cC.N;
+  // du(2..5) of the current and the next plane in registers: the next plane's loads are in
+  // flight while the current one is computed
+  double duc[4], dun[4];
+  if (active) {
+    const int nn = nidx(i, j, k0);
+#pragma unroll
+    for (int m = 0; m < 4; m++) duc[m] = a.du[(size_t)(m + 1) * N + nn];
+  }
   for (int k = k0; k <= k1; k++) {
     const int b = (k - k0) & 1;
     if (k < k1) {
       ring_issue(k + HZ + 1);
       plane_issue(k + 1, b ^ 1);
+      if (active) {
+        const int nn = nidx(i, j, k + 1);
+#pragma unroll
+        for (int m = 0; m < 4; m++) dun[m] = a.du[(size_t)(m + 1) * N + nn];
+      }
     }
     cp_async_commit();
     cp_async_wait<1>();
@@ -630,11 +666,12 @@ __global__ void __launch_bounds__(VE_THREADS, 2) k_visc_div(DivArgs a) {
         double uk = cdiff_g<CD>([&](int o) { return rx[o]; }, 0, i, cC.nx);
         double ui = cdiff_g<CD>([&](int o) { return ry[o * VE_TX]; }, 1, j, cC.ny);
         double us = cdiff_g<CD>([&](int o) { return ring[(sl[o + HZ] * 4 + m) * VE_THREADS + tid]; }, 2, k, cC.nz);
-        double* o = a.du + (size_t)(m + 1) * N + nn;
-        *o = *o + (uk + ui + us) * ajac;
+        a.du[(size_t)(m + 1) * N + nn] = duc[m] + (uk + ui + us) * ajac;
       }
     }
     __syncthreads();
+#pragma unroll
+    for (int m = 0; m < 4; m++) duc[m] = dun[m];
   }
 }
 
