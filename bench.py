@@ -40,11 +40,17 @@ def parse():
     ap.add_argument("--steps", type=int, default=40)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="flatplate", choices=["flatplate", "isotropic"])
+    ap.add_argument("--workload", default="flatplate", choices=["flatplate", "isotropic", "jet", "reactors"],
+                    help="flatplate = the headline configuration; isotropic, jet and reactors are the other "
+                         "configurations of the metric (64^3 decaying turbulence, the 384x256x256 reacting H2 jet, "
+                         "2^20 batched 0-D reactors)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=5)
-    ap.add_argument("--nz", type=int, default=128, help="spanwise cells of the flat-plate workload (128 = full)")
+    ap.add_argument("--character", action="store_true",
+                    help="characteristic-space inviscid flux (IF_Scheme_Character = 1) instead of component-wise")
+    ap.add_argument("--nz", type=int, default=None,
+                    help="cells along z (flat plate: 128 = full; jet: 256 = full), for small profiling runs")
     return ap.parse_args()
 
 
@@ -52,6 +58,10 @@ def make_case(workload, nz=None):
     from ocfd_b200 import cases
     if workload == "isotropic":
         return cases.isotropic(n=64), "isotropic-64^3-WENO5-CD6-SW (decaying turbulence, M_t 0.3, Re_lambda 70)"
+    if workload == "jet":
+        n = nz or 256
+        c = cases.jet(nx=384, ny=256, nz=n)
+        return c, "jet-%dx%dx%d-H2air-9sp-19reac-WENO5-CD6-Wilke-implicitChem" % c.shape
     c = cases.flatplate(nx=1024, ny=160, nz=nz or 128, scheme="HYBRID")
     return c, "flatplate-1024x160x%d-M2.25-HYBRID(UD7L/WENO7/WENO5)-CD6-SW-BoundaryLayerBC" % (nz or 128)
 
@@ -117,8 +127,9 @@ class Clocks:
 #  visc_ev: read u,v,w,T,d,di (6) ; write Ev1..Ev3 (12)                   = 18 doubles
 #  visc_div: read Ev (12) ; read + write du(2..5) (8)                     = 20 doubles
 #  rk_prims: read f,fn,du,di,d (17) ; write f,d,u,v,w,T,p,Et,di (13)      = 30 doubles
+#  chem (reacting workloads): read + write di (Ns), Et, f5, read T, p          = 22 doubles (Ns = 9)
 ALG_BYTES_PER_CELL = {"flux_x": 88, "flux_y": 128, "flux_z": 128, "visc_ev": 144, "visc_div": 160,
-                      "rk_prims": 240}
+                      "rk_prims": 240, "chem": 176}
 
 # algorithmic FP64 operations per cell of one launch on the flat-plate workload (hand count of the
 # kernels' arithmetic; a division or a square root counts as one operation; UD7L interfaces: the
@@ -139,28 +150,37 @@ def main_reference(a):
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import pyoracle
     cores = pyoracle.lib().ocfd_cpu_set_threads(os.cpu_count() or 1)
+    if a.workload == "reactors":
+        return reactors_reference(a, pyoracle, cores)
     # size the per-step sample so that warmup + steps take about two minutes
-    probe, _ = make_case(a.workload, nz=8) if a.workload == "flatplate" else make_case(a.workload)
-    o = pyoracle.OracleSolver(probe)
-    o.init_state()
-    t0 = time.perf_counter()
-    o.step(probe.dt, 0.0)
-    rate = probe.ncell / (time.perf_counter() - t0)
-    o.close()
+    rate = 0.0
+    if a.workload == "flatplate":
+        probe, _ = make_case(a.workload, nz=8)
+        o = pyoracle.OracleSolver(probe)
+        o.init_state()
+        t0 = time.perf_counter()
+        o.step(probe.dt, 0.0)
+        rate = probe.ncell / (time.perf_counter() - t0)
+        o.close()
     if a.workload == "flatplate":
         nz = int(max(8, min(128, 120.0 * rate / (1024 * 160 * (a.steps + a.warmup)))))
         c, name = make_case(a.workload, nz=nz)
         sample = "per step: one full time step of a 1024x160x%d slab of the workload (z periodic)" % nz
+    elif a.workload == "jet":
+        from ocfd_b200 import cases
+        c, name = cases.jet(nx=96, ny=64, nz=64), make_case("jet", nz=8)[1].replace("96x64x8", "384x256x256")
+        sample = "per step: one reacting time step of the jet on a 96x64x64 grid (same physics)"
     else:
         c, name = make_case(a.workload)
         sample = "per step: one full time step of the 64^3 workload"
+    reac, nsub = int(getattr(c, "if_reaction", 0) or 0), int(getattr(c, "nsub", 1) or 1)
     o = pyoracle.OracleSolver(c)
     o.init_state()
     for s in range(a.warmup):
-        o.step(c.dt, s * c.dt)
+        o.step(c.dt, s * c.dt, reac, nsub)
     t0 = time.perf_counter()
     for s in range(a.steps):
-        o.step(c.dt, (a.warmup + s) * c.dt)
+        o.step(c.dt, (a.warmup + s) * c.dt, reac, nsub)
     el = time.perf_counter() - t0
     o.close()
     val = c.ncell * a.steps / el / 1e6
@@ -171,6 +191,107 @@ def main_reference(a):
                       "sample_cells": c.ncell},
            "cpu_baseline": {"value": val, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample},
            "e2e": {"value": val, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out))
+    return 0
+
+
+# ---------------------------------------------------------------- batched 0-D reactors (2^20)
+RMETRIC = "Mreactor-solves/s on 1 B200: 2^20 H2-air reactors, implicit Euler, uneven sub-steps"
+RUNIT = "Mreactor-solves/s"
+
+
+def reactors_reference(a, pyoracle, cores):
+    from ocfd_b200 import abi, cases
+    n = 8192
+    names, th, kin, di, E, dt, nsub, T = cases.reactors(n=n, seed=1)
+    for s in range(a.warmup):
+        pyoracle.chem_batch(th, kin, 1, abi.CHEM_IMPLICIT, di.copy(), E.copy(), dt, nsub)
+    t0 = time.perf_counter()
+    for s in range(a.steps):
+        pyoracle.chem_batch(th, kin, 1, abi.CHEM_IMPLICIT, di.copy(), E.copy(), dt, nsub)
+    el = time.perf_counter() - t0
+    val = n * a.steps / el / 1e6
+    out = {"metric": RMETRIC, "value": val, "unit": RUNIT, "n_gpus": a.gpus, "steps": a.steps, "warmup": a.warmup,
+           "ms_per_step": el * 1e3 / a.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+           "dtype": "f64", "data": "synthetic (seeded)", "impl": "reference",
+           "config": {"workload": "reactors-2^20-H2air-9sp-implicitEuler", "sample_reactors": n},
+           "cpu_baseline": {"value": val, "unit": RUNIT, "cores": cores, "kind": "port",
+                            "sample": "per step: %d reactors drawn like the 2^20 workload" % n},
+           "e2e": {"value": val, "unit": RUNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out))
+    return 0
+
+
+def main_reactors(a):
+    """2^20 independent constant-volume H2-air reactors through the persistent work-queue kernel
+    (ocfd_gpu_chem_batch_device); one step = one pass over all reactors."""
+    import numpy as np
+    import torch
+    from ocfd_b200 import abi, cases, solver
+    L = solver.lib()
+    import ctypes as C
+    n = 2 ** 20
+    names, th, kin, di, E, dt, nsub, T = cases.reactors(n=n, seed=0)
+    solver.chem_setup(th, kin, 1, abi.CHEM_IMPLICIT)
+    dev = torch.device("cuda", 0)
+    d_di0, d_e0 = torch.from_numpy(di).to(dev), torch.from_numpy(E).to(dev)
+    d_dt, d_ns = torch.from_numpy(dt).to(dev), torch.from_numpy(nsub).to(dev)
+    d_di, d_e = d_di0.clone(), d_e0.clone()
+    torch.cuda.synchronize()
+    # the library launches on its own stream: the restoring copies and the events go there too
+    st = torch.cuda.ExternalStream(L.ocfd_gpu_stream())
+
+    def one():
+        d_di.copy_(d_di0)
+        d_e.copy_(d_e0)
+        solver.chem_batch_device(n, d_di.data_ptr(), d_e.data_ptr(), d_dt.data_ptr(), d_ns.data_ptr())
+
+    with torch.cuda.stream(st):
+        for s in range(a.warmup):
+            one()
+        st.synchronize()
+        with Clocks(0) as clk:
+            ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            ev0.record(st)
+            for s in range(a.steps):
+                one()
+            ev1.record(st)
+            st.synchronize()
+    ms = ev0.elapsed_time(ev1)
+    value = n * a.steps / (ms * 1e-3) / 1e6
+    # e2e: host arrays through ocfd_gpu_chem_batch (copies in and out inside the call)
+    e2e = None
+    if not a.no_e2e:
+        hdi, he = di.copy(), E.copy()
+        solver.chem_batch(hdi, he, dt, nsub)
+        t0 = time.perf_counter()
+        ne = max(1, min(a.steps, 5))
+        for s in range(ne):
+            hdi[:], he[:] = di, E
+            solver.chem_batch(hdi, he, dt, nsub)
+        el = time.perf_counter() - t0
+        e2e = {"value": n * ne / el / 1e6, "unit": RUNIT, "h2d_bytes_per_step": di.nbytes + E.nbytes + dt.nbytes + nsub.nbytes,
+               "d2h_bytes_per_step": di.nbytes + E.nbytes, "timing": "host wall clock around each synchronous call"}
+    cpu = None
+    if not a.no_cpu:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import pyoracle
+        cores = pyoracle.lib().ocfd_cpu_set_threads(os.cpu_count() or 1)
+        m = 8192
+        _, _, _, sdi, sE, sdt, sns, _ = cases.reactors(n=m, seed=1)
+        t0 = time.perf_counter()
+        pyoracle.chem_batch(th, kin, 1, abi.CHEM_IMPLICIT, sdi.copy(), sE.copy(), sdt, sns)
+        el = time.perf_counter() - t0
+        cpu = {"value": m / el / 1e6, "unit": RUNIT, "cores": cores, "kind": "port",
+               "sample": "%d reactors drawn like the 2^20 workload" % m}
+    sub = int(nsub.sum())
+    out = {"metric": RMETRIC, "value": value, "unit": RUNIT, "n_gpus": 1, "steps": a.steps, "warmup": a.warmup,
+           "ms_per_step": ms / a.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+           "dtype": "f64", "data": "synthetic (seeded)",
+           "config": {"workload": "reactors-2^20-H2air-9sp-implicitEuler", "reactors": n, "substeps_total": sub,
+                      "substeps_per_s": sub * a.steps / (ms * 1e-3),
+                      "l2": "inputs re-copied from a pristine device copy before each pass"},
+           "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": None, "clocks": clk.summary()}
     print(json.dumps(out))
     return 0
 
@@ -209,13 +330,17 @@ def main_ours(a):
         return float(t.item())
 
     c, name = make_case(a.workload, nz=a.nz)
+    if a.character:
+        c.params.if_scheme_character = 1
+        name += "-characteristic"
     g = solver.Solver(c)
     state_gb = L.ocfd_gpu_device_bytes() / 1e9
     g.init_state()
     dt = c.dt
     tt = 0.0
     chk = solver._chk
-    chk(L.ocfd_gpu_run(dt, tt, a.warmup, 0, 1))
+    reac, nsub = int(getattr(c, "if_reaction", 0) or 0), int(getattr(c, "nsub", 1) or 1)
+    chk(L.ocfd_gpu_run(dt, tt, a.warmup, reac, nsub))
     tt += a.warmup * dt
 
     # ---- device-resident throughput ----
@@ -223,7 +348,7 @@ def main_ours(a):
     l0 = L.ocfd_gpu_launch_count()
     with Clocks(0) as clk:
         chk(L.ocfd_gpu_event_record(0))
-        chk(L.ocfd_gpu_run(dt, tt, a.steps, 0, 1))
+        chk(L.ocfd_gpu_run(dt, tt, a.steps, reac, nsub))
         chk(L.ocfd_gpu_event_record(1))
         ms = C.c_double()
         chk(L.ocfd_gpu_event_elapsed(0, 1, C.byref(ms)))
@@ -237,7 +362,7 @@ def main_ours(a):
     solver.Solver.profile(True)
     for s in range(2):
         g.tt = tt
-        g.step(dt)
+        g.step(dt, reac, nsub)
         tt += dt
     prof = solver.Solver.profile_read()
     solver.Solver.profile(False)
@@ -298,7 +423,7 @@ def main_ours(a):
         chk(L.ocfd_gpu_event_record(2))
         for s in range(a.e2e_steps):
             chk(L.ocfd_gpu_upload_state(abi.dptr(hf), abi.dptr(hdi), abi.dptr(hpr)))
-            chk(L.ocfd_gpu_run(dt, tt, 1, 0, 1))
+            chk(L.ocfd_gpu_run(dt, tt, 1, reac, nsub))
             tt += dt
             chk(L.ocfd_gpu_download_state(abi.dptr(hf), abi.dptr(hdi), None))
         chk(L.ocfd_gpu_event_record(3))
@@ -321,14 +446,19 @@ def main_ours(a):
         if a.workload == "flatplate":
             cs, _ = make_case("flatplate", nz=16)
             sample = "one time step of a 1024x160x16 slab of the workload (z periodic), after one warm-up step"
+        elif a.workload == "jet":
+            from ocfd_b200 import cases
+            cs = cases.jet(nx=96, ny=64, nz=64)
+            sample = "one reacting time step of the jet on a 96x64x64 grid (same physics), after one warm-up step"
         else:
             cs, _ = make_case("isotropic")
             sample = "one time step of the 64^3 workload after one warm-up step"
         o = pyoracle.OracleSolver(cs)
         o.init_state()
-        o.step(cs.dt, 0.0)
+        creac, cnsub = int(getattr(cs, "if_reaction", 0) or 0), int(getattr(cs, "nsub", 1) or 1)
+        o.step(cs.dt, 0.0, creac, cnsub)
         t0 = time.perf_counter()
-        o.step(cs.dt, cs.dt)
+        o.step(cs.dt, cs.dt, creac, cnsub)
         el = time.perf_counter() - t0
         o.close()
         cpu = {"value": cs.ncell / el / 1e6, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample}
@@ -337,7 +467,7 @@ def main_ours(a):
         out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps,
                "warmup": a.warmup, "ms_per_step": el_ms / a.steps, "higher_is_better": True, "scaling": "weak",
                "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
-               "config": {"workload": name, "cells_per_gpu": c.ncell, "dt": dt, "chemistry": "off (non-reacting air)",
+               "config": {"workload": name, "cells_per_gpu": c.ncell, "dt": dt, "chemistry": ("plain FP64 implicit Euler, %d sub-step(s) per step" % nsub) if reac else "off (non-reacting air)",
                           "parallelism": "replicas x%d (no data-path collective)" % world,
                           "l2": "device state %.1f GB per GPU >> 126 MB L2; no flush between steps" % state_gb},
                "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches),
@@ -351,4 +481,8 @@ def main_ours(a):
 
 if __name__ == "__main__":
     a = parse()
-    sys.exit(main_reference(a) if a.impl == "reference" else main_ours(a))
+    if a.impl == "reference":
+        sys.exit(main_reference(a))
+    if a.workload == "reactors":
+        sys.exit(main_reactors(a) if int(os.environ.get("RANK", "0")) == 0 else 0)
+    sys.exit(main_ours(a))

@@ -42,6 +42,9 @@ struct DevConst {
   double amu0, pr, sc;
   double mu_an[OCFD_MAX_SPEC][4], k_an[OCFD_MAX_SPEC][4];
   double d_an[OCFD_MAX_SPEC][OCFD_MAX_SPEC][4];
+  // Wilke pair constants of comput_vis_coeff, sqrt(Mi(j)/Mi(k)) and sqrt(8*(1+Mi(k)/Mi(j))):
+  // cell-independent, evaluated on the host with the same correctly rounded operations
+  double wk_a[OCFD_MAX_SPEC][OCFD_MAX_SPEC], wk_b[OCFD_MAX_SPEC][OCFD_MAX_SPEC];
   // kinetics
   int nreac, rereac, timeadv;
   int af_type[OCFD_MAX_REAC], tr_reac[OCFD_MAX_REAC];
@@ -396,8 +399,8 @@ __device__ __forceinline__ double dev_viscosity(double T, const double* Xi) {
     double pk0 = 0.0;
 #pragma unroll
     for (int j = 0; j < NS; j++) {
-      double s = 1.0 + sqrt(mui[k] / mui[j] * sqrt(cC.Mi[j] / cC.Mi[k]));
-      double pkj = q2(s) / sqrt(8.0 * (1.0 + cC.Mi[k] / cC.Mi[j]));
+      double s = 1.0 + sqrt(mui[k] / mui[j] * cC.wk_a[k][j]);
+      double pkj = q2(s) / cC.wk_b[k][j];
       pk0 = pk0 + Xi[j] * pkj;
     }
     mu = mu + Xi[k] * mui[k] / pk0;
@@ -428,19 +431,23 @@ __device__ __forceinline__ void dev_diffusion(double* amd, double amu, double T,
     return;
   }
   double L = log(T);
+  // D2(k,j) = D2(min,max) (the reference fills the table symmetrically), so each pair is
+  // evaluated once; walking the pairs (a < b) a-major adds to ds(k) the terms j = 0..k-1 and then
+  // j = k+1..NS-1, the reference's order for every k
+  double ds[NS];
 #pragma unroll
-  for (int k = 0; k < NS; k++) {
-    double ds = 0.0;
+  for (int k = 0; k < NS; k++) ds[k] = 0.0;
 #pragma unroll
-    for (int j = 0; j < NS; j++) {
-      if (j == k) continue;
-      int a = k < j ? k : j, b = k < j ? j : k;  // D2(k,j) = D2(min,max) (symmetric fill of the reference)
+  for (int a = 0; a < NS; a++)
+#pragma unroll
+    for (int b = a + 1; b < NS; b++) {
       double D2 = exp(cC.d_an[a][b][0] + cC.d_an[a][b][1] * L + cC.d_an[a][b][2] * q2(L) + cC.d_an[a][b][3] * q3(L)) *
                   1.0e-4;
-      ds = ds + Xi[j] / D2;
+      ds[a] = ds[a] + Xi[b] / D2;
+      ds[b] = ds[b] + Xi[a] / D2;
     }
-    amd[k] = (1.0 - Xi[k]) / (ds + 1.0e-20) * 1.013e5 / p;
-  }
+#pragma unroll
+  for (int k = 0; k < NS; k++) amd[k] = (1.0 - Xi[k]) / (ds[k] + 1.0e-20) * 1.013e5 / p;
 }
 
 // ---------------------------------------------------------------- reconstructions

@@ -96,9 +96,10 @@ struct Tile<2> {
   static constexpr int C = 24, NL = 16, MINB = 3;
 };
 
-template <int DIR, bool SCALAR>
+// NC components per point: the five flow fluxes, or G species of a scalar sweep
+template <int DIR, int NC_>
 struct FluxTile {
-  static constexpr int C = Tile<DIR>::C, NL = Tile<DIR>::NL, P = C + 8, NC = SCALAR ? 1 : 5;
+  static constexpr int C = Tile<DIR>::C, NL = Tile<DIR>::NL, P = C + 8, NC = NC_;
   static constexpr int NCS = 2 * NC;        // (component, sign) pairs: plus components, then minus
   static constexpr int NI = (C + 1) * NL;   // interfaces of a tile
   static_assert((P * NL) % FLUX_THREADS == 0, "split phase must fill whole rounds");
@@ -107,9 +108,10 @@ struct FluxTile {
 
 struct FluxArgs {
   const double *d, *u, *v, *w, *p, *Et;  // halo arrays
-  const double* fs;                      // scalar (species density) for SCALAR sweeps
+  const double* fs;                      // species densities di (Ns x H) for SCALAR sweeps
   const double* Rh;                      // hybrid sensor (halo array)
-  double* out;                           // du (5 x N) or Dus (N)
+  double* out;                           // du (5 x N) or Dus of every species (Ns x N)
+  int nbz;                               // blocks along the third grid dimension per species group
   Geo g;
 };
 
@@ -140,9 +142,11 @@ __device__ __forceinline__ double ud7l_signed(const double* v, bool plus) {
 //     UD7L, then the listed ones run the general reconstruction (closures, WENO5/7, OMP6), so a
 //     warp never carries the WENO branches for the lanes that need only UD7L;
 //  3. flux difference (hh(i) - hh(i-1)) / d, combined into du as the reference does per sweep.
-template <int DIR, int SCHEME, int SPLIT, bool SEP, bool SCALAR>
+// SCALAR sweeps (du_scaler_invis, OCFD_scaler_inviscous.f90) carry G species per block: the
+// split velocity is formed once per point for the group, and blockIdx.z also selects the group.
+template <int DIR, int SCHEME, int SPLIT, bool SEP, bool SCALAR, int G = 1>
 __global__ void __launch_bounds__(FLUX_THREADS, Tile<DIR>::MINB) k_flux(FluxArgs a) {
-  using T = FluxTile<DIR, SCALAR>;
+  using T = FluxTile<DIR, SCALAR ? G : 5>;
   constexpr int C = T::C, NL = T::NL, P = T::P, NC = T::NC, NCS = T::NCS, NI = T::NI;
   constexpr bool HYB = SCHEME == OCFD_SCHEME_HYBRID;
   constexpr int VS = DIR == 0 ? 1 : NL;  // stride of consecutive sweep points in shared memory
@@ -159,7 +163,10 @@ __global__ void __launch_bounds__(FLUX_THREADS, Tile<DIR>::MINB) k_flux(FluxArgs
   const int n = DIR == 0 ? cC.nx : (DIR == 1 ? cC.ny : cC.nz);
   const int s0 = (DIR == 0 ? blockIdx.x : blockIdx.y) * C + 1;  // first cell of the chunk
   const int l0 = DIR == 0 ? blockIdx.y * NL + 1 : blockIdx.x * NL + 1;
-  const int bz = blockIdx.z + 1;
+  const int grp = SCALAR ? (int)blockIdx.z / a.nbz : 0;
+  const int bz = (SCALAR ? (int)blockIdx.z - grp * a.nbz : (int)blockIdx.z) + 1;
+  const double* fsg = SCALAR ? a.fs + (size_t)grp * G * cC.H : nullptr;
+  double* outg = SCALAR ? a.out + (size_t)grp * G * cC.N : a.out;
   const int nl_max = DIR == 0 ? cC.ny : cC.nx;
   const int ncell = min(C, n - s0 + 1);
   const int stride = hstride(DIR);
@@ -181,18 +188,21 @@ __global__ void __launch_bounds__(FLUX_THREADS, Tile<DIR>::MINB) k_flux(FluxArgs
     else { l = idx % NL; p = idx / NL; }
     const int s = s0 - 4 + p;
     const bool line_ok = l0 + l <= nl_max;
-    double fp[5], fm[5];
+    double fp[NC], fm[NC];
     if (line_ok && p < ncell + 8) {
       int i, j, k;
       coords(s, l, i, j, k);
       const int q = hidx(i, j, k);
       double A1, A2, A3;
       metric_dir<SEP>(a.g, DIR, i, j, k, q, A1, A2, A3);
-      if (SCALAR) {
+      if constexpr (SCALAR) {
         double vs = A1 * __ldg(a.u + q) + A2 * __ldg(a.v + q) + A3 * __ldg(a.w + q);
-        double fsq = __ldg(a.fs + q);
-        fp[0] = 0.5 * (vs + fabs(vs)) * fsq;
-        fm[0] = 0.5 * (vs - fabs(vs)) * fsq;
+#pragma unroll
+        for (int c = 0; c < NC; c++) {
+          double fsq = __ldg(fsg + (size_t)c * cC.H + q);
+          fp[c] = 0.5 * (vs + fabs(vs)) * fsq;
+          fm[c] = 0.5 * (vs - fabs(vs)) * fsq;
+        }
       } else {
         double pp = __ldg(a.p + q), et = __ldg(a.Et + q), dd = __ldg(a.d + q);
         double gamma = pp / et + 1.0;
@@ -251,7 +261,7 @@ __global__ void __launch_bounds__(FLUX_THREADS, Tile<DIR>::MINB) k_flux(FluxArgs
         coords(s0 + t, l, i, j, k);
         const int nn = nidx(i, j, k);
 #pragma unroll
-        for (int c = 0; c < NC; c++) pre[r][c] = a.out[(size_t)c * N + nn];
+        for (int c = 0; c < NC; c++) pre[r][c] = outg[(size_t)c * N + nn];
       }
     }
   }
@@ -261,13 +271,13 @@ __global__ void __launch_bounds__(FLUX_THREADS, Tile<DIR>::MINB) k_flux(FluxArgs
   const int nfast = NCS * NI;
   for (int idx = threadIdx.x; idx < nfast + NCS * nq; idx += FLUX_THREADS) {
     int cs, it, scm = 0;
-    if (idx < nfast) {
+    if (!HYB || idx < nfast) {
       cs = idx / NI;
       it = idx - cs * NI;
     } else {
-      const int r = idx - nfast;
-      cs = r / nq;
-      const int e = squeue[r - cs * nq];
+      const int r = idx - nfast, nqd = HYB ? nq : 1;  // this branch runs only for HYBRID
+      cs = r / nqd;
+      const int e = squeue[r - cs * nqd];
       it = e & 0xffff;
       scm = e >> 16;
     }
@@ -311,7 +321,7 @@ __global__ void __launch_bounds__(FLUX_THREADS, Tile<DIR>::MINB) k_flux(FluxArgs
       const double* hp = sh + c * NI;
       const double* hm = sh + (NC + c) * NI;
       double val = (hp[i1] - hp[i0] + hm[i1] - hm[i0]) * h1;
-      double* o = a.out + (size_t)c * N + nn;
+      double* o = outg + (size_t)c * N + nn;
       if (DIR == 0) *o = val;
       else if (DIR == 1) *o = pre[r][c] + val;
       else *o = -(pre[r][c] + val) * ajac;
@@ -328,9 +338,9 @@ __global__ void __launch_bounds__(FLUX_THREADS, Tile<DIR>::MINB) k_flux(FluxArgs
   }
 }
 
-template <int DIR, bool SCALAR>
+template <int DIR, bool SCALAR, int G = 1>
 constexpr size_t flux_smem() {
-  return FluxTile<DIR, SCALAR>::smem;
+  return FluxTile<DIR, SCALAR ? G : 5>::smem;
 }
 
 // ---------------------------------------------------------------- CD6 / CD8 derivative
@@ -676,84 +686,199 @@ __global__ void __launch_bounds__(VE_THREADS, 2) k_visc_div(DivArgs a) {
 }
 
 // ---------------------------------------------------------------- species: viscous part
-// du_scaler_viscous (OCFD_scaler_viscous.f90:4-79). ci = fs/d over the full halo range first.
-static __global__ void k_ci(const double* fs, const double* d, double* ci, long long H) {
-  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t < H) ci[t] = fs[t] / d[t];
+// du_scaler_viscous (OCFD_scaler_viscous.f90:4-79) for every species of a stage at once. The
+// reference loops over species, each pass using du(:,:,:,1) and Ev1 as scratch; no species reads
+// another's result within a stage except the enthalpy-flux sums Qp, which are accumulated here in
+// the reference's species order, so the batched form computes the same numbers.
+// ci = fs / d over the full halo range first (blockIdx.y = species)
+static __global__ void k_ci(const double* di, const double* d, double* ci, long long H) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const size_t o = (size_t)blockIdx.y * H;
+  if (t < H) ci[o + t] = di[o + t] / d[t];
 }
-template <bool SEP>
-__global__ void __launch_bounds__(256) k_scal_ev(int ks, const double* ci, const double* d, const double* T,
-                                                 const double* amd, double* qpx, double* qpy, double* qpz, double* e1,
-                                                 double* e2, double* e3, Geo g) {
+// One thread per (cell, species): a block is 32 consecutive cells (threadIdx.x) x NS species
+// (threadIdx.y), so every species' loads are coalesced and the NS stencil evaluations of a cell
+// run in parallel. The enthalpy-flux sums Qp go through shared memory and are added by the
+// species-0 thread in species order.
+template <int NS, bool SEP>
+__global__ void __launch_bounds__(32 * NS) k_scal_ev(const double* ci, const double* d, const double* T,
+                                                     const double* amd, double* qpx, double* qpy, double* qpz,
+                                                     double* e1, double* e2, double* e3, Geo g) {
+  __shared__ double sq[3][NS][32];
+  const int ks = threadIdx.y, lane = threadIdx.x;
   int i, j, k;
-  if (!cell_of((long long)blockIdx.x * blockDim.x + threadIdx.x, i, j, k)) return;
-  const int q = hidx(i, j, k), nn = nidx(i, j, k);
-  double uk = cdiff(ci, q, 0, i, cC.nx), ui = cdiff(ci, q, 1, j, cC.ny), us = cdiff(ci, q, 2, k, cC.nz);
-  double A[9], A1[9];
-  metric_all<SEP>(g, i, j, k, q, A, A1);
-  double hi = dev_hi(ks, T[q]);
-  double cix = uk * A[0] + ui * A[3] + us * A[6];
-  double ciy = uk * A[1] + ui * A[4] + us * A[7];
-  double ciz = uk * A[2] + ui * A[5] + us * A[8];
-  double dD = d[q] * amd[(size_t)ks * cC.N + nn];
-  double E1 = dD * cix, E2 = dD * ciy, E3 = dD * ciz;
-  if (ks == 0) {
-    qpx[nn] = 0.0 + E1 * hi;
-    qpy[nn] = 0.0 + E2 * hi;
-    qpz[nn] = 0.0 + E3 * hi;
-  } else {
-    qpx[nn] = qpx[nn] + E1 * hi;
-    qpy[nn] = qpy[nn] + E2 * hi;
-    qpz[nn] = qpz[nn] + E3 * hi;
+  const bool ok = cell_of((long long)blockIdx.x * 32 + lane, i, j, k);
+  int nn = 0;
+  if (ok) {
+    const int q = hidx(i, j, k);
+    nn = nidx(i, j, k);
+    const long long H = cC.H, N = cC.N;
+    double A[9], A1[9];
+    metric_all<SEP>(g, i, j, k, q, A, A1);
+    const double* c = ci + (size_t)ks * H;
+    double uk = cdiff(c, q, 0, i, cC.nx), ui = cdiff(c, q, 1, j, cC.ny), us = cdiff(c, q, 2, k, cC.nz);
+    double hi = dev_hi(ks, T[q]);
+    double cix = uk * A[0] + ui * A[3] + us * A[6];
+    double ciy = uk * A[1] + ui * A[4] + us * A[7];
+    double ciz = uk * A[2] + ui * A[5] + us * A[8];
+    double dD = d[q] * amd[(size_t)ks * N + nn];
+    double E1 = dD * cix, E2 = dD * ciy, E3 = dD * ciz;
+    sq[0][ks][lane] = E1 * hi;
+    sq[1][ks][lane] = E2 * hi;
+    sq[2][ks][lane] = E3 * hi;
+    const size_t o = (size_t)ks * H + q;
+    e1[o] = E1 * A1[0] + E2 * A1[1] + E3 * A1[2];
+    e2[o] = E1 * A1[3] + E2 * A1[4] + E3 * A1[5];
+    e3[o] = E1 * A1[6] + E2 * A1[7] + E3 * A1[8];
   }
-  e1[q] = E1 * A1[0] + E2 * A1[1] + E3 * A1[2];
-  e2[q] = E1 * A1[3] + E2 * A1[4] + E3 * A1[5];
-  e3[q] = E1 * A1[6] + E2 * A1[7] + E3 * A1[8];
+  __syncthreads();
+  if (ok && ks == 0) {
+    // Qp = 0 before the first species, then Qp = Qp + flux * h_k
+    double qx = 0.0 + sq[0][0][lane], qy = 0.0 + sq[1][0][lane], qz = 0.0 + sq[2][0][lane];
+#pragma unroll
+    for (int m = 1; m < NS; m++) {
+      qx = qx + sq[0][m][lane];
+      qy = qy + sq[1][m][lane];
+      qz = qz + sq[2][m][lane];
+    }
+    qpx[nn] = qx;
+    qpy[nn] = qy;
+    qpz[nn] = qz;
+  }
 }
-template <bool SEP>
-__global__ void __launch_bounds__(256) k_scal_div(const double* e1, const double* e2, const double* e3, double* dus,
-                                                  Geo g) {
+template <int NS, bool SEP>
+__global__ void __launch_bounds__(32 * NS) k_scal_div(const double* e1, const double* e2, const double* e3,
+                                                      double* dus, Geo g) {
+  const int ks = threadIdx.y;
   int i, j, k;
-  if (!cell_of((long long)blockIdx.x * blockDim.x + threadIdx.x, i, j, k)) return;
+  if (!cell_of((long long)blockIdx.x * 32 + threadIdx.x, i, j, k)) return;
   const int q = hidx(i, j, k), nn = nidx(i, j, k);
-  double uk = cdiff(e1, q, 0, i, cC.nx), ui = cdiff(e2, q, 1, j, cC.ny), us = cdiff(e3, q, 2, k, cC.nz);
-  dus[nn] = dus[nn] + (uk + ui + us) * metric_jac<SEP>(g, i, j, k, q);
+  const size_t o = (size_t)ks * cC.H;
+  double uk = cdiff(e1 + o, q, 0, i, cC.nx), ui = cdiff(e2 + o, q, 1, j, cC.ny), us = cdiff(e3 + o, q, 2, k, cC.nz);
+  double* du = dus + (size_t)ks * cC.N + nn;
+  *du = *du + (uk + ui + us) * metric_jac<SEP>(g, i, j, k, q);
 }
-// Scalar_time_adv_RK3 (OCFD_Time_Adv.f90:134-166)
+// Scalar_time_adv_RK3 (OCFD_Time_Adv.f90:134-166), blockIdx.y = species
 static __global__ void k_scal_rk(int krk, double dt, const double* dus, const double* din, double* di) {
   int i, j, k;
   if (!cell_of((long long)blockIdx.x * blockDim.x + threadIdx.x, i, j, k)) return;
+  const size_t oh = (size_t)blockIdx.y * cC.H, on = (size_t)blockIdx.y * cC.N;
   const int q = hidx(i, j, k), nn = nidx(i, j, k);
   const double ra[3] = {0.0, 3.0 / 4.0, 1.0 / 3.0}, rb[3] = {1.0, 1.0 / 4.0, 2.0 / 3.0};
-  if (krk == 1) di[q] = din[nn] + dt * dus[nn];
-  else di[q] = ra[krk - 1] * din[nn] + rb[krk - 1] * (di[q] + dt * dus[nn]);
+  if (krk == 1) di[oh + q] = din[on + nn] + dt * dus[on + nn];
+  else di[oh + q] = ra[krk - 1] * din[on + nn] + rb[krk - 1] * (di[oh + q] + dt * dus[on + nn]);
 }
 
-// comput_Amu_Amk_AMD for NS > 1 (Comput_flow_variables.f90:69-98)
+// comput_Amu_Amk_AMD for NS > 1 (Comput_flow_variables.f90:69-98; comput_vis_coeff,
+// comput_thermal_conductivity, comput_diffusion_coeff of TRANSPORT_modules.f90:259-426).
+// One thread per (cell, species): a block is 32 consecutive cells (threadIdx.x) x NS species
+// (threadIdx.y). The per-species exponentials, the Wilke rows and the NS (NS-1) / 2 distinct
+// binary-diffusion pairs are spread over a cell's NS threads; every sum is taken from shared
+// memory in the reference's order, so the results equal the one-thread-per-cell evaluation.
 template <int NS>
-__global__ void __launch_bounds__(128) k_transport(const double* d, const double* T, const double* p,
-                                                   const double* di, double* amu, double* amk, double* amd) {
+__global__ void __launch_bounds__(32 * NS) k_transport(const double* d, const double* T, const double* p,
+                                                       const double* di, double* amu, double* amk, double* amd) {
+  constexpr int NP = NS * (NS - 1) / 2;
+  __shared__ double sX[NS][32], sD0[NS][32], sMu[NS][32], sK[NS][32], sW[NS][32], sD2[NP > 0 ? NP : 1][32];
+  const int ks = threadIdx.y, lane = threadIdx.x;
   int i, j, k;
-  if (!cell_of((long long)blockIdx.x * blockDim.x + threadIdx.x, i, j, k)) return;
-  const int q = hidx(i, j, k), nn = nidx(i, j, k);
-  double d0[NS], Xi[NS], X0 = 0.0;
-#pragma unroll
-  for (int m = 0; m < NS; m++) {
-    d0[m] = di[(size_t)m * cC.H + q];
-    Xi[m] = d0[m] / cC.Mi[m];
-    X0 = X0 + Xi[m];
+  const bool ok = cell_of((long long)blockIdx.x * 32 + lane, i, j, k);
+  const int q = ok ? hidx(i, j, k) : 0, nn = ok ? nidx(i, j, k) : 0;
+  const double Tq = ok ? T[q] : 300.0;
+  if (ok) {
+    const double d0 = di[(size_t)ks * cC.H + q];
+    sD0[ks][lane] = d0;
+    sX[ks][lane] = d0 / cC.Mi[ks];
   }
+  __syncthreads();
+  {
+    double X0 = 0.0;
 #pragma unroll
-  for (int m = 0; m < NS; m++) Xi[m] = Xi[m] / X0;
-  double Tq = T[q];
-  double mu = dev_viscosity<NS>(Tq, Xi);
-  double cp = dev_Cp<NS>(d[q], d0, Tq);
-  amu[nn] = mu;
-  amk[nn] = dev_conductivity<NS>(mu, cp, Tq, Xi);
-  double ad[NS];
-  dev_diffusion<NS>(ad, mu, Tq, d[q], p[q], Xi);
+    for (int m = 0; m < NS; m++) X0 = X0 + sX[m][lane];
+    sW[ks][lane] = sX[ks][lane] / X0;  // mole fraction of species ks
+  }
+  __syncthreads();
+  double Xi[NS];
 #pragma unroll
-  for (int m = 0; m < NS; m++) amd[(size_t)m * cC.N + nn] = ad[m];
+  for (int m = 0; m < NS; m++) Xi[m] = sW[m][lane];
+  const double L = log(Tq);
+  if (cC.flag_vis != 0)
+    sMu[ks][lane] = exp(cC.mu_an[ks][0] + cC.mu_an[ks][1] * L + cC.mu_an[ks][2] * q2(L) + cC.mu_an[ks][3] * q3(L)) * 0.1;
+  if (cC.flag_cond != 0)
+    sK[ks][lane] = exp(cC.k_an[ks][0] + cC.k_an[ks][1] * L + cC.k_an[ks][2] * q2(L) + cC.k_an[ks][3] * q3(L)) * 1.0e-5;
+  if (cC.flag_diff != 0) {
+    for (int pi = ks; pi < NP; pi += NS) {  // pair pi = (a, b), a < b, enumerated a-major
+      int a = 0, r = pi;
+      while (r >= NS - 1 - a) { r -= NS - 1 - a; a++; }
+      const int b = a + 1 + r;
+      sD2[pi][lane] =
+          exp(cC.d_an[a][b][0] + cC.d_an[a][b][1] * L + cC.d_an[a][b][2] * q2(L) + cC.d_an[a][b][3] * q3(L)) * 1.0e-4;
+    }
+  }
+  __syncthreads();
+  // viscosity: Wilke row ks (or Sutherland)
+  double mu;
+  if (cC.flag_vis == 0) {
+    const double TA = 288.15, TC = 110.4;
+    mu = cC.amu0 * sqrt(q3(Tq / TA)) * (TA + TC) / (TC + Tq);
+  } else {
+    const double muk = sMu[ks][lane];
+    double pk0 = 0.0;
+#pragma unroll
+    for (int jj = 0; jj < NS; jj++) {
+      double s1 = 1.0 + sqrt(muk / sMu[jj][lane] * cC.wk_a[ks][jj]);
+      double pkj = q2(s1) / cC.wk_b[ks][jj];
+      pk0 = pk0 + Xi[jj] * pkj;
+    }
+    sW[ks][lane] = Xi[ks] * muk / pk0;
+    __syncthreads();
+    mu = 0.0;
+#pragma unroll
+    for (int m = 0; m < NS; m++) mu = mu + sW[m][lane];
+  }
+  if (!ok) return;
+  if (ks == 0) {
+    double cp;
+    {
+      double dd[NS];
+#pragma unroll
+      for (int m = 0; m < NS; m++) dd[m] = sD0[m][lane];
+      cp = dev_Cp<NS>(d[q], dd, Tq);
+    }
+    double kk;
+    if (cC.flag_cond == 0) {
+      kk = mu * cp / cC.pr;
+    } else {
+      double a1 = 0.0, a2 = 0.0;
+#pragma unroll
+      for (int m = 0; m < NS; m++) {
+        const double ki = sK[m][lane];
+        a1 = a1 + Xi[m] * ki;
+        a2 = a2 + Xi[m] / ki;
+      }
+      kk = 0.5 * (a1 + 1.0 / a2);
+    }
+    amu[nn] = mu;
+    amk[nn] = kk;
+  }
+  double ad;
+  if (cC.flag_diff == 0) {
+    double d0 = 0.0;
+#pragma unroll
+    for (int m = 0; m < NS; m++) d0 = d0 + Xi[m] * cC.Mi[m];
+    ad = mu * (1.0 - Xi[ks] * cC.Mi[ks] / d0) / ((1.0 - Xi[ks]) * cC.sc * d[q] + 1.0e-20);
+  } else {
+    double ds = 0.0;
+#pragma unroll
+    for (int jj = 0; jj < NS; jj++) {
+      if (jj == ks) continue;
+      const int a = ks < jj ? ks : jj, b = ks < jj ? jj : ks;
+      const int pi = a * NS - a * (a + 1) / 2 + (b - a - 1);
+      ds = ds + Xi[jj] / sD2[pi][lane];
+    }
+    ad = (1.0 - Xi[ks]) / (ds + 1.0e-20) * 1.013e5 / p[q];
+  }
+  amd[(size_t)ks * cC.N + nn] = ad;
 }
 
 // ---------------------------------------------------------------- halo exchange (single rank)

@@ -53,6 +53,7 @@ struct Lib {
   double *f = nullptr, *fn = nullptr, *du = nullptr, *d = nullptr, *u = nullptr, *v = nullptr, *w = nullptr,
          *T = nullptr, *p = nullptr, *Et[2] = {nullptr, nullptr}, *di = nullptr, *din = nullptr, *Rh = nullptr;
   double *ev[12] = {}, *amu = nullptr, *amk = nullptr, *amd = nullptr, *qp[3] = {}, *ci = nullptr, *se[3] = {};
+  double* dus = nullptr;  // Dus of every species (Ns x N)
   double *X = nullptr, *Y = nullptr, *Z = nullptr, *met[19] = {}, *d1[3] = {}, *edge[6] = {}, *partial = nullptr;
   double *inlet = nullptr, *upper = nullptr, *wall = nullptr, *ht_dev = nullptr;
   int *nonref = nullptr, *patches = nullptr;
@@ -162,12 +163,14 @@ void exchange_v(const std::vector<double*>& fields, int dirmask) {
 }
 
 // ---- flux dispatch (kernels compiled in ocfd_flux_{x,y,z}.cu) ----
-void launch_flux(int dir, const FluxArgs& a, bool scalar) {
-  KTimer t(scalar ? KC_SPECIES : KC_FLUX_X + dir);
+// group = 0: the flow fluxes; else a scalar sweep of every species, group species per block
+void launch_flux(int dir, const FluxArgs& a, int group = 0, int ngroups = 1) {
+  KTimer t(group ? KC_SPECIES : KC_FLUX_X + dir);
   const ocfd_params& P = L->P;
-  if (dir == 0) launch_flux_x(P.scheme_invis, P.flux_splitting, L->sep, scalar, a, P.nx, P.ny, P.nz, L->st);
-  else if (dir == 1) launch_flux_y(P.scheme_invis, P.flux_splitting, L->sep, scalar, a, P.nx, P.ny, P.nz, L->st);
-  else launch_flux_z(P.scheme_invis, P.flux_splitting, L->sep, scalar, a, P.nx, P.ny, P.nz, L->st);
+  const bool ch = P.if_scheme_character == 1;
+  if (dir == 0) launch_flux_x(P.scheme_invis, P.flux_splitting, L->sep, group, ngroups, ch, a, P.nx, P.ny, P.nz, L->st);
+  else if (dir == 1) launch_flux_y(P.scheme_invis, P.flux_splitting, L->sep, group, ngroups, ch, a, P.nx, P.ny, P.nz, L->st);
+  else launch_flux_z(P.scheme_invis, P.flux_splitting, L->sep, group, ngroups, ch, a, P.nx, P.ny, P.nz, L->st);
   LAUNCH_CHECK();
 }
 
@@ -333,7 +336,7 @@ void stage_t(int krk, double dt1) {
   double* Etc = L->Et[L->cur];
   if (NS > 1) {
     KTimer t(KC_SPECIES);
-    k_transport<NS><<<nblk(N, 128), 128, 0, L->st>>>(L->d, L->T, L->p, L->di, L->amu, L->amk, L->amd);
+    k_transport<NS><<<nblk(N, 32), dim3(32, NS), 0, L->st>>>(L->d, L->T, L->p, L->di, L->amu, L->amk, L->amd);
     LAUNCH_CHECK();
   }
   {
@@ -350,38 +353,40 @@ void stage_t(int krk, double dt1) {
   fa.d = L->d; fa.u = L->u; fa.v = L->v; fa.w = L->w; fa.p = L->p; fa.Et = Etc; fa.Rh = L->Rh;
   fa.g = L->geo;
   if (NS > 1) {
-    for (int m = 0; m < NS; m++) {
-      double* fs = L->di + (size_t)m * H;
-      fa.fs = fs;
-      fa.out = L->du;
-      for (int dd = 0; dd < 3; dd++) launch_flux(dd, fa, true);
-      if (L->P.if_viscous == 1) {
-        KTimer t(KC_SPECIES);
-        k_ci<<<nblk(H, 256), 256, 0, L->st>>>(fs, L->d, L->ci, H);
-        LAUNCH_CHECK();
-        if (L->sep) k_scal_ev<true><<<nblk(N, 256), 256, 0, L->st>>>(m, L->ci, L->d, L->T, L->amd, L->qp[0], L->qp[1], L->qp[2], L->se[0], L->se[1], L->se[2], L->geo);
-        else k_scal_ev<false><<<nblk(N, 256), 256, 0, L->st>>>(m, L->ci, L->d, L->T, L->amd, L->qp[0], L->qp[1], L->qp[2], L->se[0], L->se[1], L->se[2], L->geo);
-        LAUNCH_CHECK();
-      }
-      if (L->P.if_viscous == 1) {
-        exchange({L->se[0]}, 1);
-        exchange({L->se[1]}, 2);
-        exchange({L->se[2]}, 4);
-        KTimer t(KC_SPECIES);
-        if (L->sep) k_scal_div<true><<<nblk(N, 256), 256, 0, L->st>>>(L->se[0], L->se[1], L->se[2], L->du, L->geo);
-        else k_scal_div<false><<<nblk(N, 256), 256, 0, L->st>>>(L->se[0], L->se[1], L->se[2], L->du, L->geo);
-        LAUNCH_CHECK();
-      }
+    // every species at once (du_scaler_invis / du_scaler_viscous / Scalar_time_adv_RK3 of the
+    // reference's species loop): Dus of species m is dus + m N
+    const int grp = NS % 3 == 0 ? 3 : 1;
+    fa.fs = L->di;
+    fa.out = L->dus;
+    for (int dd = 0; dd < 3; dd++) launch_flux(dd, fa, grp, NS / grp);
+    if (L->P.if_viscous == 1) {
       {
         KTimer t(KC_SPECIES);
-        k_scal_rk<<<nblk(N, 256), 256, 0, L->st>>>(krk, dt1, L->du, L->din + (size_t)m * N, fs);
+        k_ci<<<dim3(nblk(H, 256), NS), 256, 0, L->st>>>(L->di, L->d, L->ci, H);
+        LAUNCH_CHECK();
+        if (L->sep) k_scal_ev<NS, true><<<nblk(N, 32), dim3(32, NS), 0, L->st>>>(L->ci, L->d, L->T, L->amd, L->qp[0], L->qp[1], L->qp[2], L->se[0], L->se[1], L->se[2], L->geo);
+        else k_scal_ev<NS, false><<<nblk(N, 32), dim3(32, NS), 0, L->st>>>(L->ci, L->d, L->T, L->amd, L->qp[0], L->qp[1], L->qp[2], L->se[0], L->se[1], L->se[2], L->geo);
         LAUNCH_CHECK();
       }
+      for (int dd = 0; dd < 3; dd++) {
+        std::vector<double*> fl;
+        for (int m = 0; m < NS; m++) fl.push_back(L->se[dd] + (size_t)m * H);
+        exchange_v(fl, 1 << dd);
+      }
+      KTimer t(KC_SPECIES);
+      if (L->sep) k_scal_div<NS, true><<<nblk(N, 32), dim3(32, NS), 0, L->st>>>(L->se[0], L->se[1], L->se[2], L->dus, L->geo);
+      else k_scal_div<NS, false><<<nblk(N, 32), dim3(32, NS), 0, L->st>>>(L->se[0], L->se[1], L->se[2], L->dus, L->geo);
+      LAUNCH_CHECK();
+    }
+    {
+      KTimer t(KC_SPECIES);
+      k_scal_rk<<<dim3(nblk(N, 256), NS), 256, 0, L->st>>>(krk, dt1, L->dus, L->din, L->di);
+      LAUNCH_CHECK();
     }
   }
   fa.fs = nullptr;
   fa.out = L->du;
-  for (int dd = 0; dd < 3; dd++) launch_flux(dd, fa, false);
+  for (int dd = 0; dd < 3; dd++) launch_flux(dd, fa);
   if (L->P.if_viscous == 1) {
     ViscArgs va{};
     va.d = L->d; va.u = L->u; va.v = L->v; va.w = L->w; va.T = L->T; va.di = L->di;
@@ -553,6 +558,12 @@ void fill_trans(DevConst& c, const ocfd_transport* tr, int ns) {
       c.mu_an[k][m] = tr->mu_an[k][m];
       c.k_an[k][m] = tr->k_an[k][m];
       for (int j = 0; j < ns; j++) c.d_an[k][j][m] = tr->d_an[k][j][m];
+    }
+  // Wilke pair constants (needs Mi: fill_thermo runs first)
+  for (int k = 0; k < ns; k++)
+    for (int j = 0; j < ns; j++) {
+      c.wk_a[k][j] = std::sqrt(c.Mi[j] / c.Mi[k]);
+      c.wk_b[k][j] = std::sqrt(8.0 * (1.0 + c.Mi[k] / c.Mi[j]));
     }
 }
 
@@ -737,7 +748,7 @@ int validate(const ocfd_params* p) {
       return OCFD_ERR_UNSUPPORTED;
     }
   }
-  if (p->if_scheme_character != 0) { g_err = "IF_Scheme_Character=1 (characteristic flux) is not built"; return OCFD_ERR_UNSUPPORTED; }
+  if (p->if_scheme_character != 0 && p->if_scheme_character != 1) { g_err = "IF_Scheme_Character must be 0 or 1"; return OCFD_ERR_PARAM; }
   if (!(p->ibc == OCFD_BC_NONE || p->ibc == OCFD_BC_BOUNDARYLAYER || p->ibc == OCFD_BC_JET)) { g_err = "boundary condition not built (BC_NONE, BC_BOUNDARYLAYER, BC_JET)"; return OCFD_ERR_UNSUPPORTED; }
   if (p->wall_catalysis != 0) return bad("only non-catalytic walls");
   if (!(p->chem_timeadv == 1 || p->chem_timeadv == 2 || p->chem_timeadv == 3 || p->chem_timeadv == -1)) return bad("CHEM_TimeAdv must be 1, 2, 3 or -1");
@@ -847,7 +858,12 @@ int ocfd_gpu_init(const ocfd_params* p, const ocfd_thermo* th, const ocfd_kineti
     for (int m = 0; m < 8; m++) add(H, 8);
     add(NS * H, 8); add(NS * N, 8); add(H, 8);
     for (int m = 0; m < 12; m++) add(H, 8);
-    if (NS > 1) { add(N, 8); add(N, 8); add(NS * N, 8); for (int m = 0; m < 3; m++) add(N, 8); add(H, 8); for (int m = 0; m < 3; m++) add(H, 8); }
+    if (NS > 1) {
+      add(N, 8); add(N, 8); add(NS * N, 8);                              // amu, amk, amd
+      for (int m = 0; m < 3; m++) add(N, 8);                             // qp
+      add(NS * H, 8); for (int m = 0; m < 3; m++) add(NS * H, 8);        // ci, se
+      add(NS * N, 8);                                                    // dus
+    }
     for (int m = 0; m < 3; m++) add(H, 8);
     if (!L->sep) for (int m = 0; m < 19; m++) add(H, 8);
     for (int m = 0; m < 3; m++) add(nn[m] + 2 * OCFD_L, 8);
@@ -872,8 +888,9 @@ int ocfd_gpu_init(const ocfd_params* p, const ocfd_thermo* th, const ocfd_kineti
     if (NS > 1) {
       L->amu = alloc<double>(N); L->amk = alloc<double>(N); L->amd = alloc<double>(NS * N);
       for (int m = 0; m < 3; m++) L->qp[m] = alloc<double>(N);
-      L->ci = alloc<double>(H);
-      for (int m = 0; m < 3; m++) L->se[m] = alloc<double>(H);
+      L->ci = alloc<double>((size_t)NS * H);
+      for (int m = 0; m < 3; m++) L->se[m] = alloc<double>((size_t)NS * H);
+      L->dus = alloc<double>((size_t)NS * N);
     }
     L->X = alloc<double>(H); L->Y = alloc<double>(H); L->Z = alloc<double>(H);
     if (!L->sep) for (int m = 0; m < 19; m++) L->met[m] = alloc<double>(H);
@@ -907,8 +924,9 @@ int ocfd_gpu_init(const ocfd_params* p, const ocfd_thermo* th, const ocfd_kineti
     if (NS > 1) {
       fill(L->amu, N, 0.0); fill(L->amk, N, 0.0); fill(L->amd, NS * N, 0.0);
       for (int m = 0; m < 3; m++) fill(L->qp[m], N, 0.0);
-      fill(L->ci, H, 0.0);
-      for (int m = 0; m < 3; m++) fill(L->se[m], H, 0.0);
+      fill(L->ci, (size_t)NS * H, 0.0);
+      for (int m = 0; m < 3; m++) fill(L->se[m], (size_t)NS * H, 0.0);
+      fill(L->dus, (size_t)NS * N, 0.0);
     }
     // init_mesh
     CK(cudaMemcpyAsync(L->X, coords, sizeof(double) * H, cudaMemcpyHostToDevice, L->st));

@@ -5,13 +5,15 @@
 #include "ocfd_flow.cuh"
 
 namespace ocfd {
-// one sweep direction; throws std::runtime_error on a bad scheme id
-void launch_flux_x(int scheme, int split, bool sep, bool scalar, const FluxArgs& a, int nx, int ny, int nz,
-                   cudaStream_t st);
-void launch_flux_y(int scheme, int split, bool sep, bool scalar, const FluxArgs& a, int nx, int ny, int nz,
-                   cudaStream_t st);
-void launch_flux_z(int scheme, int split, bool sep, bool scalar, const FluxArgs& a, int nx, int ny, int nz,
-                   cudaStream_t st);
+// one sweep direction; group = 0 for the flow fluxes, else the species per block of a scalar
+// sweep over ngroups x group species (1 or 3); character selects the characteristic-space flow
+// flux (IF_Scheme_Character = 1); throws std::runtime_error on a bad scheme id
+void launch_flux_x(int scheme, int split, bool sep, int group, int ngroups, bool character, const FluxArgs& a,
+                   int nx, int ny, int nz, cudaStream_t st);
+void launch_flux_y(int scheme, int split, bool sep, int group, int ngroups, bool character, const FluxArgs& a,
+                   int nx, int ny, int nz, cudaStream_t st);
+void launch_flux_z(int scheme, int split, bool sep, int group, int ngroups, bool character, const FluxArgs& a,
+                   int nx, int ny, int nz, cudaStream_t st);
 void launch_chem_cells(int ns, long long ncell, double* f, double* Et, double* T, double* p, double* di, double dt2,
                        int nsub, int* nfail, cudaStream_t st);
 void launch_chem_batch(int ns, int sms, int n, double* di, double* e, const double* dt, const int* nsub,

@@ -480,6 +480,141 @@ struct Oracle {
     }
   }
 
+  /* One direction of du_inviscous_Character (OCFD_inviscous_character.f90:3-160) with
+   * flux_charteric (:162-319): at every interface the split fluxes of the stencil are projected
+   * on the left eigenvectors of the interface-averaged state, reconstructed component by
+   * component, summed (h0 = h+ + h-) and projected back with the right eigenvectors; HYBRID
+   * interfaces that take the linear scheme skip the projection. A closed face with the default
+   * closure takes the non-reflecting physical-space flux at interfaces 0 and n. */
+  void inviscid_dir_char(int dir, double* out) {
+    int n = dir == 0 ? nx : (dir == 1 ? ny : nz);
+    long s = dir == 0 ? 1 : (dir == 1 ? HX : HX * HY);
+    double h1 = 1.0 / (dir == 0 ? hx : (dir == 1 ? hy : hz));
+    const double* A1a = M[M_AKX1 + 3 * dir].data();
+    const double* A2a = M[M_AKX1 + 3 * dir + 1].data();
+    const double* A3a = M[M_AKX1 + 3 * dir + 2].data();
+    int sb[2] = {P.scheme_boundary[2 * dir], P.scheme_boundary[2 * dir + 1]};
+    const int* bnd = bound[dir];
+    int n1 = dir == 0 ? ny : nx, n2 = dir == 2 ? ny : nz;
+    const int ia = (bnd[0] == 0 || sb[0] != 0) ? 0 : 1;
+    const int ib = (bnd[1] == 0 || sb[1] != 0) ? n : n - 1;
+    const int W = n + 2 * L;
+#pragma omp parallel
+    {
+      std::vector<double> fpb(5 * W), fmb(5 * W), hh(5 * (n + 1));
+      std::vector<int> scm(n + 1, 0);
+#pragma omp for collapse(2)
+      for (int b = 1; b <= n2; b++)
+        for (int a = 1; a <= n1; a++) {
+          int i0 = a, j0 = a, k0 = b;
+          if (dir == 0) { j0 = a; k0 = b; }
+          if (dir == 1) { i0 = a; k0 = b; }
+          if (dir == 2) { i0 = a; j0 = b; }
+          long base = ih(dir == 0 ? 0 : i0, dir == 1 ? 0 : j0, dir == 2 ? 0 : k0); /* point index 0 */
+          if (S.scheme == OCFD_SCHEME_HYBRID)
+            for (int i = 0; i <= n; i++) scm[i] = set_hybrid(std::max(Rh[base + i * s], Rh[base + (i + 1) * s]));
+          for (int i = 1 - L; i <= n + L; i++) {
+            long q = base + i * s;
+            double fp[5], fm[5];
+            split(Et[q], p[q], cc[q], d[q], u[q], v[q], w[q], A1a[q], A2a[q], A3a[q], fp, fm);
+            for (int m = 0; m < 5; m++) {
+              fpb[m * W + (i + L - 1)] = fp[m];
+              fmb[m * W + (i + L - 1)] = fm[m];
+            }
+          }
+          auto FP = [&](int i, int m) { return fpb[m * W + (i + L - 1)]; };
+          auto FM = [&](int i, int m) { return fmb[m * W + (i + L - 1)]; };
+          for (int i = ia; i <= ib; i++) {
+            double fpc[8][5], fmc[8][5]; /* stencil offsets -3..4 at [mm + 3] */
+            double S1[5][5];
+            const bool lin = scm[i] == 1;
+            if (lin) {
+              for (int mm = -3; mm <= 4; mm++)
+                for (int m = 0; m < 5; m++) { fpc[mm + 3][m] = FP(i + mm, m); fmc[mm + 3][m] = FM(i + mm, m); }
+            } else {
+              long q0 = base + i * s, q1 = base + (i + 1) * s;
+              double u1 = (u[q0] + u[q1]) * 0.5, v1 = (v[q0] + v[q1]) * 0.5, w1 = (w[q0] + w[q1]) * 0.5;
+              double c1 = (cc[q0] + cc[q1]) * 0.5, p1 = (p[q0] + p[q1]) * 0.5, Et1 = (Et[q0] + Et[q1]) * 0.5;
+              double a1 = (A1a[q0] + A1a[q1]) * 0.5, a2 = (A2a[q0] + A2a[q1]) * 0.5, a3 = (A3a[q0] + A3a[q1]) * 0.5;
+              double Sm[5][5];
+              char_matrices(u1, v1, w1, c1, p1, Et1, a1, a2, a3, Sm, S1);
+              for (int mm = -3; mm <= 4; mm++) {
+                double xp[5], xm[5];
+                for (int m = 0; m < 5; m++) { xp[m] = FP(i + mm, m); xm[m] = FM(i + mm, m); }
+                for (int r = 0; r < 5; r++) {
+                  fpc[mm + 3][r] = Sm[r][0] * xp[0] + Sm[r][1] * xp[1] + Sm[r][2] * xp[2] + Sm[r][3] * xp[3] + Sm[r][4] * xp[4];
+                  fmc[mm + 3][r] = Sm[r][0] * xm[0] + Sm[r][1] * xm[1] + Sm[r][2] * xm[2] + Sm[r][3] * xm[3] + Sm[r][4] * xm[4];
+                }
+              }
+            }
+            double h0[5];
+            for (int m = 0; m < 5; m++) {
+              double gp[8], gm[8];
+              for (int mm = 0; mm < 8; mm++) { gp[mm] = fpc[mm][m]; gm[mm] = fmc[mm][m]; }
+              double ha = iface_flux(true, S, gp + 3, i, n, bnd, sb, scm[i]);
+              double hb = iface_flux(false, S, gm + 3, i, n, bnd, sb, scm[i]);
+              h0[m] = ha + hb;
+            }
+            for (int m = 0; m < 5; m++)
+              hh[m * (n + 1) + i] = lin ? h0[m]
+                                        : S1[m][0] * h0[0] + S1[m][1] * h0[1] + S1[m][2] * h0[2] + S1[m][3] * h0[3] +
+                                              S1[m][4] * h0[4];
+          }
+          if (bnd[0] == 1 && sb[0] == 0)
+            for (int m = 0; m < 5; m++)
+              hh[m * (n + 1)] = (2.0 * FP(1, m) + 5.0 * FP(2, m) - FP(3, m) + 2.0 * FM(3, m) - 7.0 * FM(2, m) +
+                                 11.0 * FM(1, m)) / 6.0;
+          if (bnd[1] == 1 && sb[1] == 0)
+            for (int m = 0; m < 5; m++)
+              hh[m * (n + 1) + n] = (2.0 * FP(n - 2, m) - 7.0 * FP(n - 1, m) + 11.0 * FP(n, m) + 2.0 * FM(n, m) +
+                                     5.0 * FM(n - 1, m) - FM(n - 2, m)) / 6.0;
+          for (int m = 0; m < 5; m++)
+            for (int i = 1; i <= n; i++) {
+              int ii = dir == 0 ? i : i0, jj = dir == 1 ? i : j0, kk = dir == 2 ? i : k0;
+              long a2 = in(ii, jj, kk) + (long)m * N;
+              double val = (hh[m * (n + 1) + i] - hh[m * (n + 1) + i - 1]) * h1;
+              if (dir == 0) out[a2] = val;
+              else if (dir == 1) out[a2] = out[a2] + val;
+              else out[a2] = -(out[a2] + val) * M[M_AJAC][ih(ii, jj, kk)];
+            }
+        }
+    }
+  }
+
+  /* left (S) and right (S1) eigenvector matrices of the flux Jacobian along the metric vector
+   * a at the interface-averaged state (OCFD_inviscous_character.f90:213-270) */
+  static void char_matrices(double u1, double v1, double w1, double c1, double p1, double Et1, double a1, double a2,
+                            double a3, double Sm[5][5], double S1[5][5]) {
+    double ss = std::sqrt(a1 * a1 + a2 * a2 + a3 * a3);
+    double n1 = a1 / ss, n2 = a2 / ss, n3 = a3 / ss;
+    double l1, l2, l3;
+    if (std::fabs(n3) <= std::fabs(n2)) {
+      ss = std::sqrt(n1 * n1 + n2 * n2);
+      l1 = -n2 / ss; l2 = n1 / ss; l3 = 0.0;
+    } else {
+      ss = std::sqrt(n1 * n1 + n3 * n3);
+      l1 = -n3 / ss; l2 = 0.0; l3 = n1 / ss;
+    }
+    double m1 = n2 * l3 - n3 * l2, m2 = n3 * l1 - n1 * l3, m3 = n1 * l2 - n2 * l1;
+    double un = u1 * n1 + v1 * n2 + w1 * n3, ul = u1 * l1 + v1 * l2 + w1 * l3, um = u1 * m1 + v1 * m2 + w1 * m3;
+    double V2 = (u1 * u1 + v1 * v1 + w1 * w1) * 0.5;
+    double gamma = p1 / Et1 + 1.0;
+    double KK = (gamma - 1.0) / (c1 * c1);
+    double KK1 = KK * 0.5, X1 = 1.0 / (2.0 * c1), Hh = V2 + 1.0 / KK;
+    double A[5][5] = {{1.0 - KK * V2, KK * u1, KK * v1, KK * w1, -KK},
+                      {-ul, l1, l2, l3, 0.0},
+                      {-um, m1, m2, m3, 0.0},
+                      {KK1 * V2 + X1 * un, -X1 * n1 - KK1 * u1, -X1 * n2 - KK1 * v1, -X1 * n3 - KK1 * w1, KK1},
+                      {KK1 * V2 - X1 * un, X1 * n1 - KK1 * u1, X1 * n2 - KK1 * v1, X1 * n3 - KK1 * w1, KK1}};
+    double B[5][5] = {{1.0, 0.0, 0.0, 1.0, 1.0},
+                      {u1, l1, m1, u1 - c1 * n1, u1 + c1 * n1},
+                      {v1, l2, m2, v1 - c1 * n2, v1 + c1 * n2},
+                      {w1, l3, m3, w1 - c1 * n3, w1 + c1 * n3},
+                      {V2, ul, um, Hh - c1 * un, Hh + c1 * un}};
+    for (int r = 0; r < 5; r++)
+      for (int c = 0; c < 5; c++) { Sm[r][c] = A[r][c]; S1[r][c] = B[r][c]; }
+  }
+
   /* comput_cc (Comput_flow_variables.f90:50-63) over the full halo range */
   void comput_cc() {
 #pragma omp parallel for
@@ -491,9 +626,15 @@ struct Oracle {
 
   void du_inviscous() {
     comput_cc();
-    inviscid_dir(0, nullptr, du.data(), 5);
-    inviscid_dir(1, nullptr, du.data(), 5);
-    inviscid_dir(2, nullptr, du.data(), 5);
+    if (P.if_scheme_character == 1) { /* OCFD_Time_Adv.f90:76-80 */
+      inviscid_dir_char(0, du.data());
+      inviscid_dir_char(1, du.data());
+      inviscid_dir_char(2, du.data());
+    } else {
+      inviscid_dir(0, nullptr, du.data(), 5);
+      inviscid_dir(1, nullptr, du.data(), 5);
+      inviscid_dir(2, nullptr, du.data(), 5);
+    }
     if (P.if_mass_force == 1) {
       for (int k = 1; k <= nz; k++)
         for (int j = 1; j <= ny; j++)

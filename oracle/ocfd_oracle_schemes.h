@@ -337,4 +337,48 @@ inline void flux_pencil(bool plus, const SchemeSet& S, const double* v, double* 
   }
 }
 
+/* One interface i of a pencil of n cells for the characteristic-space flux, following flux_x1
+ * (sign +) and flux_x2 (sign -) of OCFD_inviscous_character.f90:321-425: f points at the
+ * stencil value of interface i (f[mm] = value at i + mm). Interior points take the scheme (HYBRID
+ * by its per-interface index), points near a closed face the WENO5-type boundary schemes. */
+inline double iface_flux(bool plus, const SchemeSet& S, const double* f, int i, int n, const int bnd[2],
+                         const int sb[2], int scm) {
+  static const OMP omp;
+  const int Ka = plus ? S.Ka1 : S.Ka2, Kb = plus ? S.Kb1 : S.Kb2;
+  const bool inner = (bnd[0] == 0 || i > -Ka || sb[0] == -1) && (bnd[1] == 0 || i <= n - Kb || sb[1] == -1);
+  if (inner) {
+    int sc = S.scheme;
+    if (sc == OCFD_SCHEME_HYBRID) sc = scm == 1 ? 4 : (scm == 2 ? 2 : 1);
+    switch (sc) {
+      case 3: return plus ? omp6P(omp, f) : omp6M(omp, f);
+      case 2: return plus ? hh_weno7P(f) : hh_weno7M(f);
+      case 4: return plus ? ud7lP(S.UD7L, f) : ud7lM(S.UD7L, f);
+      default: return plus ? hh_weno5P(f) : hh_weno5M(f);
+    }
+  }
+  if (i <= -Ka && bnd[0] == 1 && sb[0] != -1) { /* left face */
+    if (sb[0] == 0) {
+      if (plus) {
+        if (i == 1) return (2.0 * f[0] + 5.0 * f[1] - f[2]) / 6.0;
+        if (i == 2) return hh_weno5P_bnd(f, 1);
+        return hh_weno5P(f);
+      }
+      if (i == 1) return hh_weno5M_bnd(f, 1);
+      return hh_weno5M(f);
+    }
+    return plus ? hh_weno5P(f) : hh_weno5M(f); /* Scheme_boundary = 1 */
+  }
+  /* right face (i > n - Kb, bnd[1] == 1, sb[1] != -1) */
+  if (sb[1] == 0) {
+    if (plus) {
+      if (i == n - 1) return hh_weno5P_bnd(f, 2);
+      return hh_weno5P(f);
+    }
+    if (i == n - 1) return (2.0 * f[1] + 5.0 * f[0] - f[-1]) / 6.0;
+    if (i == n - 2) return hh_weno5M_bnd(f, 2);
+    return hh_weno5M(f);
+  }
+  return plus ? hh_weno5P(f) : hh_weno5M(f);
+}
+
 }  // namespace ocfd_oracle

@@ -242,7 +242,38 @@ def test_bad_parameters_rejected(gpu):
         gpu.Solver(c)
     assert ei.value.code == abi.ERR_PARAM
     c = cases.isotropic(n=12)
-    c.params.if_scheme_character = 1
+    c.params.ibc = 108  # a boundary-condition family the library does not carry
     with pytest.raises(gpu.OcfdError) as ei:
         gpu.Solver(c)
     assert ei.value.code == abi.ERR_UNSUPPORTED
+
+
+# ---------------------------------------------------------------- characteristic-space flux
+@pytest.mark.parametrize("scheme", ["WENO5", "WENO7", "OMP6"])
+def test_characteristic_isotropic_bitwise(oracle, gpu, scheme):
+    """IF_Scheme_Character = 1 on a periodic box: projections on the eigenvectors of the
+    interface-averaged state, component-wise reconstruction, back projection."""
+    c = cases.isotropic(n=16, scheme=scheme)
+    c.params.if_scheme_character = 1
+    so, sg, *_ = run_pair(oracle, gpu, c, 2)
+    assert_bitwise(so, sg)
+
+
+@pytest.mark.parametrize("variant", ["default", "all"])
+def test_characteristic_flatplate_bitwise(oracle, gpu, variant):
+    """HYBRID with the characteristic flux: linear interfaces skip the projection, closed faces
+    take the boundary closures and the non-reflecting physical flux at interfaces 0 and n."""
+    c = cases.flatplate(nx=40, ny=24, nz=12, scheme="HYBRID", lx=0.01, ly=0.004, y1=2e-5)
+    c.params.if_scheme_character = 1
+    if variant == "all":
+        _variant(c.params, "all")
+    so, sg, *_ = run_pair(oracle, gpu, c, 2)
+    assert_bitwise(so, sg)
+
+
+def test_characteristic_llf_weno5_flatplate_bitwise(oracle, gpu):
+    c = cases.flatplate(nx=40, ny=24, nz=12, scheme="WENO5", lx=0.01, ly=0.004, y1=2e-5)
+    c.params.if_scheme_character = 1
+    c.params.flux_splitting = abi.SPLIT_LLF
+    so, sg, *_ = run_pair(oracle, gpu, c, 2)
+    assert_bitwise(so, sg)
