@@ -640,6 +640,85 @@ __global__ void k_metric_ratio(double* const* m, long long H) {
   double jac = m[G_AJAC][t];
   for (int a = 0; a < 9; a++) m[G_AKX1 + a][t] = m[a][t] / jac;
 }
+// Jac_Ghost_Boundary (OCFD_GhostCell.f90:1-160, 366-580) on the ghost slab of one face: LAP planes
+// outside the face, tangential interior range. Thread t -> (depth 1..LAP, tangential a, b).
+__device__ __forceinline__ bool ghost_point(int face, long long t, int& g, int& a, int& b, int& n) {
+  const int dir = face / 2, side = face % 2;
+  n = dir == 0 ? cC.nx : (dir == 1 ? cC.ny : cC.nz);
+  const int ta = dir == 0 ? cC.ny : cC.nx, tb = dir == 2 ? cC.ny : cC.nz;
+  if (t >= (long long)ta * tb * OCFD_L) return false;
+  a = (int)(t % ta) + 1;
+  const int l = (int)((t / ta) % OCFD_L) + 1;
+  b = (int)(t / ta / OCFD_L) + 1;
+  g = side == 0 ? 1 - l : n + l;
+  return true;
+}
+__device__ __forceinline__ int face_at(int dir, int s, int a, int b) {
+  return dir == 0 ? hidx(s, a, b) : (dir == 1 ? hidx(a, s, b) : hidx(a, b, s));
+}
+// Ghost_Cell = 1: copy the face plane's metrics, extrapolate the coordinates linearly
+__global__ void k_jac_ghost1(int face, double* X, double* Y, double* Z, double* const* m) {
+  int g, a, b, n;
+  if (!ghost_point(face, (long long)blockIdx.x * blockDim.x + threadIdx.x, g, a, b, n)) return;
+  const int dir = face / 2, side = face % 2;
+  const int qg = face_at(dir, g, a, b), qb = face_at(dir, side == 0 ? 1 : n, a, b);
+  const int q2 = face_at(dir, side == 0 ? 2 : n - 1, a, b);
+  for (int k = 0; k < 10; k++) m[k][qg] = m[k][qb];
+  const double f = side == 0 ? (1.0 - g) : (double)(g - n);
+  X[qg] = X[qb] + f * (X[qb] - X[q2]);
+  Y[qg] = Y[qb] + f * (Y[qb] - Y[q2]);
+  Z[qg] = Z[qb] + f * (Z[qb] - Z[q2]);
+}
+// Ghost_Cell = 2: mirror the coordinates (x_g = 2 x_b - x_mirror) ...
+__global__ void k_jac_ghost2_coords(int face, double* X, double* Y, double* Z) {
+  int g, a, b, n;
+  if (!ghost_point(face, (long long)blockIdx.x * blockDim.x + threadIdx.x, g, a, b, n)) return;
+  const int dir = face / 2, side = face % 2;
+  const int qg = face_at(dir, g, a, b), qb = face_at(dir, side == 0 ? 1 : n, a, b);
+  const int qm = face_at(dir, side == 0 ? 2 - g : 2 * n - g, a, b);
+  X[qg] = 2.0 * X[qb] - X[qm];
+  Y[qg] = 2.0 * Y[qb] - Y[qm];
+  Z[qg] = 2.0 * Z[qb] - Z[qm];
+}
+// ... and recompute the metrics there (comput_Jacobian3d_Ghost): derivatives one-sided at the ends
+// of each range, 2nd-order central next to them, 4th-order central elsewhere
+__global__ void k_jac_ghost2_metric(int face, const double* X, const double* Y, const double* Z, double* const* m) {
+  int g, a, b, n;
+  if (!ghost_point(face, (long long)blockIdx.x * blockDim.x + threadIdx.x, g, a, b, n)) return;
+  const int dir = face / 2, side = face % 2;
+  int lo[3] = {1, 1, 1}, hi[3] = {cC.nx, cC.ny, cC.nz};
+  lo[dir] = side == 0 ? 1 - OCFD_L : n;
+  hi[dir] = side == 0 ? 1 : n + OCFD_L;
+  int i = dir == 0 ? g : a, j = dir == 0 ? a : (dir == 1 ? g : b), k = dir == 2 ? g : b;
+  if (dir == 2) { i = a; j = b; }
+  const int q = hidx(i, j, k);
+  const int pos[3] = {i, j, k};
+  auto der = [&](const double* A, int dd) {
+    const double* f = A + q;
+    const int s = hstride(dd);
+    const double h = cC.h[dd];
+    const int ps = pos[dd];
+    if (ps == lo[dd]) return (-3.0 * f[0] + 4.0 * f[s] - f[2 * s]) / (2.0 * h);
+    if (ps == hi[dd]) return (f[-2 * s] - 4.0 * f[-s] + 3.0 * f[0]) / (2.0 * h);
+    if (ps == lo[dd] + 1 || ps == hi[dd] - 1) return (f[s] - f[-s]) / (2.0 * h);
+    return (8.0 * (f[s] - f[-s]) - (f[2 * s] - f[-2 * s])) / (12.0 * h);
+  };
+  double xi1 = der(X, 0), yi1 = der(Y, 0), zi1 = der(Z, 0);
+  double xj1 = der(X, 1), yj1 = der(Y, 1), zj1 = der(Z, 1);
+  double xk1 = der(X, 2), yk1 = der(Y, 2), zk1 = der(Z, 2);
+  double jac = 1.0 / (xi1 * yj1 * zk1 + yi1 * zj1 * xk1 + zi1 * xj1 * yk1 - zi1 * yj1 * xk1 - yi1 * xj1 * zk1 -
+                      xi1 * zj1 * yk1);
+  m[G_AJAC][q] = jac;
+  m[G_AKX][q] = jac * (yj1 * zk1 - zj1 * yk1);
+  m[G_AKY][q] = jac * (zj1 * xk1 - xj1 * zk1);
+  m[G_AKZ][q] = jac * (xj1 * yk1 - yj1 * xk1);
+  m[G_AIX][q] = jac * (yk1 * zi1 - zk1 * yi1);
+  m[G_AIY][q] = jac * (zk1 * xi1 - xk1 * zi1);
+  m[G_AIZ][q] = jac * (xk1 * yi1 - yk1 * xi1);
+  m[G_ASX][q] = jac * (yi1 * zj1 - zi1 * yj1);
+  m[G_ASY][q] = jac * (zi1 * xj1 - xi1 * zj1);
+  m[G_ASZ][q] = jac * (xi1 * yj1 - yi1 * xj1);
+}
 // tensor-product grids: dx/dxi(i), dy/deta(j), dz/dzeta(k) with the same CD6/CD8 + closures
 __global__ void k_metric1d(const double* X, const double* Y, const double* Z, double* dx, double* dy, double* dz) {
   int t = blockIdx.x * blockDim.x + threadIdx.x;
@@ -741,10 +820,9 @@ int validate(const ocfd_params* p) {
   if (!(p->flux_splitting == 1 || p->flux_splitting == 2)) return bad("Flux_Splitting must be 1 or 2");
   for (int m = 0; m < 6; m++) {
     if (p->scheme_boundary[m] < -1 || p->scheme_boundary[m] > 1) return bad("Scheme_boundary must be -1, 0 or 1");
-    if (p->ghost_cell[m] != 0) {
-      // ghost cells need the Jacobian ghost extension of init_mesh (Jac_Ghost_boundary,
-      // OCFD_GhostCell.f90:1-160, 366-580) as well as the flow extrapolation; not built
-      g_err = "Ghost_Cell != 0 is not built";
+    if (p->ghost_cell[m] < 0 || p->ghost_cell[m] > 2) {
+      // Ghost_Cell = -1 is the reference's user-defined ghost cell (OCFD_GhostCell_UserDef.f90)
+      g_err = "Ghost_Cell must be 0, 1 or 2 (user-defined ghost cells are not carried)";
       return OCFD_ERR_UNSUPPORTED;
     }
   }
@@ -850,6 +928,8 @@ int ocfd_gpu_init(const ocfd_params* p, const ocfd_thermo* th, const ocfd_kineti
     CK(cudaMemcpyToSymbol(cC, &c, sizeof(DevConst)));
 
     L->sep = separable(p, coords);
+    for (int m = 0; m < 6; m++)
+      if (p->ghost_cell[m] != 0) L->sep = false;  // ghost slabs carry their own metrics
     const long long H = c.H, N = c.N;
     const int NS = p->n_spec;
     size_t total = 0;
@@ -965,6 +1045,21 @@ int ocfd_gpu_init(const ocfd_params* p, const ocfd_thermo* th, const ocfd_kineti
       }
       std::vector<double*> ml(L->met, L->met + 10);
       exchange_v(ml, 7);
+      // Jac_Ghost_boundary: all Ghost_Cell = 1 faces, then the Ghost_Cell = 2 faces
+      for (int pass = 1; pass <= 2; pass++)
+        for (int face = 0; face < 6; face++) {
+          if (p->ghost_cell[face] != pass) continue;
+          const int dir = face / 2;
+          const long long na = dir == 0 ? p->ny : p->nx, nb = dir == 2 ? p->ny : p->nz;
+          const unsigned nbk = nblk(na * nb * OCFD_L, 128);
+          if (pass == 1) {
+            k_jac_ghost1<<<nbk, 128, 0, L->st>>>(face, L->X, L->Y, L->Z, met_ptrs);
+          } else {
+            k_jac_ghost2_coords<<<nbk, 128, 0, L->st>>>(face, L->X, L->Y, L->Z);
+            k_jac_ghost2_metric<<<nbk, 128, 0, L->st>>>(face, L->X, L->Y, L->Z, met_ptrs);
+          }
+          LAUNCH_CHECK();
+        }
       k_metric_ratio<<<nblk(H, 256), 256, 0, L->st>>>(met_ptrs, H);
       LAUNCH_CHECK();
     }

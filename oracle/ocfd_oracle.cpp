@@ -146,7 +146,7 @@ struct Oracle {
     nx = P.nx; ny = P.ny; nz = P.nz; L = P.lap; NS = P.n_spec;
     if (L != 4 || NS < 1 || NS > OCFD_MAX_SPEC || nx < 8 || ny < 8 || nz < 8) { err = "bad sizes"; return OCFD_ERR_PARAM; }
     for (int m = 0; m < 6; m++)
-      if (P.ghost_cell[m] != 0) { err = "Ghost_Cell != 0 (needs Jac_Ghost_boundary) is not restated"; return OCFD_ERR_UNSUPPORTED; }
+      if (P.ghost_cell[m] < 0 || P.ghost_cell[m] > 2) { err = "Ghost_Cell must be 0, 1 or 2"; return OCFD_ERR_UNSUPPORTED; }
     HX = nx + 2 * L; HY = ny + 2 * L; HZ = nz + 2 * L; H = HX * HY * HZ; N = (long)nx * ny * nz;
     hx = 1.0 / (nx - 1.0); hy = 1.0 / (ny - 1.0); hz = 1.0 / (nz - 1.0);
     for (int dd = 0; dd < 3; dd++) bound[dd][0] = bound[dd][1] = P.iperiodic[dd] == 0 ? 1 : 0;
@@ -195,6 +195,7 @@ struct Oracle {
       jacobian();
     }
     for (int m = 0; m < 10; m++) exch(M[m].data());
+    jac_ghost();
     for (long q = 0; q < H; q++) {
       double jac = M[M_AJAC][q];
       for (int m = 0; m < 9; m++) M[M_AKX1 + m][q] = M[M_AKX + m][q] / jac;
@@ -239,6 +240,85 @@ struct Oracle {
         }
     }
     return 0;
+  }
+
+  /* Jac_Ghost_boundary (OCFD_GhostCell.f90:1-6): on every face with Ghost_Cell = 1 the ghost
+   * slab (LAP planes outside the face, tangential interior range) copies the face plane's metrics
+   * and extrapolates the coordinates linearly (Jac_Ghost_Extent_1st, :18-160); with Ghost_Cell = 2
+   * the coordinates are mirrored (x_g = 2 x_b - x_mirror) and the metrics recomputed in the slab
+   * by comput_Jacobian3d_Ghost (:366-580), whose derivatives are one-sided at the ends of each
+   * range, 2nd-order central next to them and 4th-order central elsewhere. */
+  void jac_ghost() {
+    for (int pass = 1; pass <= 2; pass++)
+      for (int face = 0; face < 6; face++) {
+        if (P.ghost_cell[face] != pass) continue;
+        const int dir = face / 2, side = face % 2;
+        const int n = dir == 0 ? nx : (dir == 1 ? ny : nz);
+        const int ta = dir == 0 ? ny : nx, tb = dir == 2 ? ny : nz; /* tangential sizes */
+        auto at = [&](int s, int a, int b) {
+          return dir == 0 ? ih(s, a, b) : (dir == 1 ? ih(a, s, b) : ih(a, b, s));
+        };
+        const int g0 = side == 0 ? 1 - L : n + 1, g1 = side == 0 ? 0 : n + L;
+        const int ib = side == 0 ? 1 : n;
+        for (int b = 1; b <= tb; b++)
+          for (int a = 1; a <= ta; a++)
+            for (int g = g0; g <= g1; g++) {
+              long qg = at(g, a, b), qb = at(ib, a, b);
+              if (pass == 1) {
+                for (int m = 0; m < 10; m++) M[m][qg] = M[m][qb];
+                long q2 = at(side == 0 ? 2 : n - 1, a, b);
+                double f = side == 0 ? (1.0 - g) : (double)(g - n);
+                X[qg] = X[qb] + f * (X[qb] - X[q2]);
+                Y[qg] = Y[qb] + f * (Y[qb] - Y[q2]);
+                Z[qg] = Z[qb] + f * (Z[qb] - Z[q2]);
+              } else {
+                long qm = at(side == 0 ? 2 - g : 2 * n - g, a, b);
+                X[qg] = 2.0 * X[qb] - X[qm];
+                Y[qg] = 2.0 * Y[qb] - Y[qm];
+                Z[qg] = 2.0 * Z[qb] - Z[qm];
+              }
+            }
+        if (pass == 2) {
+          /* derivative ranges: [lo, hi] along each direction */
+          int lo[3] = {1, 1, 1}, hi[3] = {nx, ny, nz};
+          lo[dir] = side == 0 ? 1 - L : n;
+          hi[dir] = side == 0 ? 1 : n + L;
+          const double hh[3] = {hx, hy, hz};
+          const long st[3] = {1, HX, HX * HY};
+          auto der = [&](const std::vector<double>& A, long q, int dd, int pos) {
+            const double* f = A.data() + q;
+            const long s = st[dd];
+            const double h = hh[dd];
+            if (pos == lo[dd]) return (-3.0 * f[0] + 4.0 * f[s] - f[2 * s]) / (2.0 * h);
+            if (pos == hi[dd]) return (f[-2 * s] - 4.0 * f[-s] + 3.0 * f[0]) / (2.0 * h);
+            if (pos == lo[dd] + 1 || pos == hi[dd] - 1) return (f[s] - f[-s]) / (2.0 * h);
+            return (8.0 * (f[s] - f[-s]) - (f[2 * s] - f[-2 * s])) / (12.0 * h);
+          };
+          for (int b = 1; b <= tb; b++)
+            for (int a = 1; a <= ta; a++)
+              for (int g = g0; g <= g1; g++) {
+                int i = dir == 0 ? g : a, j = dir == 0 ? a : (dir == 1 ? g : b), k = dir == 2 ? g : b;
+                if (dir == 2) { i = a; j = b; }
+                long q = ih(i, j, k);
+                int pos[3] = {i, j, k};
+                double xi1 = der(X, q, 0, pos[0]), yi1 = der(Y, q, 0, pos[0]), zi1 = der(Z, q, 0, pos[0]);
+                double xj1 = der(X, q, 1, pos[1]), yj1 = der(Y, q, 1, pos[1]), zj1 = der(Z, q, 1, pos[1]);
+                double xk1 = der(X, q, 2, pos[2]), yk1 = der(Y, q, 2, pos[2]), zk1 = der(Z, q, 2, pos[2]);
+                double jac = 1.0 / (xi1 * yj1 * zk1 + yi1 * zj1 * xk1 + zi1 * xj1 * yk1 - zi1 * yj1 * xk1 -
+                                    yi1 * xj1 * zk1 - xi1 * zj1 * yk1);
+                M[M_AJAC][q] = jac;
+                M[M_AKX][q] = jac * (yj1 * zk1 - zj1 * yk1);
+                M[M_AKY][q] = jac * (zj1 * xk1 - xj1 * zk1);
+                M[M_AKZ][q] = jac * (xj1 * yk1 - yj1 * xk1);
+                M[M_AIX][q] = jac * (yk1 * zi1 - zk1 * yi1);
+                M[M_AIY][q] = jac * (zk1 * xi1 - xk1 * zi1);
+                M[M_AIZ][q] = jac * (xk1 * yi1 - yk1 * xi1);
+                M[M_ASX][q] = jac * (yi1 * zj1 - zi1 * yj1);
+                M[M_ASY][q] = jac * (zi1 * xj1 - xi1 * zj1);
+                M[M_ASZ][q] = jac * (xi1 * yj1 - yi1 * xj1);
+              }
+        }
+      }
   }
 
   void periodic_shift() {

@@ -232,7 +232,7 @@ def test_negative_energy_repair_bitwise(oracle, gpu):
 
 def test_bad_parameters_rejected(gpu):
     c = cases.isotropic(n=12)
-    c.params.ghost_cell[0] = 1
+    c.params.ghost_cell[0] = -1  # user-defined ghost cells
     with pytest.raises(gpu.OcfdError) as ei:
         gpu.Solver(c)
     assert ei.value.code == abi.ERR_UNSUPPORTED
@@ -277,3 +277,38 @@ def test_characteristic_llf_weno5_flatplate_bitwise(oracle, gpu):
     c.params.flux_splitting = abi.SPLIT_LLF
     so, sg, *_ = run_pair(oracle, gpu, c, 2)
     assert_bitwise(so, sg)
+
+
+# ---------------------------------------------------------------- ghost cells
+GHOST_CASES = {
+    "wall_copy_weno5": {2: (1, 1)},                 # j- wall: Ghost_Cell 1, Scheme_boundary 1
+    "outlet_mirror_inner": {1: (2, -1)},            # i+ outlet: Ghost_Cell 2, Scheme_boundary -1
+    "upper_mirror_weno5": {3: (2, 1)},              # j+ upper: Ghost_Cell 2, Scheme_boundary 1
+    "three_faces": {1: (2, 1), 2: (1, 1), 3: (2, -1)},
+}
+
+
+@pytest.mark.parametrize("name", list(GHOST_CASES))
+def test_ghost_cells_flatplate_bitwise(oracle, gpu, name):
+    """Ghost_Cell 1 / 2 faces: the Jacobian ghost slabs of init_mesh (copy or mirrored
+    coordinates + comput_Jacobian3d_Ghost) and the flow extrapolation after every boundary
+    condition, read by the WENO5 (Scheme_boundary 1) or interior (-1) schemes at the face."""
+    c = cases.flatplate(nx=40, ny=24, nz=12, scheme="WENO5", lx=0.01, ly=0.004, y1=2e-5)
+    for face, (gc, sb) in GHOST_CASES[name].items():
+        c.params.ghost_cell[face] = gc
+        c.params.scheme_boundary[face] = sb
+    o = oracle.OracleSolver(c)
+    mo = o.metrics()
+    o.close()
+    g = gpu.Solver(c)
+    mg = g.metrics()
+    g.close()
+    assert np.array_equal(mo, mg)  # full halo arrays, ghost slabs included
+    so, sg, *_ = run_pair(oracle, gpu, c, 2)
+    assert_bitwise(so, sg)
+    pro, prg = so[2], sg[2]
+    for face in GHOST_CASES[name]:  # the ghost cells of the primitive arrays too
+        dim = 3 - face // 2  # arrays are (var, k, j, i)
+        sl = [slice(None), slice(L, -L), slice(L, -L), slice(L, -L)]
+        sl[dim] = slice(0, L) if face % 2 == 0 else slice(-L, None)
+        assert np.array_equal(pro[tuple(sl)], prg[tuple(sl)])
