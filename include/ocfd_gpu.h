@@ -246,6 +246,14 @@ int ocfd_gpu_finalize(void);
  * (roofline denominator for the FP64-bound kernels). */
 double ocfd_gpu_fp64_peak_gflops(void);
 
+/* ---- learned chemistry surrogate (no counterpart in the reference) ----
+ * Tensor-core GEMM of the surrogate's dense layers, exposed for testing: on device pointers,
+ * C(M x N) = A(M x K) . B(N x K)^T (+ bias(N)) (+ C when beta = 1), then GELU when act = 1.
+ * A and B are BF16 read through element strides (A(m,k) = A[m*sam + k*sak], B(n,k) =
+ * B[n*sbn + k*sbk]), C is FP32 with leading dimension ldc. Synchronous. */
+int ocfd_gpu_gemm_bf16(int M, int N, int K, const void* A, long long sam, long long sak, const void* B, long long sbn,
+                       long long sbk, float* C, long long ldc, const float* bias, int beta, int act);
+
 #ifdef __cplusplus
 }
 #endif

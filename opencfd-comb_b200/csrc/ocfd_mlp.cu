@@ -1,0 +1,184 @@
+// Dense layers of the chemistry surrogate on the 5th-generation tensor cores (tcgen05, TMEM).
+//
+// k_gemm_bf16: C(M x N) = A(M x K) . B(N x K)^T with BF16 operands and FP32 accumulation. A and B are
+// read from global memory through arbitrary element strides (so the same kernel serves x . W^T in
+// the forward pass and dY . W, dY^T . X in the backward pass) and staged into shared memory in the
+// canonical K-major layout; one elected thread issues the K = 16 MMAs of a 64-wide K block into a
+// 128 x BN FP32 accumulator in TMEM and commits them to an mbarrier; the epilogue reads TMEM
+// (one output row per thread) and applies bias, accumulation, GELU and a BF16 copy.
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "ocfd_tc.cuh"
+
+namespace ocfd {
+namespace mlp {
+
+constexpr int BM = 128, BK = 64, THREADS = 128;
+constexpr long long WAIT_LIMIT = 1LL << 24;  // mbarrier polls before the kernel reports a timeout
+
+struct GemmArgs {
+  const __nv_bfloat16* A;
+  long long sam, sak;  // A(m, k) = A[m * sam + k * sak]
+  const __nv_bfloat16* B;
+  long long sbn, sbk;  // B(n, k) = B[n * sbn + k * sbk]
+  float* C;            // C(m, n) = C[m * ldc + n], FP32 (may be null when only Cb is wanted)
+  long long ldc;
+  __nv_bfloat16* Cb;  // optional BF16 copy of the epilogue output
+  long long ldcb;
+  float* pre;  // optional FP32 copy before the activation (for the backward pass), ld = ldc
+  const float* bias;
+  int M, N, K;
+  int beta;  // 1: C = C + A . B^T
+  int act;   // 0: none, 1: GELU
+  int* err;  // set to 1 when an mbarrier wait runs out
+};
+
+__device__ __forceinline__ float gelu(float x) { return 0.5f * x * (1.0f + erff(x * 0.70710678118654752f)); }
+
+template <int BN>
+struct GemmSmem {
+  static constexpr int A_BYTES = BM * BK * 2, B_BYTES = BN * BK * 2;
+  // padded so that at most four blocks share an SM (4 x BN <= 512 TMEM columns)
+  static constexpr int BYTES = 57344;
+  static_assert(A_BYTES + B_BYTES + 64 <= BYTES, "tile does not fit");
+};
+
+// stage a rows x BK tile (rows from r0, K from k0) of a strided BF16 matrix into the K-major layout
+template <int R>
+__device__ __forceinline__ void stage(uint8_t* dst, const __nv_bfloat16* src, long long sr, long long sk, int r0,
+                                      int nr, int k0, int nk) {
+  for (int c = threadIdx.x; c < R * (BK / 8); c += THREADS) {
+    const int r = c % R, kc = c / R;
+    const int gr = r0 + r;
+    __align__(16) __nv_bfloat16 v[8];
+#pragma unroll
+    for (int j = 0; j < 8; j++) {
+      const int gk = k0 + kc * 8 + j;
+      v[j] = (gr < nr && gk < nk) ? src[(long long)gr * sr + (long long)gk * sk] : __float2bfloat16(0.0f);
+    }
+    *reinterpret_cast<uint4*>(dst + tc::kmajor_off(r, kc * 8, R)) = *reinterpret_cast<const uint4*>(v);
+  }
+}
+
+template <int BN>
+__global__ void __launch_bounds__(THREADS) k_gemm_bf16(GemmArgs g) {
+  extern __shared__ __align__(1024) uint8_t sm[];
+  uint8_t* sA = sm;
+  uint8_t* sB = sm + GemmSmem<BN>::A_BYTES;
+  uint64_t* bar = reinterpret_cast<uint64_t*>(sB + GemmSmem<BN>::B_BYTES);
+  uint32_t* tslot = reinterpret_cast<uint32_t*>(bar + 1);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int m0 = blockIdx.x * BM, n0 = blockIdx.y * BN;
+
+  if (warp == 0) tc::tmem_alloc(tslot, BN);
+  if (tid == 0) {
+    tc::mbar_init(bar, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  tc::fence_before();
+  __syncthreads();
+  tc::fence_after();
+  const uint32_t tmem = *tslot;
+  constexpr uint32_t idesc = tc::idesc_bf16(BM, BN);
+  const uint32_t aaddr = tc::smem_u32(sA), baddr = tc::smem_u32(sB);
+  bool ok = true;
+  uint32_t phase = 0;
+  const int nkb = (g.K + BK - 1) / BK;
+  for (int kb = 0; kb < nkb && ok; kb++) {
+    stage<BM>(sA, g.A, g.sam, g.sak, m0, g.M, kb * BK, g.K);
+    stage<BN>(sB, g.B, g.sbn, g.sbk, n0, g.N, kb * BK, g.K);
+    tc::fence_proxy_async();  // generic-proxy smem writes -> visible to the tensor core
+    __syncthreads();
+    if (tid == 0) {
+      tc::fence_after();
+#pragma unroll
+      for (int s = 0; s < BK / 16; s++) {
+        const uint64_t ad = tc::smem_desc(aaddr + s * 2 * (BM * 16), BM * 16, 128);
+        const uint64_t bd = tc::smem_desc(baddr + s * 2 * (BN * 16), BN * 16, 128);
+        tc::mma_bf16(tmem, ad, bd, idesc, (kb > 0 || s > 0) ? 1u : 0u);
+      }
+      tc::mma_commit(tc::smem_u32(bar));
+    }
+    ok = tc::mbar_wait(bar, phase, WAIT_LIMIT);
+    phase ^= 1u;
+  }
+  if (!ok) {
+    if (lane == 0) atomicExch(g.err, 1);
+    // give the tensor core a last bounded chance to finish before the TMEM is released
+    tc::mbar_wait(bar, phase ^ 1u, WAIT_LIMIT);
+  } else {
+    tc::fence_after();
+    const int row = m0 + 32 * warp + lane;
+#pragma unroll 1
+    for (int c0 = 0; c0 < BN; c0 += 32) {
+      float v[32];
+      tc::tmem_ld32(tmem + ((uint32_t)(32 * warp) << 16) + (uint32_t)c0, v);
+      if (row < g.M) {
+#pragma unroll
+        for (int j = 0; j < 32; j++) {
+          const int n = n0 + c0 + j;
+          if (n >= g.N) break;
+          float val = v[j];
+          if (g.bias) val += g.bias[n];
+          const long long o = (long long)row * g.ldc + n;
+          if (g.beta) val += g.C[o];
+          if (g.pre) g.pre[o] = val;
+          if (g.act == 1) val = gelu(val);
+          if (g.C) g.C[o] = val;
+          if (g.Cb) g.Cb[(long long)row * g.ldcb + n] = __float2bfloat16(val);
+        }
+      }
+    }
+  }
+  tc::fence_before();
+  __syncthreads();
+  if (warp == 0) tc::tmem_dealloc(tmem, BN);
+}
+
+int launch_gemm(const GemmArgs& g, cudaStream_t st) {
+  constexpr int BN = 128;
+  static bool attr = false;
+  if (!attr) {
+    cudaError_t e = cudaFuncSetAttribute(k_gemm_bf16<BN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         GemmSmem<BN>::BYTES);
+    if (e != cudaSuccess) return -2;
+    attr = true;
+  }
+  if (g.M <= 0 || g.N <= 0 || g.K <= 0) return 0;
+  dim3 grid((g.M + BM - 1) / BM, (g.N + BN - 1) / BN);
+  k_gemm_bf16<BN><<<grid, THREADS, GemmSmem<BN>::BYTES, st>>>(g);
+  return cudaGetLastError() == cudaSuccess ? 0 : -2;
+}
+
+}  // namespace mlp
+}  // namespace ocfd
+
+extern "C" {
+// C = A . B^T (+ bias, + C, GELU) on device pointers; synchronous; 0, -1 (bad sizes), -2 (CUDA
+// error) or -6 (an mbarrier wait ran out)
+int ocfd_gpu_gemm_bf16(int M, int N, int K, const void* A, long long sam, long long sak, const void* B, long long sbn,
+                       long long sbk, float* C, long long ldc, const float* bias, int beta, int act) {
+  using namespace ocfd::mlp;
+  if (M < 0 || N < 0 || K < 0 || !A || !B || !C) return -1;
+  int* derr = nullptr;
+  if (cudaMalloc(&derr, sizeof(int)) != cudaSuccess) return -2;
+  cudaMemset(derr, 0, sizeof(int));
+  GemmArgs g{};
+  g.A = static_cast<const __nv_bfloat16*>(A);
+  g.sam = sam; g.sak = sak;
+  g.B = static_cast<const __nv_bfloat16*>(B);
+  g.sbn = sbn; g.sbk = sbk;
+  g.C = C; g.ldc = ldc; g.bias = bias;
+  g.M = M; g.N = N; g.K = K; g.beta = beta; g.act = act; g.err = derr;
+  int rc = launch_gemm(g, 0);
+  if (cudaDeviceSynchronize() != cudaSuccess) rc = -2;
+  int herr = 0;
+  cudaMemcpy(&herr, derr, sizeof(int), cudaMemcpyDeviceToHost);
+  cudaFree(derr);
+  if (rc == 0 && herr) rc = -6;
+  return rc;
+}
+}

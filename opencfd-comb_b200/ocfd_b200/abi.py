@@ -141,4 +141,6 @@ GPU_SIGNATURES = {
     "ocfd_gpu_pinned_free": (I, [C.c_void_p]),
     "ocfd_gpu_step_launches": (I, []),
     "ocfd_gpu_chem_batch_noalloc": (I, [I, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "ocfd_gpu_gemm_bf16": (I, [I, I, I, C.c_void_p, C.c_longlong, C.c_longlong, C.c_void_p, C.c_longlong,
+                               C.c_longlong, C.c_void_p, C.c_longlong, C.c_void_p, I, I]),
 }
