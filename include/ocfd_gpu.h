@@ -254,6 +254,34 @@ double ocfd_gpu_fp64_peak_gflops(void);
 int ocfd_gpu_gemm_bf16(int M, int N, int K, const void* A, long long sam, long long sak, const void* B, long long sbn,
                        long long sbk, float* C, long long ldc, const float* bias, int beta, int act);
 
+/* The surrogate: a BF16 MLP (inputs T, log p, Y_1..Y_Ns, log dt; three hidden layers of 256, GELU;
+ * outputs dY_1..dY_Ns, dT) for 0-D reactors of the mechanism given to ocfd_gpu_chem_setup (or
+ * ocfd_gpu_init), 2 <= N_SPEC <= 9. All reactor arrays are device pointers, di as n x N_SPEC.
+ * ocfd_gpu_surrogate_init: seeded initial weights (for ocfd_gpu_surrogate_grad).
+ * ocfd_gpu_surrogate_train: trains on n reactors (di0, e0, dt) and their FP64-integrated states
+ * (di1, e1) with Adam (cosine-decayed lr), batch a multiple of 128; proj is the N_SPEC x N_SPEC
+ * projection onto element-conserving composition changes; loss_history gets one value per epoch.
+ * ocfd_gpu_surrogate_predict: ungated network updates (di_out, e_out), T0 + dT_pred (T_pred) and
+ * the temperature of the updated state's energy (T_energy).
+ * ocfd_gpu_chem_batch_surrogate: gated surrogate chemistry in place; reactors whose |T_energy -
+ * T_pred| exceeds tol_T, whose composition goes negative or whose input lies outside the training
+ * range are advanced by the FP64 implicit integrator instead; n_fallback gets their number.
+ * ocfd_gpu_surrogate_blob: save (set 0) / load (set 1) weights, normalisation and projection as
+ * floats; host NULL returns the size. ocfd_gpu_surrogate_grad: loss and parameter gradients of
+ * one batch of normalised inputs / targets (B x 16 floats, host), for gradient checks.
+ * ocfd_gpu_chem_temperature: T of n reactors from densities and energy (comput_T). */
+int ocfd_gpu_surrogate_init(unsigned seed);
+int ocfd_gpu_surrogate_train(int n, const double* d_di0, const double* d_e0, const double* d_dt, const double* d_di1,
+                             const double* d_e1, const double* proj, int epochs, int batch, double lr, unsigned seed,
+                             double* loss_history);
+int ocfd_gpu_surrogate_predict(int n, const double* d_di, const double* d_e, const double* d_dt, double* d_di_out,
+                               double* d_e_out, double* d_T_pred, double* d_T_energy);
+int ocfd_gpu_chem_batch_surrogate(int n, double* d_di, double* d_e, const double* d_dt, const int* d_nsub,
+                                  double tol_T, int* n_fallback);
+long long ocfd_gpu_surrogate_blob(float* host, long long nfloats, int set);
+int ocfd_gpu_surrogate_grad(int B, const float* x, const float* t, float* grads, double* loss);
+int ocfd_gpu_chem_temperature(int n, const double* d_di, const double* d_e, double* d_T);
+
 #ifdef __cplusplus
 }
 #endif

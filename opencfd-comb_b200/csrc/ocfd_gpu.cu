@@ -807,6 +807,13 @@ __global__ void k_fp64_peak(double* out, int iters, double a, double b) {
 }
 }  // namespace ocfd
 
+namespace ocfd {
+// the species count and the stream of the current set-up (ocfd_gpu_init or ocfd_gpu_chem_setup),
+// for the surrogate module
+int current_nspec() { return L && L->have_kin ? L->NS : 0; }
+cudaStream_t current_stream() { return L ? L->st : nullptr; }
+}  // namespace ocfd
+
 namespace {
 
 int validate(const ocfd_params* p) {

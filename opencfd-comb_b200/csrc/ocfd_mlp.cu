@@ -11,6 +11,7 @@
 
 #include <cstdint>
 
+#include "ocfd_mlp.h"
 #include "ocfd_tc.cuh"
 
 namespace ocfd {
@@ -19,24 +20,13 @@ namespace mlp {
 constexpr int BM = 128, BK = 64, THREADS = 128;
 constexpr long long WAIT_LIMIT = 1LL << 24;  // mbarrier polls before the kernel reports a timeout
 
-struct GemmArgs {
-  const __nv_bfloat16* A;
-  long long sam, sak;  // A(m, k) = A[m * sam + k * sak]
-  const __nv_bfloat16* B;
-  long long sbn, sbk;  // B(n, k) = B[n * sbn + k * sbk]
-  float* C;            // C(m, n) = C[m * ldc + n], FP32 (may be null when only Cb is wanted)
-  long long ldc;
-  __nv_bfloat16* Cb;  // optional BF16 copy of the epilogue output
-  long long ldcb;
-  float* pre;  // optional FP32 copy before the activation (for the backward pass), ld = ldc
-  const float* bias;
-  int M, N, K;
-  int beta;  // 1: C = C + A . B^T
-  int act;   // 0: none, 1: GELU
-  int* err;  // set to 1 when an mbarrier wait runs out
-};
+
 
 __device__ __forceinline__ float gelu(float x) { return 0.5f * x * (1.0f + erff(x * 0.70710678118654752f)); }
+// d GELU / dx = Phi(x) + x phi(x)
+__device__ __forceinline__ float gelu_grad(float x) {
+  return 0.5f * (1.0f + erff(x * 0.70710678118654752f)) + x * 0.39894228040143268f * expf(-0.5f * x * x);
+}
 
 template <int BN>
 struct GemmSmem {
@@ -125,8 +115,12 @@ __global__ void __launch_bounds__(THREADS) k_gemm_bf16(GemmArgs g) {
           if (g.bias) val += g.bias[n];
           const long long o = (long long)row * g.ldc + n;
           if (g.beta) val += g.C[o];
-          if (g.pre) g.pre[o] = val;
-          if (g.act == 1) val = gelu(val);
+          if (g.act == 1) {
+            if (g.pre) g.pre[o] = val;
+            val = gelu(val);
+          } else if (g.act == 2) {
+            val *= gelu_grad(g.pre[o]);
+          }
           if (g.C) g.C[o] = val;
           if (g.Cb) g.Cb[(long long)row * g.ldcb + n] = __float2bfloat16(val);
         }

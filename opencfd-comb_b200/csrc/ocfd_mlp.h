@@ -1,0 +1,31 @@
+// Dense-layer GEMM of the chemistry surrogate (tcgen05, ocfd_mlp.cu), shared with the surrogate's
+// training and inference code (ocfd_surrogate.cu).
+#pragma once
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+namespace ocfd {
+namespace mlp {
+
+struct GemmArgs {
+  const __nv_bfloat16* A;
+  long long sam, sak;  // A(m, k) = A[m * sam + k * sak]
+  const __nv_bfloat16* B;
+  long long sbn, sbk;  // B(n, k) = B[n * sbn + k * sbk]
+  float* C;            // C(m, n) = C[m * ldc + n], FP32 (may be null when only Cb is wanted)
+  long long ldc;
+  __nv_bfloat16* Cb;  // optional BF16 copy of the epilogue output
+  long long ldcb;
+  float* pre;  // act 1: FP32 copy before the activation is written here; act 2: read from here
+  const float* bias;
+  int M, N, K;
+  int beta;  // 1: C = C + A . B^T
+  int act;   // 0: none, 1: GELU, 2: multiply by GELU'(pre) (backward through the activation)
+  int* err;  // set to 1 when an mbarrier wait runs out
+};
+
+// launches k_gemm_bf16 on stream st; 0 or -2 (CUDA error)
+int launch_gemm(const GemmArgs& g, cudaStream_t st);
+
+}  // namespace mlp
+}  // namespace ocfd

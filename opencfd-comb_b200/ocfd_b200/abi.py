@@ -143,4 +143,13 @@ GPU_SIGNATURES = {
     "ocfd_gpu_chem_batch_noalloc": (I, [I, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "ocfd_gpu_gemm_bf16": (I, [I, I, I, C.c_void_p, C.c_longlong, C.c_longlong, C.c_void_p, C.c_longlong,
                                C.c_longlong, C.c_void_p, C.c_longlong, C.c_void_p, I, I]),
+    "ocfd_gpu_surrogate_init": (I, [C.c_uint]),
+    "ocfd_gpu_surrogate_train": (I, [I, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, PD, I, I, D,
+                                     C.c_uint, PD]),
+    "ocfd_gpu_surrogate_predict": (I, [I, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                       C.c_void_p]),
+    "ocfd_gpu_chem_batch_surrogate": (I, [I, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, D, PI]),
+    "ocfd_gpu_surrogate_blob": (C.c_longlong, [C.POINTER(C.c_float), C.c_longlong, I]),
+    "ocfd_gpu_surrogate_grad": (I, [I, C.POINTER(C.c_float), C.POINTER(C.c_float), C.POINTER(C.c_float), PD]),
+    "ocfd_gpu_chem_temperature": (I, [I, C.c_void_p, C.c_void_p, C.c_void_p]),
 }

@@ -1,0 +1,140 @@
+"""Learned chemistry surrogate over the library's C ABI (no counterpart in the reference).
+
+The network maps a 0-D reactor state (T, log p, Y_k, log dt) to its increments (dY_k, dT) over dt.
+It is trained on the GPU by the library's own tensor-core kernels on states that the FP64 implicit
+integrator produced, and it is applied behind a gate: the composition change is projected so that
+element and total mass are conserved exactly, the energy follows the reference's formation-enthalpy
+bookkeeping, T comes from the conserved energy, and a reactor whose network temperature disagrees
+with that T by more than tol_T (or whose composition goes negative, or whose state lies outside the
+training range) is advanced by the FP64 integrator instead.
+"""
+import ctypes as C
+import re
+
+import numpy as np
+
+from . import abi, cases, solver
+
+ELEMENT_MASS = {"H": 1.00794e-3, "O": 15.9994e-3, "N": 14.0067e-3, "C": 12.0107e-3, "AR": 39.948e-3,
+                "HE": 4.002602e-3}
+
+
+def composition(name):
+    """Atoms per molecule of a species name such as H2O2 or HO2."""
+    out = {}
+    for el, cnt in re.findall(r"(AR|HE|[A-Z])(\d*)", name.upper()):
+        out[el] = out.get(el, 0) + (int(cnt) if cnt else 1)
+    return out
+
+
+def element_projection(names, mi):
+    """P = I - G^T (G G^T)^-1 G, G(e, k) = a_ek M_e / M_k: dY -> P dY keeps every element's mass
+    fraction (and so the total mass) unchanged."""
+    comps = [composition(n) for n in names]
+    els = sorted({e for c in comps for e in c})
+    G = np.array([[c.get(e, 0) * ELEMENT_MASS[e] / mi[k] for k, c in enumerate(comps)] for e in els])
+    return np.eye(len(names)) - G.T @ np.linalg.solve(G @ G.T, G), G
+
+
+def _dev(torch, a, dtype=None):
+    t = torch.from_numpy(np.ascontiguousarray(a)).to("cuda")
+    return t if dtype is None else t.to(dtype)
+
+
+class Surrogate:
+    """Training and evaluation driver (device buffers through torch, kernels through the C ABI)."""
+
+    def __init__(self):
+        import torch
+        self.torch = torch
+        self.L = solver.lib()
+        self.names, self.th, self.kin, _ = cases.h2air_structs()
+        self.ns = len(self.names)
+        solver.chem_setup(self.th, self.kin, 1, abi.CHEM_IMPLICIT)
+        self.mi = np.array([self.th.mi[k] for k in range(self.ns)])
+        self.proj, self.G = element_projection(self.names, self.mi)
+
+    def reactors(self, n, seed):
+        names, th, kin, di, E, dt, nsub, T = cases.reactors(n=n, seed=seed)
+        return di, E, dt, nsub
+
+    def fp64(self, di, E, dt, nsub):
+        """FP64 implicit integration on the GPU (device tensors in, updated copies out)."""
+        t = self.torch
+        # fresh copies (synchronous host-to-device), not clones: the library runs on its own stream
+        d_di, d_e = _dev(t, di), _dev(t, E)
+        d_dt, d_ns = _dev(t, dt), _dev(t, nsub)
+        solver.chem_batch_device(len(E), d_di.data_ptr(), d_e.data_ptr(), d_dt.data_ptr(), d_ns.data_ptr())
+        return d_di, d_e
+
+    def temperature(self, d_di, d_e):
+        T = self.torch.empty(d_e.shape[0], dtype=self.torch.float64, device="cuda")
+        solver._chk(self.L.ocfd_gpu_chem_temperature(d_e.shape[0], d_di.data_ptr(), d_e.data_ptr(), T.data_ptr()))
+        return T
+
+    def train(self, n=1 << 18, epochs=30, batch=1024, lr=2e-3, seed=0):
+        di, E, dt, nsub = self.reactors(n, seed)
+        t = self.torch
+        d_di0, d_e0, d_dt = _dev(t, di), _dev(t, E), _dev(t, dt)
+        d_di1, d_e1 = self.fp64(di, E, dt, nsub)
+        hist = np.zeros(epochs)
+        P = np.ascontiguousarray(self.proj)
+        solver._chk(self.L.ocfd_gpu_surrogate_train(n, d_di0.data_ptr(), d_e0.data_ptr(), d_dt.data_ptr(),
+                                                    d_di1.data_ptr(), d_e1.data_ptr(), abi.dptr(P), epochs, batch,
+                                                    lr, seed, abi.dptr(hist)))
+        return hist
+
+    def evaluate(self, n=1 << 16, seed=12345, tol_T=5.0):
+        """Held-out reactors: errors of the ungated network and of the gated surrogate against the
+        FP64 integrator, the fallback fraction and the element-conservation residual."""
+        t = self.torch
+        di, E, dt, nsub = self.reactors(n, seed)
+        d_di, d_e, d_dt, d_ns = _dev(t, di), _dev(t, E), _dev(t, dt), _dev(t, nsub)
+        f_di, f_e = self.fp64(di, E, dt, nsub)
+        T_ref = self.temperature(f_di, f_e)
+        o_di = t.empty_like(d_di)
+        o_e, Tp, Te = t.empty_like(d_e), t.empty_like(d_e), t.empty_like(d_e)
+        t.cuda.synchronize()
+        solver._chk(self.L.ocfd_gpu_surrogate_predict(n, d_di.data_ptr(), d_e.data_ptr(), d_dt.data_ptr(),
+                                                      o_di.data_ptr(), o_e.data_ptr(), Tp.data_ptr(), Te.data_ptr()))
+        g_di, g_e = _dev(t, di), _dev(t, E)
+        nfb = C.c_int()
+        solver._chk(self.L.ocfd_gpu_chem_batch_surrogate(n, g_di.data_ptr(), g_e.data_ptr(), d_dt.data_ptr(),
+                                                         d_ns.data_ptr(), tol_T, C.byref(nfb)))
+        T_g = self.temperature(g_di, g_e)
+        T0 = self.temperature(d_di, d_e)
+
+        def Y(x):
+            x = x.cpu().numpy()
+            return x / x.sum(axis=1, keepdims=True)
+
+        Yr, Yn, Yg, Y0 = Y(f_di), Y(o_di), Y(g_di), Y(d_di)
+        Tr = T_ref.cpu().numpy()
+        el0 = Y0 @ self.G.T
+        return {
+            "n": n,
+            "fallback_fraction": nfb.value / n,
+            "ungated_T_err_max_K": float(np.abs(Te.cpu().numpy() - Tr).max()),
+            "ungated_T_err_rel_max": float((np.abs(Te.cpu().numpy() - Tr) / Tr).max()),
+            "ungated_Y_err_max": float(np.abs(Yn - Yr).max()),
+            "gated_T_err_max_K": float(np.abs(T_g.cpu().numpy() - Tr).max()),
+            "gated_T_err_rel_max": float((np.abs(T_g.cpu().numpy() - Tr) / Tr).max()),
+            "gated_Y_err_max": float(np.abs(Yg - Yr).max()),
+            "no_reaction_T_err_max_K": float(np.abs(T0.cpu().numpy() - Tr).max()),
+            "no_reaction_Y_err_max": float(np.abs(Y0 - Yr).max()),
+            "element_residual_max": float(np.abs(Yg @ self.G.T - el0).max()),
+        }
+
+    def blob(self):
+        n = self.L.ocfd_gpu_surrogate_blob(None, 0, 0)
+        buf = (C.c_float * n)()
+        rc = self.L.ocfd_gpu_surrogate_blob(buf, n, 0)
+        if rc != 0:
+            raise solver.OcfdError(rc, "surrogate blob")
+        return np.frombuffer(buf, dtype=np.float32).copy()
+
+    def load(self, blob):
+        b = np.ascontiguousarray(blob, dtype=np.float32)
+        rc = self.L.ocfd_gpu_surrogate_blob(b.ctypes.data_as(C.POINTER(C.c_float)), len(b), 1)
+        if rc != 0:
+            raise solver.OcfdError(rc, "surrogate blob")

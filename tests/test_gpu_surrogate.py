@@ -1,0 +1,81 @@
+"""The learned chemistry surrogate: gradients of the library's tensor-core training pass against the
+CPU reference of the network, training progress, and the gated surrogate against the FP64 implicit
+integrator on held-out reactors (accuracy, exact element conservation, what the trained network
+gains over no network)."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def sg():
+    from ocfd_b200 import surrogate
+    return surrogate.Surrogate()
+
+
+def test_gradients_match_cpu_reference(sg):
+    import pymlp
+    L = sg.L
+    assert L.ocfd_gpu_surrogate_init(3) == 0
+    nblob = L.ocfd_gpu_surrogate_blob(None, 0, 0)
+    blob = (C.c_float * nblob)()
+    assert L.ocfd_gpu_surrogate_blob(blob, nblob, 0) == 0
+    params = pymlp.unpack(np.frombuffer(blob, dtype=np.float32))
+    rng = np.random.default_rng(5)
+    B, nout = 256, sg.ns + 1
+    x = np.zeros((B, 16), np.float32)
+    x[:, :sg.ns + 3] = rng.standard_normal((B, sg.ns + 3))
+    t = np.zeros((B, 16), np.float32)
+    t[:, :nout] = rng.standard_normal((B, nout))
+    g = np.zeros(sum(r * c + r for r, c in zip(pymlp.ROWS, pymlp.COLS)), np.float32)
+    loss = C.c_double()
+    fp = C.POINTER(C.c_float)
+    assert L.ocfd_gpu_surrogate_grad(B, x.ctypes.data_as(fp), t.ctypes.data_as(fp), g.ctypes.data_as(fp),
+                                     C.byref(loss)) == 0
+    ref_loss, ref = pymlp.loss_and_grads(params, x.astype(np.float64), t.astype(np.float64), nout)
+    assert abs(loss.value - ref_loss) <= 1e-5 * ref_loss
+    p = 0
+    for l, (r, c) in enumerate(zip(pymlp.ROWS, pymlp.COLS)):
+        gw = g[p:p + r * c].reshape(r, c)
+        p += r * c
+        gb = g[p:p + r]
+        p += r
+        rw, rb = ref[l]
+        assert np.abs(gw - rw).max() <= 5e-3 * np.abs(rw).max(), l
+        assert np.abs(gb - rb).max() <= 5e-3 * np.abs(rb).max(), l
+
+
+@pytest.fixture(scope="module")
+def trained(sg):
+    hist = sg.train(n=1 << 17, epochs=12, batch=1024, lr=2e-3, seed=0)
+    return sg, hist
+
+
+def test_training_reduces_loss(trained):
+    sg, hist = trained
+    assert np.isfinite(hist).all()
+    assert hist[-1] < 0.2 * hist[0], hist
+
+
+def test_gated_surrogate_against_fp64(trained):
+    sg, _ = trained
+    tol_T = 5.0
+    r = sg.evaluate(n=1 << 15, seed=4242, tol_T=tol_T)
+    # element (and so total) mass conserved to rounding by the projection
+    assert r["element_residual_max"] <= 1e-12, r
+    # accepted reactors are within the gate, the rest took the FP64 path
+    assert r["fallback_fraction"] < 1.0, r
+    assert r["gated_T_err_rel_max"] <= 0.01, r
+    assert r["gated_Y_err_max"] <= 1e-2, r
+    # the trained network gains over no network: far smaller errors than assuming no reaction
+    assert r["ungated_T_err_max_K"] < 0.5 * r["no_reaction_T_err_max_K"], r
+
+
+def test_blob_roundtrip(trained):
+    sg, _ = trained
+    b = sg.blob()
+    sg.load(b)
+    assert np.array_equal(sg.blob(), b)
