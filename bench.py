@@ -40,13 +40,16 @@ def parse():
     ap.add_argument("--steps", type=int, default=40)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="flatplate", choices=["flatplate", "isotropic", "jet", "reactors"],
+    ap.add_argument("--workload", default="flatplate", choices=["flatplate", "isotropic", "jet", "reactors", "surrogate"],
                     help="flatplate = the headline configuration; isotropic, jet and reactors are the other "
                          "configurations of the metric (64^3 decaying turbulence, the 384x256x256 reacting H2 jet, "
                          "2^20 batched 0-D reactors)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=5)
+    ap.add_argument("--sg-train", type=int, default=1 << 21, help="surrogate workload: training reactors")
+    ap.add_argument("--sg-epochs", type=int, default=20, help="surrogate workload: training epochs")
+    ap.add_argument("--sg-tol", type=float, default=5.0, help="surrogate workload: gate tolerance on T (K)")
     ap.add_argument("--character", action="store_true",
                     help="characteristic-space inviscid flux (IF_Scheme_Character = 1) instead of component-wise")
     ap.add_argument("--nz", type=int, default=None,
@@ -150,7 +153,7 @@ def main_reference(a):
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import pyoracle
     cores = pyoracle.lib().ocfd_cpu_set_threads(os.cpu_count() or 1)
-    if a.workload == "reactors":
+    if a.workload in ("reactors", "surrogate"):  # the reference has only the FP64 integrator
         return reactors_reference(a, pyoracle, cores)
     # size the per-step sample so that warmup + steps take about two minutes
     rate = 0.0
@@ -292,6 +295,94 @@ def main_reactors(a):
                       "substeps_per_s": sub * a.steps / (ms * 1e-3),
                       "l2": "inputs re-copied from a pristine device copy before each pass"},
            "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": None, "clocks": clk.summary()}
+    print(json.dumps(out))
+    return 0
+
+
+# ---------------------------------------------------------------- surrogate chemistry (C4)
+SMETRIC = "Mreactor-solves/s on 1 B200: plain FP64 vs gated surrogate chemistry at <=1% T error, 2^20 H2-air reactors"
+MLP_FLOPS_PER_SAMPLE = 2 * (16 * 256 + 256 * 256 * 2 + 256 * 16)  # padded forward pass
+
+
+def main_surrogate(a):
+    """Trains the surrogate on FP64-integrated reactors, then times the plain FP64 batch and the
+    gated surrogate on 2^20 held-out reactors (device-resident inputs restored before every pass)."""
+    import numpy as np
+    import torch
+    import ctypes as C
+    from ocfd_b200 import solver, surrogate
+    sg = surrogate.Surrogate()
+    L = sg.L
+    t0 = time.perf_counter()
+    hist = sg.train(n=a.sg_train, epochs=a.sg_epochs, batch=1024, lr=2e-3, seed=0)
+    train_s = time.perf_counter() - t0
+    n = 1 << 20
+    di, E, dt, nsub = sg.reactors(n, 4242)
+    dev = torch.device("cuda")
+    p_di, p_e = torch.from_numpy(di).to(dev), torch.from_numpy(E).to(dev)
+    d_dt, d_ns = torch.from_numpy(dt).to(dev), torch.from_numpy(nsub).to(dev)
+    w_di, w_e = p_di.clone(), p_e.clone()
+    o_di, o_e = torch.empty_like(p_di), torch.empty_like(p_e)
+    Tp, Te = torch.empty_like(p_e), torch.empty_like(p_e)
+    torch.cuda.synchronize()
+    st = torch.cuda.ExternalStream(L.ocfd_gpu_stream())
+    nfb = C.c_int()
+
+    def plain():
+        w_di.copy_(p_di)
+        w_e.copy_(p_e)
+        solver.chem_batch_device(n, w_di.data_ptr(), w_e.data_ptr(), d_dt.data_ptr(), d_ns.data_ptr())
+
+    def gated():
+        w_di.copy_(p_di)
+        w_e.copy_(p_e)
+        solver._chk(L.ocfd_gpu_chem_batch_surrogate(n, w_di.data_ptr(), w_e.data_ptr(), d_dt.data_ptr(),
+                                                    d_ns.data_ptr(), a.sg_tol, C.byref(nfb)))
+
+    def network():
+        solver._chk(L.ocfd_gpu_surrogate_predict(n, p_di.data_ptr(), p_e.data_ptr(), d_dt.data_ptr(),
+                                                 o_di.data_ptr(), o_e.data_ptr(), Tp.data_ptr(), Te.data_ptr()))
+
+    def timed(fn, k):
+        with torch.cuda.stream(st):
+            for _ in range(a.warmup):
+                fn()
+            st.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(st)
+            for _ in range(k):
+                fn()
+            e1.record(st)
+            st.synchronize()
+        return e0.elapsed_time(e1) / k
+
+    k = max(1, min(a.steps, 5))
+    with Clocks(0) as clk:
+        ms_plain = timed(plain, k)
+        ms_gated = timed(gated, k)
+        ms_net = timed(network, k)
+    acc = sg.evaluate(n=n, seed=4242, tol_T=a.sg_tol)
+    peaks_file = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    bf16_peak = None
+    if os.path.exists(peaks_file):
+        with open(peaks_file) as fh:
+            pk = json.load(fh)
+        bf16_peak = pk.get("bf16_tflops")
+    net_tflops = n * MLP_FLOPS_PER_SAMPLE / (ms_net * 1e-3) / 1e12
+    out = {"metric": SMETRIC, "value": n / (ms_gated * 1e-3) / 1e6, "unit": RUNIT, "n_gpus": 1, "steps": k,
+           "warmup": a.warmup, "ms_per_step": ms_gated, "higher_is_better": True, "scaling": "weak",
+           "vs_baseline": None, "dtype": "bf16 network + f64 fallback", "data": "synthetic (seeded)",
+           "config": {"workload": "reactors-2^20-H2air-9sp gated surrogate (MLP 12-256-256-256-10, GELU)",
+                      "train_reactors": a.sg_train, "epochs": a.sg_epochs, "train_seconds": train_s,
+                      "loss_first_last": [float(hist[0]), float(hist[-1])], "tol_T_K": a.sg_tol},
+           "plain_fp64": {"value": n / (ms_plain * 1e-3) / 1e6, "ms": ms_plain},
+           "speedup_vs_plain": ms_plain / ms_gated,
+           "accuracy": acc, "fallback_fraction": nfb.value / n,
+           "roofline": {"bound": "tensor", "kernel": "network pass (4 tcgen05 GEMMs + features + gate)",
+                        "achieved": net_tflops, "peak": bf16_peak, "unit": "TFLOP/s",
+                        "frac": (net_tflops / bf16_peak) if bf16_peak else None, "traffic": None,
+                        "flops_per_sample": MLP_FLOPS_PER_SAMPLE, "ms": ms_net},
+           "cpu_baseline": None, "e2e": None, "gpu_launches": None, "clocks": clk.summary()}
     print(json.dumps(out))
     return 0
 
@@ -485,4 +576,6 @@ if __name__ == "__main__":
         sys.exit(main_reference(a))
     if a.workload == "reactors":
         sys.exit(main_reactors(a) if int(os.environ.get("RANK", "0")) == 0 else 0)
+    if a.workload == "surrogate":
+        sys.exit(main_surrogate(a) if int(os.environ.get("RANK", "0")) == 0 else 0)
     sys.exit(main_ours(a))

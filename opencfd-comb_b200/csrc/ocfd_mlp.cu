@@ -20,8 +20,6 @@ namespace mlp {
 constexpr int BM = 128, BK = 64, THREADS = 128;
 constexpr long long WAIT_LIMIT = 1LL << 24;  // mbarrier polls before the kernel reports a timeout
 
-
-
 __device__ __forceinline__ float gelu(float x) { return 0.5f * x * (1.0f + erff(x * 0.70710678118654752f)); }
 // d GELU / dx = Phi(x) + x phi(x)
 __device__ __forceinline__ float gelu_grad(float x) {
@@ -30,42 +28,56 @@ __device__ __forceinline__ float gelu_grad(float x) {
 
 template <int BN>
 struct GemmSmem {
-  static constexpr int A_BYTES = BM * BK * 2, B_BYTES = BN * BK * 2;
-  // padded so that at most four blocks share an SM (4 x BN <= 512 TMEM columns)
-  static constexpr int BYTES = 57344;
-  static_assert(A_BYTES + B_BYTES + 64 <= BYTES, "tile does not fit");
+  static constexpr int A_BYTES = BM * BK * 2, B_BYTES = BN * BK * 2, STAGE = A_BYTES + B_BYTES;
+  static constexpr int BYTES = 2 * STAGE + 64;  // two pipeline stages, two mbarriers, TMEM address
+  static_assert(BYTES <= 113 * 1024, "two blocks per SM");
 };
 
-// stage a rows x BK tile (rows from r0, K from k0) of a strided BF16 matrix into the K-major layout
+// stage a rows x BK tile (rows from r0, K from k0) of a strided BF16 matrix into the K-major layout;
+// 16-byte vector loads where the rows are contiguous along K and aligned, element loads otherwise
 template <int R>
 __device__ __forceinline__ void stage(uint8_t* dst, const __nv_bfloat16* src, long long sr, long long sk, int r0,
-                                      int nr, int k0, int nk) {
+                                      int nr, int k0, int nk, bool vec) {
+  // item c -> 8-row group c / 64, row (c % 8) of it, K-chunk (c / 8) % 8: eight lanes store one
+  // contiguous 128-byte row run of a chunk column (no bank conflict) and every row is read in
+  // 64-byte runs from global memory
   for (int c = threadIdx.x; c < R * (BK / 8); c += THREADS) {
-    const int r = c % R, kc = c / R;
-    const int gr = r0 + r;
-    __align__(16) __nv_bfloat16 v[8];
+    const int w = c & 63;
+    const int r = (c >> 6) * 8 + (w & 7), kc = w >> 3;
+    const int gr = r0 + r, gk0 = k0 + kc * 8;
+    uint4 val;
+    if (vec && gr < nr && gk0 + 8 <= nk) {
+      val = __ldg(reinterpret_cast<const uint4*>(src + (long long)gr * sr + gk0));
+    } else {
+      __align__(16) __nv_bfloat16 v[8];
 #pragma unroll
-    for (int j = 0; j < 8; j++) {
-      const int gk = k0 + kc * 8 + j;
-      v[j] = (gr < nr && gk < nk) ? src[(long long)gr * sr + (long long)gk * sk] : __float2bfloat16(0.0f);
+      for (int j = 0; j < 8; j++) {
+        const int gk = gk0 + j;
+        v[j] = (gr < nr && gk < nk) ? src[(long long)gr * sr + (long long)gk * sk] : __float2bfloat16(0.0f);
+      }
+      val = *reinterpret_cast<const uint4*>(v);
     }
-    *reinterpret_cast<uint4*>(dst + tc::kmajor_off(r, kc * 8, R)) = *reinterpret_cast<const uint4*>(v);
+    *reinterpret_cast<uint4*>(dst + tc::kmajor_off(r, kc * 8, R)) = val;
   }
 }
 
+// Two-stage pipeline: the tiles of K block kb + 1 are staged while the MMAs of block kb run; a
+// buffer is refilled only after the mbarrier of the MMAs that read it (two blocks earlier) fired.
 template <int BN>
 __global__ void __launch_bounds__(THREADS) k_gemm_bf16(GemmArgs g) {
+  using SM = GemmSmem<BN>;
   extern __shared__ __align__(1024) uint8_t sm[];
-  uint8_t* sA = sm;
-  uint8_t* sB = sm + GemmSmem<BN>::A_BYTES;
-  uint64_t* bar = reinterpret_cast<uint64_t*>(sB + GemmSmem<BN>::B_BYTES);
-  uint32_t* tslot = reinterpret_cast<uint32_t*>(bar + 1);
+  uint64_t* bar = reinterpret_cast<uint64_t*>(sm + 2 * SM::STAGE);  // bar[0], bar[1]
+  uint32_t* tslot = reinterpret_cast<uint32_t*>(bar + 2);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int m0 = blockIdx.x * BM, n0 = blockIdx.y * BN;
+  const bool va = g.sak == 1 && g.sam % 8 == 0 && (reinterpret_cast<uintptr_t>(g.A) & 15) == 0;
+  const bool vb = g.sbk == 1 && g.sbn % 8 == 0 && (reinterpret_cast<uintptr_t>(g.B) & 15) == 0;
 
   if (warp == 0) tc::tmem_alloc(tslot, BN);
   if (tid == 0) {
-    tc::mbar_init(bar, 1);
+    tc::mbar_init(&bar[0], 1);
+    tc::mbar_init(&bar[1], 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   tc::fence_before();
@@ -73,32 +85,34 @@ __global__ void __launch_bounds__(THREADS) k_gemm_bf16(GemmArgs g) {
   tc::fence_after();
   const uint32_t tmem = *tslot;
   constexpr uint32_t idesc = tc::idesc_bf16(BM, BN);
-  const uint32_t aaddr = tc::smem_u32(sA), baddr = tc::smem_u32(sB);
   bool ok = true;
-  uint32_t phase = 0;
   const int nkb = (g.K + BK - 1) / BK;
   for (int kb = 0; kb < nkb && ok; kb++) {
-    stage<BM>(sA, g.A, g.sam, g.sak, m0, g.M, kb * BK, g.K);
-    stage<BN>(sB, g.B, g.sbn, g.sbk, n0, g.N, kb * BK, g.K);
+    const int buf = kb & 1;
+    if (kb >= 2) ok = tc::mbar_wait(&bar[buf], (uint32_t)(((kb - 2) >> 1) & 1), WAIT_LIMIT);
+    if (!ok) break;
+    uint8_t* sA = sm + buf * SM::STAGE;
+    uint8_t* sB = sA + SM::A_BYTES;
+    stage<BM>(sA, g.A, g.sam, g.sak, m0, g.M, kb * BK, g.K, va);
+    stage<BN>(sB, g.B, g.sbn, g.sbk, n0, g.N, kb * BK, g.K, vb);
     tc::fence_proxy_async();  // generic-proxy smem writes -> visible to the tensor core
     __syncthreads();
     if (tid == 0) {
       tc::fence_after();
+      const uint32_t aaddr = tc::smem_u32(sA), baddr = tc::smem_u32(sB);
 #pragma unroll
       for (int s = 0; s < BK / 16; s++) {
         const uint64_t ad = tc::smem_desc(aaddr + s * 2 * (BM * 16), BM * 16, 128);
         const uint64_t bd = tc::smem_desc(baddr + s * 2 * (BN * 16), BN * 16, 128);
         tc::mma_bf16(tmem, ad, bd, idesc, (kb > 0 || s > 0) ? 1u : 0u);
       }
-      tc::mma_commit(tc::smem_u32(bar));
+      tc::mma_commit(tc::smem_u32(&bar[buf]));
     }
-    ok = tc::mbar_wait(bar, phase, WAIT_LIMIT);
-    phase ^= 1u;
   }
+  // the last commit covers every MMA issued before it
+  if (ok) ok = tc::mbar_wait(&bar[(nkb - 1) & 1], (uint32_t)(((nkb - 1) >> 1) & 1), WAIT_LIMIT);
   if (!ok) {
     if (lane == 0) atomicExch(g.err, 1);
-    // give the tensor core a last bounded chance to finish before the TMEM is released
-    tc::mbar_wait(bar, phase ^ 1u, WAIT_LIMIT);
   } else {
     tc::fence_after();
     const int row = m0 + 32 * warp + lane;
@@ -107,22 +121,45 @@ __global__ void __launch_bounds__(THREADS) k_gemm_bf16(GemmArgs g) {
       float v[32];
       tc::tmem_ld32(tmem + ((uint32_t)(32 * warp) << 16) + (uint32_t)c0, v);
       if (row < g.M) {
+        const bool full = n0 + c0 + 32 <= g.N;
+        // the common case (whole 32-column run inside N, bias, no accumulation, BF16 output with
+        // aligned rows): one pass, 16-byte stores
+        if (full && !g.beta && g.act != 2 && !g.C && g.Cb && (g.ldcb % 8) == 0 &&
+            (reinterpret_cast<uintptr_t>(g.Cb) & 15) == 0) {
+          const long long o = (long long)row * g.ldc + n0 + c0;
 #pragma unroll
-        for (int j = 0; j < 32; j++) {
-          const int n = n0 + c0 + j;
-          if (n >= g.N) break;
-          float val = v[j];
-          if (g.bias) val += g.bias[n];
-          const long long o = (long long)row * g.ldc + n;
-          if (g.beta) val += g.C[o];
-          if (g.act == 1) {
-            if (g.pre) g.pre[o] = val;
-            val = gelu(val);
-          } else if (g.act == 2) {
-            val *= gelu_grad(g.pre[o]);
+          for (int q = 0; q < 4; q++) {
+            __align__(16) __nv_bfloat16 pk[8];
+#pragma unroll
+            for (int j = 0; j < 8; j++) {
+              const int jj = q * 8 + j;
+              float val = v[jj] + (g.bias ? g.bias[n0 + c0 + jj] : 0.0f);
+              if (g.act == 1) {
+                if (g.pre) g.pre[o + jj] = val;
+                val = gelu(val);
+              }
+              pk[j] = __float2bfloat16(val);
+            }
+            *reinterpret_cast<uint4*>(g.Cb + (long long)row * g.ldcb + n0 + c0 + q * 8) = *reinterpret_cast<const uint4*>(pk);
           }
-          if (g.C) g.C[o] = val;
-          if (g.Cb) g.Cb[(long long)row * g.ldcb + n] = __float2bfloat16(val);
+        } else {
+#pragma unroll
+          for (int j = 0; j < 32; j++) {
+            const int n = n0 + c0 + j;
+            if (n >= g.N) break;
+            float val = v[j];
+            if (g.bias) val += g.bias[n];
+            const long long o = (long long)row * g.ldc + n;
+            if (g.beta) val += g.C[o];
+            if (g.act == 1) {
+              if (g.pre) g.pre[o] = val;
+              val = gelu(val);
+            } else if (g.act == 2) {
+              val *= gelu_grad(g.pre[o]);
+            }
+            if (g.C) g.C[o] = val;
+            if (g.Cb) g.Cb[(long long)row * g.ldcb + n] = __float2bfloat16(val);
+          }
         }
       }
     }
@@ -132,19 +169,24 @@ __global__ void __launch_bounds__(THREADS) k_gemm_bf16(GemmArgs g) {
   if (warp == 0) tc::tmem_dealloc(tmem, BN);
 }
 
-int launch_gemm(const GemmArgs& g, cudaStream_t st) {
-  constexpr int BN = 128;
+template <int BN>
+int launch_bn(const GemmArgs& g, cudaStream_t st) {
   static bool attr = false;
   if (!attr) {
-    cudaError_t e = cudaFuncSetAttribute(k_gemm_bf16<BN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         GemmSmem<BN>::BYTES);
-    if (e != cudaSuccess) return -2;
+    if (cudaFuncSetAttribute(k_gemm_bf16<BN>, cudaFuncAttributeMaxDynamicSharedMemorySize, GemmSmem<BN>::BYTES) !=
+        cudaSuccess)
+      return -2;
     attr = true;
   }
-  if (g.M <= 0 || g.N <= 0 || g.K <= 0) return 0;
   dim3 grid((g.M + BM - 1) / BM, (g.N + BN - 1) / BN);
   k_gemm_bf16<BN><<<grid, THREADS, GemmSmem<BN>::BYTES, st>>>(g);
   return cudaGetLastError() == cudaSuccess ? 0 : -2;
+}
+
+// N > 128 takes the 256-wide tile (one A staging per row block); narrower products the 128 one
+int launch_gemm(const GemmArgs& g, cudaStream_t st) {
+  if (g.M <= 0 || g.N <= 0 || g.K <= 0) return 0;
+  return g.N > 128 ? launch_bn<256>(g, st) : launch_bn<128>(g, st);
 }
 
 }  // namespace mlp
