@@ -50,6 +50,8 @@ def parse():
     ap.add_argument("--sg-train", type=int, default=1 << 21, help="surrogate workload: training reactors")
     ap.add_argument("--sg-epochs", type=int, default=20, help="surrogate workload: training epochs")
     ap.add_argument("--sg-tol", type=float, default=5.0, help="surrogate workload: gate tolerance on T (K)")
+    ap.add_argument("--surrogate", action="store_true",
+                    help="jet workload: compare FP64 chemistry with the gated surrogate (trains it first)")
     ap.add_argument("--character", action="store_true",
                     help="characteristic-space inviscid flux (IF_Scheme_Character = 1) instead of component-wise")
     ap.add_argument("--nz", type=int, default=None,
@@ -387,6 +389,75 @@ def main_surrogate(a):
     return 0
 
 
+def main_jet_surrogate(a):
+    """C5 with the gated surrogate: the surrogate is trained on 2^21 batch reactors plus cells of a
+    jet snapshot, then the jet runs K steps with FP64 chemistry and K steps with the surrogate from
+    the same start; the line reports both throughputs and the surrogate run's temperature and
+    species errors against the FP64 run."""
+    import numpy as np
+    import ctypes as C
+    from ocfd_b200 import cases, solver, surrogate
+    nz = a.nz or 256
+    case = cases.jet(nx=384, ny=256, nz=nz)
+    name = "jet-%dx%dx%d-H2air-9sp-19reac-WENO5-CD6-Wilke" % case.shape
+    sg = surrogate.Surrogate()
+    t0 = time.perf_counter()
+    # the jet's chemical change per step is orders of magnitude below the batch reactors', so the
+    # network is trained on jet states alone (two snapshots of the run) to resolve it
+    parts = [sg.flow_samples(case, 8, 1 << 20, seed=1), sg.flow_samples(case, 16, 1 << 20, seed=2)]
+    hist = sg.train_on(parts, epochs=a.sg_epochs)
+    train_s = time.perf_counter() - t0
+    L = solver.lib()
+    chk = solver._chk
+    res = {}
+    for mode in (0, 1):
+        g = solver.Solver(case)
+        g.init_state()
+        if mode == 1:
+            chk(L.ocfd_gpu_chem_mode(1, a.sg_tol))
+        dt, tt = case.dt, 0.0
+        chk(L.ocfd_gpu_run(dt, tt, a.warmup, 1, case.nsub))
+        tt += a.warmup * dt
+        with Clocks(0) as clk:
+            chk(L.ocfd_gpu_event_record(0))
+            chk(L.ocfd_gpu_run(dt, tt, a.steps, 1, case.nsub))
+            chk(L.ocfd_gpu_event_record(1))
+            ms = C.c_double()
+            chk(L.ocfd_gpu_event_elapsed(0, 1, C.byref(ms)))
+        reasons = (C.c_longlong * 5)()
+        rejected = L.ocfd_gpu_chem_surrogate_rejected(reasons) if mode == 1 else 0
+        f, di, prims = g.download_state()
+        g.close()
+        Li = 4
+        T = prims[4][Li:-Li, Li:-Li, Li:-Li]
+        dd = di[:, Li:-Li, Li:-Li, Li:-Li]
+        Y = dd / dd.sum(axis=0, keepdims=True)
+        res[mode] = dict(ms=ms.value / a.steps, T=T, Y=Y, rejected=rejected, reasons=list(reasons), clocks=clk.summary())
+    T0, T1 = res[0]["T"], res[1]["T"]
+    ncell = case.ncell
+    out = {"metric": METRIC, "value": ncell / (res[1]["ms"] * 1e-3) / 1e6, "unit": UNIT, "n_gpus": 1,
+           "steps": a.steps, "warmup": a.warmup, "ms_per_step": res[1]["ms"], "higher_is_better": True,
+           "scaling": "weak", "vs_baseline": None, "dtype": "f64 flow + bf16 gated surrogate chemistry",
+           "data": "synthetic (seeded)",
+           "config": {"workload": name + "-surrogateChem", "cells_per_gpu": ncell, "dt": case.dt,
+                      "train": "2 x 2^20 cells of jet snapshots after 8 and 16 steps, %d epochs, %.0f s" %
+                               (a.sg_epochs, train_s),
+                      "loss_first_last": [float(hist[0]), float(hist[-1])], "tol_T_K": a.sg_tol},
+           "plain_fp64": {"value": ncell / (res[0]["ms"] * 1e-3) / 1e6, "ms_per_step": res[0]["ms"]},
+           "speedup_vs_plain": res[0]["ms"] / res[1]["ms"],
+           "accuracy_vs_plain_after_steps": {
+               "steps": a.warmup + a.steps,
+               "peak_T_rel_err": float(abs(T1.max() - T0.max()) / T0.max()),
+               "T_err_max_K": float(np.abs(T1 - T0).max()),
+               "Y_err_max": float(np.abs(res[1]["Y"] - res[0]["Y"]).max())},
+           "rejected_cells_last_call": int(res[1]["rejected"]),
+           "rejection_reasons": dict(zip(["negative_Y", "T_check", "T_range", "logp_range", "logdt_range"],
+                                         res[1]["reasons"])),
+           "clocks": res[1]["clocks"], "cpu_baseline": None, "e2e": None, "gpu_launches": None}
+    print(json.dumps(out))
+    return 0
+
+
 def main_ours(a):
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -578,4 +649,6 @@ if __name__ == "__main__":
         sys.exit(main_reactors(a) if int(os.environ.get("RANK", "0")) == 0 else 0)
     if a.workload == "surrogate":
         sys.exit(main_surrogate(a) if int(os.environ.get("RANK", "0")) == 0 else 0)
+    if a.workload == "jet" and a.surrogate:
+        sys.exit(main_jet_surrogate(a) if int(os.environ.get("RANK", "0")) == 0 else 0)
     sys.exit(main_ours(a))

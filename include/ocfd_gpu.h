@@ -282,6 +282,16 @@ long long ocfd_gpu_surrogate_blob(float* host, long long nfloats, int set);
 int ocfd_gpu_surrogate_grad(int B, const float* x, const float* t, float* grads, double* loss);
 int ocfd_gpu_chem_temperature(int n, const double* d_di, const double* d_e, double* d_T);
 
+/* Chemistry of the flow solver's Strang step (ocfd_gpu_step, ocfd_gpu_run, ocfd_gpu_chem_advance):
+ * mode 0 the FP64 integrator of Chemical_time_advance (default), mode 1 the gated surrogate, whose
+ * rejected cells (|T_energy - T_pred| > tol_T, negative composition, outside the training range)
+ * take the FP64 sub-steps; the step stays one CUDA graph. Mode 1 needs a trained or loaded
+ * surrogate for this mechanism. ocfd_gpu_chem_surrogate_rejected: cells that took the FP64 path in
+ * the last chemistry call; reasons (when not NULL) gets how many failed each test: negative
+ * composition, temperature check, T / log p / log dt outside the training range. */
+int ocfd_gpu_chem_mode(int mode, double tol_T);
+long long ocfd_gpu_chem_surrogate_rejected(long long* reasons /* 5 counts or NULL */);
+
 #ifdef __cplusplus
 }
 #endif

@@ -16,6 +16,14 @@
 #include "ocfd_chem.cuh"
 #include "ocfd_device.cuh"
 #include "ocfd_flow.cuh"
+
+namespace ocfd {
+// the surrogate's flow-cell chemistry (ocfd_surrogate.cu)
+int sg_cells_chem(int ns, double* f, double* Et, double* T, double* p, double* di, double dt2, int nsub, int* nfail,
+                  cudaStream_t st);
+int sg_cells_setup(int ns, long long N, double tol);
+long long sg_cells_rejected(long long* reasons);
+}  // namespace ocfd
 #include "ocfd_launch.h"
 
 using namespace ocfd;
@@ -54,6 +62,8 @@ struct Lib {
          *T = nullptr, *p = nullptr, *Et[2] = {nullptr, nullptr}, *di = nullptr, *din = nullptr, *Rh = nullptr;
   double *ev[12] = {}, *amu = nullptr, *amk = nullptr, *amd = nullptr, *qp[3] = {}, *ci = nullptr, *se[3] = {};
   double* dus = nullptr;  // Dus of every species (Ns x N)
+  int chem_mode = 0;      // 0: FP64 integrator, 1: gated surrogate (ocfd_gpu_chem_mode)
+  int g_mode = -1;        // chemistry mode of the captured graph
   double *X = nullptr, *Y = nullptr, *Z = nullptr, *met[19] = {}, *d1[3] = {}, *edge[6] = {}, *partial = nullptr;
   double *inlet = nullptr, *upper = nullptr, *wall = nullptr, *ht_dev = nullptr;
   int *nonref = nullptr, *patches = nullptr;
@@ -453,7 +463,12 @@ void flow_advance_t(double dt1) {
 template <int NS>
 void chem_t(double dt2, int nsub) {
   KTimer t(KC_CHEM);
-  launch_chem_cells(NS, L->hc.N, L->f, L->Et[L->cur], L->T, L->p, L->di, dt2, nsub, &L->sdev->newton_fail, L->st);
+  if (L->chem_mode == 1) {
+    if (sg_cells_chem(NS, L->f, L->Et[L->cur], L->T, L->p, L->di, dt2, nsub, &L->sdev->newton_fail, L->st) != 0)
+      throw std::runtime_error("surrogate chemistry not set up for this grid and mechanism");
+  } else {
+    launch_chem_cells(NS, L->hc.N, L->f, L->Et[L->cur], L->T, L->p, L->di, dt2, nsub, &L->sdev->newton_fail, L->st);
+  }
   LAUNCH_CHECK();
 }
 
@@ -1199,7 +1214,9 @@ namespace {
 // (re)captures the Strang step as a CUDA graph when dt, the chemistry switch or the Et buffer
 // parity changed since the last capture
 void ensure_graph(double dt, int if_reaction, int nsub) {
-  if (L->gexec && L->g_dt == dt && L->g_ifr == if_reaction && L->g_nsub == nsub && L->g_par == L->cur) return;
+  if (L->gexec && L->g_dt == dt && L->g_ifr == if_reaction && L->g_nsub == nsub && L->g_par == L->cur &&
+      L->g_mode == L->chem_mode)
+    return;
   if (L->gexec) { CK(cudaGraphExecDestroy(L->gexec)); L->gexec = nullptr; }
   int cur0 = L->cur;
   long long l0 = L->launches;
@@ -1219,7 +1236,7 @@ void ensure_graph(double dt, int if_reaction, int nsub) {
   CK(cudaStreamEndCapture(L->st, &graph));
   CK(cudaGraphInstantiate(&L->gexec, graph, 0));
   CK(cudaGraphDestroy(graph));
-  L->g_dt = dt; L->g_ifr = if_reaction; L->g_nsub = nsub; L->g_par = cur0;
+  L->g_dt = dt; L->g_ifr = if_reaction; L->g_nsub = nsub; L->g_par = cur0; L->g_mode = L->chem_mode;
   L->g_launches = (int)(L->launches - l0);
   L->launches = l0;
   L->cur = cur0;  // six stages: the Et buffer parity returns to its start value
@@ -1310,6 +1327,23 @@ int ocfd_gpu_pinned_free(void* ptr) {
 }
 
 int ocfd_gpu_step_launches(void) { return L ? L->g_launches : 0; }
+
+int ocfd_gpu_chem_mode(int mode, double tol_T) {
+  return guarded([&]() -> int {
+    if (!L || !L->flow_ready) { g_err = "state not initialised"; return OCFD_ERR_STATE; }
+    if (mode != 0 && mode != 1) { g_err = "chemistry mode must be 0 (FP64) or 1 (gated surrogate)"; return OCFD_ERR_PARAM; }
+    if (mode == 1) {
+      if (!L->have_kin) { g_err = "no reaction mechanism given to ocfd_gpu_init"; return OCFD_ERR_PARAM; }
+      if (!(tol_T > 0.0)) { g_err = "tol_T must be positive"; return OCFD_ERR_PARAM; }
+      int rc = sg_cells_setup(L->NS, L->hc.N, tol_T);
+      if (rc) { g_err = "the surrogate is not trained (or loaded) for this mechanism"; return rc == -2 ? OCFD_ERR_CUDA : OCFD_ERR_STATE; }
+    }
+    L->chem_mode = mode;
+    return 0;
+  });
+}
+
+long long ocfd_gpu_chem_surrogate_rejected(long long* reasons) { return sg_cells_rejected(reasons); }
 
 int ocfd_gpu_download_state(double* f, double* di, double* prims) {
   return guarded([&]() -> int {

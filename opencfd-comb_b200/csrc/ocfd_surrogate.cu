@@ -377,7 +377,10 @@ void launch_post(int n, int mode, double* di, double* e, const double* T0, const
   }
 
 // column statistics of a raw n x PAD FP32 array (host reduction of per-block partials)
-int column_stats(int n, const float* raw, double* mean, double* sd, double* mn, double* mx, cudaStream_t st) {
+// sd_floor replaces the standard deviation of a column that does not vary (above the rounding of
+// the variance): 1 for inputs, so that a constant input maps to 0
+int column_stats(int n, const float* raw, double* mean, double* sd, double* mn, double* mx, double sd_floor,
+                 cudaStream_t st) {
   const int blocks = 592;
   double* part = nullptr;
   if (cudaMalloc(&part, sizeof(double) * blocks * 4 * PAD)) return -2;
@@ -396,16 +399,216 @@ int column_stats(int n, const float* raw, double* mean, double* sd, double* mn, 
     }
     mean[c] = s1 / n;
     const double var = std::max(s2 / n - mean[c] * mean[c], 0.0);
-    sd[c] = var > 1e-30 ? std::sqrt(var) : 1.0;
+    // a column varies when its variance stands above the rounding of s2 / n - mean^2
+    const bool varies = var > 1e-20 * mean[c] * mean[c] && var > 1e-60;
+    sd[c] = varies ? std::sqrt(var) : sd_floor;
     mn[c] = a;
     mx[c] = b;
   }
   return 0;
 }
 
-}  // namespace sg
-}  // namespace ocfd
 
+// ---------------------------------------------------------------- flow cells (Chemical_time_advance)
+// the surrogate inside the Strang step: cells are read in place from the halo arrays, the gate
+// decides per cell, rejected cells go to a device list that k_chem_cells_list advances with the
+// FP64 sub-steps of the plain path; no host synchronisation, so the step stays one CUDA graph
+template <int NS>
+__global__ void k_cell_inputs(int c0, int rows, const double* __restrict__ di, const double* __restrict__ Et,
+                              double dtc, const Norm* __restrict__ nm, int nin, float* __restrict__ raw,
+                              double* __restrict__ T0, __nv_bfloat16* __restrict__ xb, int* nfail) {
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= rows) return;
+  const int t = c0 + r;
+  const int i = t % cC.nx + 1, j = (t / cC.nx) % cC.ny + 1, k = t / cC.nx / cC.ny + 1;
+  const int q = hidx(i, j, k);
+  double d[NS], rho = 0.0;
+#pragma unroll
+  for (int m = 0; m < NS; m++) {
+    d[m] = di[(size_t)m * cC.H + q];
+    rho += d[m];
+  }
+  const double T = dev_T<NS>(d, Et[q], nfail);
+  const double p = dev_P<NS>(d, T);
+  float v[PAD];
+  v[0] = (float)T;
+  v[1] = (float)log(p);
+#pragma unroll
+  for (int m = 0; m < NS; m++) v[2 + m] = (float)(d[m] / rho);
+  v[2 + NS] = (float)log(dtc);
+  for (int c = NS + 3; c < PAD; c++) v[c] = 0.0f;
+  float* o = raw + (size_t)r * PAD;
+#pragma unroll
+  for (int c = 0; c < PAD; c++) {
+    o[c] = v[c];
+    xb[(size_t)r * PAD + c] = __float2bfloat16(c < nin ? (v[c] - nm->in_mean[c]) / nm->in_std[c] : 0.0f);
+  }
+  T0[r] = T;
+}
+template <int NS>
+__global__ void k_cell_post(int c0, int rows, double* __restrict__ f, double* __restrict__ Et, double* __restrict__ Tf,
+                            double* __restrict__ pf, double* __restrict__ di, const double* __restrict__ T0,
+                            const float* __restrict__ raw, const float* __restrict__ out, const Norm* __restrict__ nm,
+                            const double* __restrict__ proj, double tol_T, int* __restrict__ list,
+                            int* __restrict__ count, int* nfail) {
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= rows) return;
+  const int t = c0 + r;
+  const int i = t % cC.nx + 1, j = (t / cC.nx) % cC.ny + 1, k = t / cC.nx / cC.ny + 1;
+  const int q = hidx(i, j, k);
+  double d0[NS], rho = 0.0, dy[NS], d1[NS];
+#pragma unroll
+  for (int m = 0; m < NS; m++) {
+    d0[m] = di[(size_t)m * cC.H + q];
+    rho += d0[m];
+  }
+  const float* o = out + (size_t)r * PAD;
+#pragma unroll
+  for (int m = 0; m < NS; m++) dy[m] = (double)o[m] * nm->out_std[m] + nm->out_mean[m];
+  const double dTp = (double)o[NS] * nm->out_std[NS] + nm->out_mean[NS];
+  // rejection reasons, counted in count[2..6]: negative composition, temperature check, T, log p and
+  // log dt outside the training range
+  int why = 0;
+#pragma unroll
+  for (int a = 0; a < NS; a++) {
+    double sacc = 0.0;
+#pragma unroll
+    for (int b = 0; b < NS; b++) sacc += proj[a * NS + b] * dy[b];
+    const double y1 = d0[a] / rho + sacc;
+    // the flow path tolerates larger dips: Rescaling_di clips negative densities at the next stage
+    if (y1 < -1.0e-4) why |= 1;
+    d1[a] = y1 * rho;
+  }
+  const double e0 = Et[q];
+  const double e1 = update_et<NS>(d0, d1, e0);
+  const double T1 = dev_T<NS>(d1, e1, nfail);
+  if (!(fabs(T1 - T0[r] - dTp) <= tol_T)) why |= 2;
+  const float* ri = raw + (size_t)r * PAD;
+  const int chk[3] = {0, 1, NS + 2};
+#pragma unroll
+  for (int qq = 0; qq < 3; qq++) {
+    const int c = chk[qq];
+    if (!(ri[c] >= nm->in_min[c] && ri[c] <= nm->in_max[c])) why |= 4 << qq;
+  }
+  if (why) {
+    list[atomicAdd(count, 1)] = t;
+#pragma unroll
+    for (int b = 0; b < 5; b++)
+      if (why >> b & 1) atomicAdd(count + 2 + b, 1);
+    return;
+  }
+#pragma unroll
+  for (int m = 0; m < NS; m++) di[(size_t)m * cC.H + q] = d1[m];
+  Et[q] = e1;
+  f[4 * cC.N + t] = f[4 * cC.N + t] + (e1 - e0);
+  Tf[q] = T1;
+  pf[q] = dev_P<NS>(d1, T1);
+}
+// Chemical_time_advance + comput_T_P for the listed cells (k_chem_cells on a cell list whose length
+// is read on the device)
+template <int NS>
+__global__ void __launch_bounds__(128) k_chem_cells_list(const int* __restrict__ list, const int* __restrict__ count,
+                                                         double* f, double* Et, double* T, double* p, double* di,
+                                                         double dt2, int nsub, int* nfail) {
+  const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= *count) return;
+  const int t = list[idx];
+  const int i = t % cC.nx + 1, j = (t / cC.nx) % cC.ny + 1, k = t / cC.nx / cC.ny + 1;
+  const int q = hidx(i, j, k);
+  double d1[NS];
+#pragma unroll
+  for (int m = 0; m < NS; m++) d1[m] = di[(size_t)m * cC.H + q];
+  double e = Et[q];
+  double f5 = f[4 * cC.N + t];
+  for (int s = 0; s < nsub; s++) {
+    double e0 = e;
+    chem_step<NS>(d1, e, dt2, nfail);
+    f5 = f5 + (e - e0);
+  }
+#pragma unroll
+  for (int m = 0; m < NS; m++) di[(size_t)m * cC.H + q] = d1[m];
+  Et[q] = e;
+  f[4 * cC.N + t] = f5;
+  double TT = dev_T<NS>(d1, e, nfail);
+  T[q] = TT;
+  p[q] = dev_P<NS>(d1, TT);
+}
+
+struct Cells {
+  long long N = 0;
+  int chunk = 0;
+  float* raw = nullptr;
+  double* T0 = nullptr;
+  __nv_bfloat16 *xb = nullptr, *hA = nullptr, *hB = nullptr;
+  float* out = nullptr;
+  int* list = nullptr;
+  int* count = nullptr;  // [0] rejected cells of the current call, [1] their total since set-up
+  double tol = 5.0;
+};
+Cells CS;
+
+template <int NS>
+void cells_chem_t(double* f, double* Et, double* T, double* p, double* di, double dt2, int nsub, int* nfail,
+                  cudaStream_t st) {
+  const long long N = CS.N;
+  cudaMemsetAsync(CS.count, 0, 8 * sizeof(int), st);
+  Gemm gemm;
+  __nv_bfloat16* hs[3] = {CS.hA, CS.hB, CS.hA};
+  for (long long c0 = 0; c0 < N; c0 += CS.chunk) {
+    const int rows = (int)std::min<long long>(CS.chunk, N - c0);
+    k_cell_inputs<NS><<<nb(rows, 128), 128, 0, st>>>((int)c0, rows, di, Et, dt2 * nsub, S.d_norm, S.nin, CS.raw,
+                                                    CS.T0, CS.xb, nfail);
+    forward(gemm, rows, CS.xb, hs, nullptr, CS.out, st);
+    k_cell_post<NS><<<nb(rows, 128), 128, 0, st>>>((int)c0, rows, f, Et, T, p, di, CS.T0, CS.raw, CS.out, S.d_norm,
+                                                  S.d_proj, CS.tol, CS.list, CS.count, nfail);
+  }
+  k_chem_cells_list<NS><<<nb(N, 128), 128, 0, st>>>(CS.list, CS.count, f, Et, T, p, di, dt2, nsub, nfail);
+}
+
+// mode 1: allocate the chunk buffers for N cells (called outside any stream capture)
+int cells_setup(long long N, double tol) {
+  if (!S.trained) return -5;
+  if (CS.N != N) {
+    void* ptrs[] = {CS.raw, CS.T0, CS.xb, CS.hA, CS.hB, CS.out, CS.list, CS.count};
+    for (void* q : ptrs)
+      if (q) cudaFree(q);
+    CS = Cells{};
+    CS.N = N;
+    CS.chunk = (int)std::min<long long>(N, 1 << 20);
+    const size_t ch = CS.chunk;
+    if (cudaMalloc(&CS.raw, ch * PAD * 4) || cudaMalloc(&CS.T0, ch * 8) || cudaMalloc(&CS.xb, ch * PAD * 2) ||
+        cudaMalloc(&CS.hA, ch * HID * 2) || cudaMalloc(&CS.hB, ch * HID * 2) || cudaMalloc(&CS.out, ch * PAD * 4) ||
+        cudaMalloc(&CS.list, (size_t)N * 4) || cudaMalloc(&CS.count, 64))
+      return -2;
+  }
+  CS.tol = tol;
+  return 0;
+}
+
+}  // namespace sg
+
+// the flow solver's chemistry through the gated surrogate (ocfd_gpu.cu, chemistry mode 1)
+int sg_cells_chem(int ns, double* f, double* Et, double* T, double* p, double* di, double dt2, int nsub, int* nfail,
+                  cudaStream_t st) {
+  using namespace sg;
+  if (!S.trained || S.ns != ns || CS.N <= 0) return -5;
+  SG_DISPATCH(ns, cells_chem_t<NSC>(f, Et, T, p, di, dt2, nsub, nfail, st));
+  return 0;
+}
+int sg_cells_setup(int ns, long long N, double tol) {
+  using namespace sg;
+  if (!S.trained || S.ns != ns) return -5;
+  return cells_setup(N, tol);
+}
+long long sg_cells_rejected(long long* reasons) {
+  using namespace sg;
+  int h[8] = {};
+  if (CS.count) cudaMemcpy(h, CS.count, sizeof(h), cudaMemcpyDeviceToHost);
+  if (reasons)
+    for (int b = 0; b < 5; b++) reasons[b] = h[2 + b];
+  return h[0];
+}
+}  // namespace ocfd
 
 // ---------------------------------------------------------------- C ABI
 namespace {
@@ -556,21 +759,29 @@ int ocfd_gpu_surrogate_train(int n, const double* d_di0, const double* d_e0, con
   SG_DISPATCH(ns, launch_raw_inputs<NSC>(n, d_di0, d_e0, d_dt, raw_in, T0, nf, st));
   SG_DISPATCH(ns, launch_raw_targets<NSC>(n, d_di0, d_di1, d_e1, T0, raw_out, nf, st));
   double mean[PAD], sd[PAD], mn[PAD], mx[PAD];
-  if ((rc = column_stats(n, raw_in, mean, sd, mn, mx, st))) return rc;
+  if ((rc = column_stats(n, raw_in, mean, sd, mn, mx, 1.0, st))) return rc;
   for (int c = 0; c < PAD; c++) {
     S.norm.in_mean[c] = (float)mean[c];
     S.norm.in_std[c] = (float)sd[c];
     S.norm.in_min[c] = (float)mn[c];
     S.norm.in_max[c] = (float)mx[c];
   }
-  if ((rc = column_stats(n, raw_out, mean, sd, mn, mx, st))) return rc;
+  // outputs whose spread is below the FP64 rounding noise of the state (std < 1e-15, e.g. an inert
+  // species) are inactive: trained against 0 and applied as their mean (stored scale 0)
+  if ((rc = column_stats(n, raw_out, mean, sd, mn, mx, 0.0, st))) return rc;
+  float out_train_std[PAD];
   for (int c = 0; c < PAD; c++) {
+    const bool active = sd[c] > 1e-15;
     S.norm.out_mean[c] = (float)mean[c];
-    S.norm.out_std[c] = (float)sd[c];
+    S.norm.out_std[c] = active ? (float)sd[c] : 0.0f;
+    out_train_std[c] = active ? (float)sd[c] : 1.0f;
   }
+  float* d_tstd = dalloc<float>(PAD, fr.v);
+  if (!d_tstd) return -2;
+  cudaMemcpyAsync(d_tstd, out_train_std, sizeof(out_train_std), cudaMemcpyHostToDevice, st);
   cudaMemcpyAsync(S.d_norm, &S.norm, sizeof(Norm), cudaMemcpyHostToDevice, st);
   k_normalize<<<nb((long long)n * PAD, 256), 256, 0, st>>>(n, S.nin, raw_in, norm_field(0), norm_field(1), X, nullptr);
-  k_normalize<<<nb((long long)n * PAD, 256), 256, 0, st>>>(n, S.nout, raw_out, norm_field(2), norm_field(3), nullptr, Tt);
+  k_normalize<<<nb((long long)n * PAD, 256), 256, 0, st>>>(n, S.nout, raw_out, norm_field(2), d_tstd, nullptr, Tt);
 
   Gemm gemm;
   const float b1 = 0.9f, b2 = 0.999f, eps = 1e-8f;

@@ -152,4 +152,6 @@ GPU_SIGNATURES = {
     "ocfd_gpu_surrogate_blob": (C.c_longlong, [C.POINTER(C.c_float), C.c_longlong, I]),
     "ocfd_gpu_surrogate_grad": (I, [I, C.POINTER(C.c_float), C.POINTER(C.c_float), C.POINTER(C.c_float), PD]),
     "ocfd_gpu_chem_temperature": (I, [I, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "ocfd_gpu_chem_mode": (I, [I, D]),
+    "ocfd_gpu_chem_surrogate_rejected": (C.c_longlong, [C.POINTER(C.c_longlong)]),
 }

@@ -84,6 +84,45 @@ class Surrogate:
                                                     lr, seed, abi.dptr(hist)))
         return hist
 
+    def flow_samples(self, case, nsteps, n_sample, seed=0):
+        """Cell states of a reacting flow after nsteps FP64 steps (a snapshot of the run), as
+        reactors with the step's chemistry time and sub-step count."""
+        g = solver.Solver(case)
+        g.init_state()
+        for s in range(nsteps):
+            g.tt = s * case.dt
+            g.step(case.dt, 1, case.nsub)
+        f, di, prims = g.download_state()
+        g.close()
+        L4 = 4
+        dii = di[:, L4:-L4, L4:-L4, L4:-L4].reshape(self.ns, -1).T
+        E = prims[6][L4:-L4, L4:-L4, L4:-L4].reshape(-1)
+        rng = np.random.default_rng(seed)
+        idx = rng.choice(len(E), size=min(n_sample, len(E)), replace=False)
+        n = len(idx)
+        return (np.ascontiguousarray(dii[idx]), np.ascontiguousarray(E[idx]), np.full(n, case.dt),
+                np.full(n, case.nsub, dtype=np.int32))
+
+    def train_on(self, parts, epochs=20, batch=1024, lr=2e-3, seed=0):
+        """Trains on the concatenation of (di, E, dt, nsub) reactor sets, targets from the FP64
+        integrator."""
+        t = self.torch
+        di = np.concatenate([p[0] for p in parts])
+        E = np.concatenate([p[1] for p in parts])
+        dt = np.concatenate([p[2] for p in parts])
+        nsub = np.concatenate([p[3] for p in parts]).astype(np.int32)
+        n = (len(E) // batch) * batch
+        di, E, dt, nsub = di[:n], E[:n], dt[:n], nsub[:n]
+        solver.chem_setup(self.th, self.kin, 1, abi.CHEM_IMPLICIT)
+        d_di0, d_e0, d_dt = _dev(t, di), _dev(t, E), _dev(t, dt)
+        d_di1, d_e1 = self.fp64(di, E, dt, nsub)
+        hist = np.zeros(epochs)
+        P = np.ascontiguousarray(self.proj)
+        solver._chk(self.L.ocfd_gpu_surrogate_train(n, d_di0.data_ptr(), d_e0.data_ptr(), d_dt.data_ptr(),
+                                                    d_di1.data_ptr(), d_e1.data_ptr(), abi.dptr(P), epochs, batch,
+                                                    lr, seed, abi.dptr(hist)))
+        return hist
+
     def evaluate(self, n=1 << 16, seed=12345, tol_T=5.0):
         """Held-out reactors: errors of the ungated network and of the gated surrogate against the
         FP64 integrator, the fallback fraction and the element-conservation residual."""

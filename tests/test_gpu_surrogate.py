@@ -79,3 +79,44 @@ def test_blob_roundtrip(trained):
     b = sg.blob()
     sg.load(b)
     assert np.array_equal(sg.blob(), b)
+
+
+def _jet_run(sg, mode, tol, steps=2):
+    from ocfd_b200 import cases, solver
+    c = cases.jet(nx=24, ny=16, nz=16)
+    g = solver.Solver(c)
+    g.init_state()
+    if mode:
+        assert sg.L.ocfd_gpu_chem_mode(1, tol) == 0
+    for s in range(steps):
+        g.tt = s * c.dt
+        g.step(c.dt, 1, c.nsub)
+    st = g.download_state()
+    rej = sg.L.ocfd_gpu_chem_surrogate_rejected(None) if mode else 0
+    g.close()
+    return st, rej
+
+
+def test_flow_surrogate_rejecting_every_cell_is_the_fp64_path(trained):
+    """With a gate that accepts nothing, every cell takes the FP64 sub-steps of the list kernel,
+    which must reproduce the plain chemistry of the Strang step bit for bit."""
+    sg, _ = trained
+    (f0, di0, p0), _ = _jet_run(sg, 0, 1.0)
+    (f1, di1, p1), rej = _jet_run(sg, 1, 1e-300)
+    assert rej == 24 * 16 * 16
+    L = 4
+    assert np.array_equal(f0, f1)
+    assert np.array_equal(di0[:, L:-L, L:-L, L:-L], di1[:, L:-L, L:-L, L:-L])
+    assert np.array_equal(p0[:, L:-L, L:-L, L:-L], p1[:, L:-L, L:-L, L:-L])
+
+
+def test_flow_surrogate_close_to_fp64(trained):
+    sg, _ = trained
+    (f0, di0, p0), _ = _jet_run(sg, 0, 1.0)
+    (f1, di1, p1), rej = _jet_run(sg, 1, 5.0)
+    L = 4
+    T0, T1 = p0[4][L:-L, L:-L, L:-L], p1[4][L:-L, L:-L, L:-L]
+    assert np.abs(T1 - T0).max() <= 0.01 * T0.max()
+    Y0 = di0[:, L:-L, L:-L, L:-L] / di0[:, L:-L, L:-L, L:-L].sum(axis=0)
+    Y1 = di1[:, L:-L, L:-L, L:-L] / di1[:, L:-L, L:-L, L:-L].sum(axis=0)
+    assert np.abs(Y1 - Y0).max() <= 1e-3
