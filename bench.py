@@ -370,7 +370,8 @@ def main_surrogate(a):
         with open(peaks_file) as fh:
             pk = json.load(fh)
         bf16_peak = pk.get("bf16_tflops")
-    net_tflops = n * MLP_FLOPS_PER_SAMPLE / (ms_net * 1e-3) / 1e12
+    # network throughput bound from below by the whole gated pass (features, 4 GEMMs, gate, fallback)
+    net_tflops = n * MLP_FLOPS_PER_SAMPLE / (ms_gated * 1e-3) / 1e12
     out = {"metric": SMETRIC, "value": n / (ms_gated * 1e-3) / 1e6, "unit": RUNIT, "n_gpus": 1, "steps": k,
            "warmup": a.warmup, "ms_per_step": ms_gated, "higher_is_better": True, "scaling": "weak",
            "vs_baseline": None, "dtype": "bf16 network + f64 fallback", "data": "synthetic (seeded)",
@@ -380,10 +381,11 @@ def main_surrogate(a):
            "plain_fp64": {"value": n / (ms_plain * 1e-3) / 1e6, "ms": ms_plain},
            "speedup_vs_plain": ms_plain / ms_gated,
            "accuracy": acc, "fallback_fraction": nfb.value / n,
-           "roofline": {"bound": "tensor", "kernel": "network pass (4 tcgen05 GEMMs + features + gate)",
+           "roofline": {"bound": "tensor", "kernel": "gated pass (features, 4 tcgen05 GEMMs, gate, fallback)",
                         "achieved": net_tflops, "peak": bf16_peak, "unit": "TFLOP/s",
                         "frac": (net_tflops / bf16_peak) if bf16_peak else None, "traffic": None,
-                        "flops_per_sample": MLP_FLOPS_PER_SAMPLE, "ms": ms_net},
+                        "flops_per_sample": MLP_FLOPS_PER_SAMPLE, "ms": ms_gated,
+                        "ungated_predict_ms": ms_net},
            "cpu_baseline": None, "e2e": None, "gpu_launches": None, "clocks": clk.summary()}
     print(json.dumps(out))
     return 0

@@ -33,31 +33,57 @@ struct GemmSmem {
   static_assert(BYTES <= 113 * 1024, "two blocks per SM");
 };
 
-// stage a rows x BK tile (rows from r0, K from k0) of a strided BF16 matrix into the K-major layout;
-// 16-byte vector loads where the rows are contiguous along K and aligned, element loads otherwise
+// stage a rows x BK tile (rows from r0, K from k0) of a strided BF16 matrix into the K-major layout.
+// Item c -> 8-row group c / 64, row (c % 8) of it, K-chunk (c / 8) % 8: eight lanes store one
+// contiguous 128-byte row run of a chunk column (no bank conflict) and every row is read in 64-byte
+// runs from global memory. With rows contiguous along K and aligned, a thread first issues all of
+// its 16-byte loads, then stores them, so the loads of the whole tile are in flight together.
 template <int R>
 __device__ __forceinline__ void stage(uint8_t* dst, const __nv_bfloat16* src, long long sr, long long sk, int r0,
                                       int nr, int k0, int nk, bool vec) {
-  // item c -> 8-row group c / 64, row (c % 8) of it, K-chunk (c / 8) % 8: eight lanes store one
-  // contiguous 128-byte row run of a chunk column (no bank conflict) and every row is read in
-  // 64-byte runs from global memory
-  for (int c = threadIdx.x; c < R * (BK / 8); c += THREADS) {
-    const int w = c & 63;
-    const int r = (c >> 6) * 8 + (w & 7), kc = w >> 3;
-    const int gr = r0 + r, gk0 = k0 + kc * 8;
-    uint4 val;
-    if (vec && gr < nr && gk0 + 8 <= nk) {
-      val = __ldg(reinterpret_cast<const uint4*>(src + (long long)gr * sr + gk0));
-    } else {
-      __align__(16) __nv_bfloat16 v[8];
+  constexpr int PER = R * (BK / 8) / THREADS;  // 16-byte chunks per thread
+  auto item = [&](int it, int& r, int& kc) {
+    const int c = threadIdx.x + it * THREADS, w = c & 63;
+    r = (c >> 6) * 8 + (w & 7);
+    kc = w >> 3;
+  };
+  if (vec) {
+    uint4 v[PER];
+#pragma unroll
+    for (int it = 0; it < PER; it++) {
+      int r, kc;
+      item(it, r, kc);
+      const int gr = r0 + r, gk0 = k0 + kc * 8;
+      if (gr < nr && gk0 + 8 <= nk) {
+        v[it] = __ldg(reinterpret_cast<const uint4*>(src + (long long)gr * sr + gk0));
+      } else {
+        __align__(16) __nv_bfloat16 e[8];
+#pragma unroll
+        for (int j = 0; j < 8; j++)
+          e[j] = (gr < nr && gk0 + j < nk) ? src[(long long)gr * sr + gk0 + j] : __float2bfloat16(0.0f);
+        v[it] = *reinterpret_cast<const uint4*>(e);
+      }
+    }
+#pragma unroll
+    for (int it = 0; it < PER; it++) {
+      int r, kc;
+      item(it, r, kc);
+      *reinterpret_cast<uint4*>(dst + tc::kmajor_off(r, kc * 8, R)) = v[it];
+    }
+  } else {
+#pragma unroll 1
+    for (int it = 0; it < PER; it++) {
+      int r, kc;
+      item(it, r, kc);
+      const int gr = r0 + r, gk0 = k0 + kc * 8;
+      __align__(16) __nv_bfloat16 e[8];
 #pragma unroll
       for (int j = 0; j < 8; j++) {
         const int gk = gk0 + j;
-        v[j] = (gr < nr && gk < nk) ? src[(long long)gr * sr + (long long)gk * sk] : __float2bfloat16(0.0f);
+        e[j] = (gr < nr && gk < nk) ? src[(long long)gr * sr + (long long)gk * sk] : __float2bfloat16(0.0f);
       }
-      val = *reinterpret_cast<const uint4*>(v);
+      *reinterpret_cast<uint4*>(dst + tc::kmajor_off(r, kc * 8, R)) = *reinterpret_cast<const uint4*>(e);
     }
-    *reinterpret_cast<uint4*>(dst + tc::kmajor_off(r, kc * 8, R)) = val;
   }
 }
 

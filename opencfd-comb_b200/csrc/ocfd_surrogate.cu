@@ -174,13 +174,20 @@ __global__ void k_loss_grad(int B, int nout, const float* __restrict__ out, cons
   gf[t] = g;
   gb[t] = __float2bfloat16(g);
 }
-// bias gradient: column sums of an FP32 B x ncol matrix
+// bias gradient: column sums of an FP32 B x ncol matrix; block = one column, threads over rows
 __global__ void k_colsum(int B, int ncol, const float* __restrict__ g, float* __restrict__ out) {
-  const int c = blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= ncol) return;
+  __shared__ float red[8];
+  const int c = blockIdx.x;
   float s = 0.0f;
-  for (int r = 0; r < B; r++) s += g[(size_t)r * ncol + c];
-  out[c] = s;
+  for (int r = threadIdx.x; r < B; r += blockDim.x) s += g[(size_t)r * ncol + c];
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    float t = 0.0f;
+    for (int w = 0; w < (int)(blockDim.x >> 5); w++) t += red[w];
+    out[c] = t;
+  }
 }
 // Adam step on FP32 master parameters, refreshing the BF16 copy
 __global__ void k_adam(long long n, float* __restrict__ p, const float* __restrict__ g, float* __restrict__ m,
@@ -658,17 +665,26 @@ int run_surrogate(int n, int mode, double* di, double* e, const double* dt, cons
                   double* eo, double* Tp, double* Te, int* n_fallback) {
   if (!S.trained) return -5;
   cudaStream_t st = current_stream();
-  const int CH = 1 << 16;
-  Freer fr;
-  float* raw = dalloc<float>((size_t)CH * PAD, fr.v);
-  double* T0 = dalloc<double>(CH, fr.v);
-  __nv_bfloat16* xb = dalloc<__nv_bfloat16>((size_t)CH * PAD, fr.v);
-  __nv_bfloat16* hA = dalloc<__nv_bfloat16>((size_t)CH * HID, fr.v);
-  __nv_bfloat16* hB = dalloc<__nv_bfloat16>((size_t)CH * HID, fr.v);
-  float* out = dalloc<float>((size_t)CH * PAD, fr.v);
-  int* fb = dalloc<int>((size_t)std::max(n, 1), fr.v);
-  int* cnt = dalloc<int>(64, fr.v);  // [0] fallback count, [1] nfail, [32..] work-queue counter + nfail
-  if (!raw || !T0 || !xb || !hA || !hB || !out || !fb || !cnt) return -2;
+  // scratch kept between calls (grown when a larger batch arrives), so no call allocates twice
+  static const int CH = 1 << 18;
+  static float* raw = nullptr;
+  static double* T0 = nullptr;
+  static __nv_bfloat16 *xb = nullptr, *hA = nullptr, *hB = nullptr;
+  static float* out = nullptr;
+  static int* fb = nullptr;
+  static int* cnt = nullptr;  // [0] fallback count, [1] nfail, [32..] work-queue counter + nfail
+  static int fb_cap = 0;
+  if (!raw) {
+    if (cudaMalloc(&raw, (size_t)CH * PAD * 4) || cudaMalloc(&T0, (size_t)CH * 8) ||
+        cudaMalloc(&xb, (size_t)CH * PAD * 2) || cudaMalloc(&hA, (size_t)CH * HID * 2) ||
+        cudaMalloc(&hB, (size_t)CH * HID * 2) || cudaMalloc(&out, (size_t)CH * PAD * 4) || cudaMalloc(&cnt, 256))
+      return -2;
+  }
+  if (n > fb_cap) {
+    if (fb) cudaFree(fb);
+    if (cudaMalloc(&fb, (size_t)n * 4)) { fb = nullptr; fb_cap = 0; return -2; }
+    fb_cap = n;
+  }
   cudaMemsetAsync(cnt, 0, 64 * sizeof(int), st);
   cudaMemsetAsync(S.d_err, 0, sizeof(int), st);
   Gemm gemm;
@@ -802,14 +818,14 @@ int ocfd_gpu_surrogate_train(int n, const double* d_di0, const double* d_e0, con
       k_loss_grad<<<nb((long long)B * PAD, 256), 256, 0, st>>>(B, S.nout, out, t, gf, gbf, dloss);
       // output layer
       gemm(gbf, 1, PAD, h[2], 1, HID, PAD, HID, B, gW[3], HID, nullptr, 0, nullptr, nullptr, 0, 0, st);
-      k_colsum<<<1, PAD, 0, st>>>(B, PAD, gf, gB[3]);
+      k_colsum<<<PAD, 256, 0, st>>>(B, PAD, gf, gB[3]);
       gemm(gbf, PAD, 1, S.wb[3], 1, HID, B, HID, PAD, dzf, HID, dzb[0], HID, pre[2], nullptr, 0, 2, st);
       int cur = 0;
       for (int l = 2; l >= 0; l--) {
         const __nv_bfloat16* hin = l > 0 ? h[l - 1] : x;
         const int Kin = S.cols[l];
         gemm(dzb[cur], 1, HID, hin, 1, Kin, HID, Kin, B, gW[l], Kin, nullptr, 0, nullptr, nullptr, 0, 0, st);
-        k_colsum<<<nb(HID, 128), 128, 0, st>>>(B, HID, dzf, gB[l]);
+        k_colsum<<<HID, 256, 0, st>>>(B, HID, dzf, gB[l]);
         if (l > 0) {
           gemm(dzb[cur], HID, 1, S.wb[l], 1, Kin, B, Kin, HID, dzf, HID, dzb[1 - cur], HID, pre[l - 1], nullptr, 0, 2,
                st);
@@ -938,14 +954,14 @@ int ocfd_gpu_surrogate_grad(int B, const float* x, const float* t, float* grads,
   forward(gemm, B, xd, h, pre, out, st);
   k_loss_grad<<<nb((long long)B * PAD, 256), 256, 0, st>>>(B, S.nout, out, td, gf, gbf, dloss);
   gemm(gbf, 1, PAD, h[2], 1, HID, PAD, HID, B, gW[3], HID, nullptr, 0, nullptr, nullptr, 0, 0, st);
-  k_colsum<<<1, PAD, 0, st>>>(B, PAD, gf, gB[3]);
+  k_colsum<<<PAD, 256, 0, st>>>(B, PAD, gf, gB[3]);
   gemm(gbf, PAD, 1, S.wb[3], 1, HID, B, HID, PAD, dzf, HID, dzb[0], HID, pre[2], nullptr, 0, 2, st);
   int cur = 0;
   for (int l = 2; l >= 0; l--) {
     const __nv_bfloat16* hin = l > 0 ? h[l - 1] : xd;
     const int Kin = S.cols[l];
     gemm(dzb[cur], 1, HID, hin, 1, Kin, HID, Kin, B, gW[l], Kin, nullptr, 0, nullptr, nullptr, 0, 0, st);
-    k_colsum<<<nb(HID, 128), 128, 0, st>>>(B, HID, dzf, gB[l]);
+    k_colsum<<<HID, 256, 0, st>>>(B, HID, dzf, gB[l]);
     if (l > 0) {
       gemm(dzb[cur], HID, 1, S.wb[l], 1, Kin, B, Kin, HID, dzf, HID, dzb[1 - cur], HID, pre[l - 1], nullptr, 0, 2, st);
       cur = 1 - cur;
