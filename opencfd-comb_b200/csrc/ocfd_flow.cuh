@@ -269,35 +269,50 @@ __global__ void __launch_bounds__(FLUX_THREADS, Tile<DIR>::MINB) k_flux(FluxArgs
   // phase 2: numerical fluxes at interfaces s0-1 .. s0-1+ncell
   const int nq = HYB ? *sqn : 0;
   const int nfast = NCS * NI;
-  for (int idx = threadIdx.x; idx < nfast + NCS * nq; idx += FLUX_THREADS) {
-    int cs, it, scm = 0;
-    if (!HYB || idx < nfast) {
-      cs = idx / NI;
-      it = idx - cs * NI;
-    } else {
-      const int r = idx - nfast, nqd = HYB ? nq : 1;  // this branch runs only for HYBRID
-      cs = r / nqd;
-      const int e = squeue[r - cs * nqd];
-      it = e & 0xffff;
-      scm = e >> 16;
-    }
-    int t, l;
+  auto decode = [&](int it, int& t, int& l) {
     if (DIR == 0) { t = it % (C + 1); l = it / (C + 1); }
     else { l = it % NL; t = it / NL; }
-    if (idx < nfast) {
-      if (l0 + l > nl_max || t > ncell) continue;
-      if (HYB && !sfast[it]) continue;
-    }
+  };
+  // one (component, sign, interface) item; false when the item is not this pass's work
+  auto item_flux = [&](int idx, double& h, int& dst) -> bool {
+    const int cs = idx / NI, it = idx - cs * NI;
+    int t, l;
+    decode(it, t, l);
+    if (l0 + l > nl_max || t > ncell) return false;
+    if (HYB && !sfast[it]) return false;
     const double* v = sf + sidx(cs, t + 3, l);
     const bool plus = cs < NC;
-    double h;
-    if (HYB && idx < nfast) {
+    if (HYB) {
       h = ud7l_signed<VS>(v, plus);
     } else {
       const int ig = s0 - 1 + t;  // reference interface index hh(ig), between cells ig and ig+1
-      h = plus ? interface_flux<SCHEME, true, VS>(v, ig, n, DIR, scm) : interface_flux<SCHEME, false, VS>(v, ig, n, DIR, scm);
+      h = plus ? interface_flux<SCHEME, true, VS>(v, ig, n, DIR, 0) : interface_flux<SCHEME, false, VS>(v, ig, n, DIR, 0);
     }
-    sh[cs * NI + it] = h;
+    dst = cs * NI + it;
+    return true;
+  };
+  // two independent items per iteration, so that their dependent FP64 chains overlap
+  for (int idx = threadIdx.x; idx < nfast; idx += 2 * FLUX_THREADS) {
+    double ha = 0.0, hb = 0.0;
+    int da = 0, db = 0;
+    const bool oa = item_flux(idx, ha, da);
+    const bool ob = idx + FLUX_THREADS < nfast && item_flux(idx + FLUX_THREADS, hb, db);
+    if (oa) sh[da] = ha;
+    if (ob) sh[db] = hb;
+  }
+  if (HYB) {  // listed interfaces: general reconstruction (closures, WENO7 / WENO5)
+    for (int r = threadIdx.x; r < NCS * nq; r += FLUX_THREADS) {
+      const int nqd = nq > 0 ? nq : 1;
+      const int cs = r / nqd;
+      const int e = squeue[r - cs * nqd];
+      const int it = e & 0xffff, scm = e >> 16;
+      int t, l;
+      decode(it, t, l);
+      const double* v = sf + sidx(cs, t + 3, l);
+      const int ig = s0 - 1 + t;
+      sh[cs * NI + it] = cs < NC ? interface_flux<SCHEME, true, VS>(v, ig, n, DIR, scm)
+                                 : interface_flux<SCHEME, false, VS>(v, ig, n, DIR, scm);
+    }
   }
   __syncthreads();
 
