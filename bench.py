@@ -54,6 +54,8 @@ def parse():
                     help="jet workload: compare FP64 chemistry with the gated surrogate (trains it first)")
     ap.add_argument("--character", action="store_true",
                     help="characteristic-space inviscid flux (IF_Scheme_Character = 1) instead of component-wise")
+    ap.add_argument("--tiles", default="auto", choices=["auto", "default"],
+                    help="stencil tiles: timed by the autotuner before the warm-up (auto) or the defaults")
     ap.add_argument("--nz", type=int, default=None,
                     help="cells along z (flat plate: 128 = full; jet: 256 = full), for small profiling runs")
     return ap.parse_args()
@@ -504,6 +506,14 @@ def main_ours(a):
     tt = 0.0
     chk = solver._chk
     reac, nsub = int(getattr(c, "if_reaction", 0) or 0), int(getattr(c, "nsub", 1) or 1)
+    tiles = {"mode": a.tiles, "choice": g.tiles()}
+    if a.tiles == "auto":
+        chk(L.ocfd_gpu_run(dt, tt, 1, reac, nsub))  # one step so that the tuner sees a running state
+        tt += dt
+        choice, tms = g.autotune(reps=5)
+        tiles = {"mode": "auto", "choice": choice,
+                 "candidate_ms": {"flux_x": tms[0:3], "flux_y": tms[3:6], "flux_z": tms[6:9],
+                                  "visc_ev_kc8_16_32_64": tms[9:13], "visc_div_kc8_16_32_64": tms[13:17]}}
     chk(L.ocfd_gpu_run(dt, tt, a.warmup, reac, nsub))
     tt += a.warmup * dt
 
@@ -633,6 +643,7 @@ def main_ours(a):
                "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
                "config": {"workload": name, "cells_per_gpu": c.ncell, "dt": dt, "chemistry": ("plain FP64 implicit Euler, %d sub-step(s) per step" % nsub) if reac else "off (non-reacting air)",
                           "parallelism": "replicas x%d (no data-path collective)" % world,
+                          "tiles": tiles,
                           "l2": "device state %.1f GB per GPU >> 126 MB L2; no flush between steps" % state_gb},
                "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches),
                "clocks": clk.summary()}

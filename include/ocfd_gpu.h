@@ -205,6 +205,21 @@ int ocfd_gpu_chem_batch_device(int n, double* d_di, double* d_e, const double* d
  * content, IF_RealGas and CHEM_TimeAdv. */
 int ocfd_gpu_chem_setup(const ocfd_thermo* th, const ocfd_kinetics* kin, int realgas, int timeadv);
 
+/* Stencil tile autotuner (no counterpart in the reference, whose loops have no tiles). A tile
+ * choice is int[5] = {flux tile shape of the x, y, z flow sweeps (0, 1, 2); k planes per block of
+ * the viscous-flux kernel and of its divergence kernel}. Shapes (cells along the sweep x pencils):
+ * x 56x4, 120x2, 24x8; y / z 24x16, 24x8, 56x8. Every choice gives bit-identical results.
+ * ocfd_gpu_autotune times each candidate on the current state (after ocfd_gpu_init_state) over reps
+ * launches, applies the fastest and remembers it for this configuration (grid, schemes, species)
+ * in the process; reps = 0 applies a remembered choice without timing when there is one. choice
+ * (may be NULL) receives the choice; ms (may be NULL, 17 doubles) the mean ms per launch of each
+ * candidate: flux x, y, z shapes 0..2, then k_visc_ev and k_visc_div at 8, 16, 32, 64 planes
+ * (-1 where not timed). The launches write only scratch arrays, so the solution is unchanged.
+ * Default choice {0, 0, 0, 16, 16}. */
+int ocfd_gpu_autotune(int reps, int* choice, double* ms);
+int ocfd_gpu_set_tiles(const int* choice);
+int ocfd_gpu_get_tiles(int* choice);
+
 /* Per-kernel-class CUDA-event timing of the non-graph launches (enable resets the totals). */
 int ocfd_gpu_profile(int enable);
 int ocfd_gpu_profile_read(int cls, double* ms, long long* count);

@@ -77,29 +77,28 @@ __device__ __forceinline__ void split_point(double Et1, double p1, double c1, do
   }
 }
 
-// Tile shapes. x sweeps run along the contiguous index, so a tile is a long chunk of few lines;
-// y / z sweeps put 16 contiguous i-lines across a half-warp and a chunk along j / k. Each
-// shape makes the split phase (C + 8 points of NL pencils) a whole number of 256-thread rounds.
-constexpr int FLUX_THREADS = 256;
+// Tile shapes: C cells along the sweep x NL pencils. x sweeps run along the contiguous index, so
+// a tile is a long chunk of few lines; y / z sweeps put NL contiguous i-lines side by side and a
+// chunk along j / k. Every shape makes the split phase (C + 8 points of NL pencils) a whole
+// number of 256-thread rounds. TS = 0 is the default shape; TS = 1, 2 are the alternatives the
+// tile autotuner times for the flow sweeps of a given grid (a tile shape changes which block
+// computes an interface, never its arithmetic, so every shape gives bit-identical fluxes):
+//   x: (C, NL) = (56, 4), (120, 2), (24, 8)        y / z: (24, 16), (24, 8), (56, 8)
 // MINB is the resident-block target given to the register allocator (3 x 256 threads per SM;
-// the shared memory of one tile, 40 KB for x and 73 KB for y / z, also fits 3 times).
-template <int DIR>
+// the shared memory of one tile, at most 42 KB for x and 73 KB for the y / z shapes 0 and 1,
+// also fits 3 times; the 79 KB of y / z shape 2 fits twice).
+constexpr int FLUX_THREADS = 256, FLUX_TILE_SHAPES = 3;
+template <int DIR, int TS = 0>
 struct Tile {
-  static constexpr int C = 56, NL = 4, MINB = 3;
-};
-template <>
-struct Tile<1> {
-  static constexpr int C = 24, NL = 16, MINB = 3;
-};
-template <>
-struct Tile<2> {
-  static constexpr int C = 24, NL = 16, MINB = 3;
+  static constexpr int C = DIR == 0 ? (TS == 0 ? 56 : TS == 1 ? 120 : 24) : (TS == 2 ? 56 : 24);
+  static constexpr int NL = DIR == 0 ? (TS == 0 ? 4 : TS == 1 ? 2 : 8) : (TS == 0 ? 16 : 8);
+  static constexpr int MINB = (DIR != 0 && TS == 2) ? 2 : 3;
 };
 
 // NC components per point: the five flow fluxes, or G species of a scalar sweep
-template <int DIR, int NC_>
+template <int DIR, int NC_, int TS = 0>
 struct FluxTile {
-  static constexpr int C = Tile<DIR>::C, NL = Tile<DIR>::NL, P = C + 8, NC = NC_;
+  static constexpr int C = Tile<DIR, TS>::C, NL = Tile<DIR, TS>::NL, P = C + 8, NC = NC_;
   static constexpr int NCS = 2 * NC;        // (component, sign) pairs: plus components, then minus
   static constexpr int NI = (C + 1) * NL;   // interfaces of a tile
   static_assert((P * NL) % FLUX_THREADS == 0, "split phase must fill whole rounds");
@@ -144,9 +143,9 @@ __device__ __forceinline__ double ud7l_signed(const double* v, bool plus) {
 //  3. flux difference (hh(i) - hh(i-1)) / d, combined into du as the reference does per sweep.
 // SCALAR sweeps (du_scaler_invis, OCFD_scaler_inviscous.f90) carry G species per block: the
 // split velocity is formed once per point for the group, and blockIdx.z also selects the group.
-template <int DIR, int SCHEME, int SPLIT, bool SEP, bool SCALAR, int G = 1>
-__global__ void __launch_bounds__(FLUX_THREADS, Tile<DIR>::MINB) k_flux(FluxArgs a) {
-  using T = FluxTile<DIR, SCALAR ? G : 5>;
+template <int DIR, int SCHEME, int SPLIT, bool SEP, bool SCALAR, int G = 1, int TS = 0>
+__global__ void __launch_bounds__(FLUX_THREADS, Tile<DIR, TS>::MINB) k_flux(FluxArgs a) {
+  using T = FluxTile<DIR, SCALAR ? G : 5, TS>;
   constexpr int C = T::C, NL = T::NL, P = T::P, NC = T::NC, NCS = T::NCS, NI = T::NI;
   constexpr bool HYB = SCHEME == OCFD_SCHEME_HYBRID;
   constexpr int VS = DIR == 0 ? 1 : NL;  // stride of consecutive sweep points in shared memory
@@ -353,9 +352,9 @@ __global__ void __launch_bounds__(FLUX_THREADS, Tile<DIR>::MINB) k_flux(FluxArgs
   }
 }
 
-template <int DIR, bool SCALAR, int G = 1>
+template <int DIR, bool SCALAR, int G = 1, int TS = 0>
 constexpr size_t flux_smem() {
-  return FluxTile<DIR, SCALAR ? G : 5>::smem;
+  return FluxTile<DIR, SCALAR ? G : 5, TS>::smem;
 }
 
 // ---------------------------------------------------------------- CD6 / CD8 derivative
@@ -411,6 +410,7 @@ struct ViscArgs {
   const double *amu, *amk;        // precomputed transport (NS > 1) or nullptr
   const double *qpx, *qpy, *qpz;  // species enthalpy fluxes (NS > 1) or nullptr
   double* ev[3][4];               // Ev1, Ev2, Ev3 (halo arrays)
+  int kc;                         // k planes marched by one block (grid.z = ceil(nz / kc))
   Geo g;
 };
 
@@ -487,15 +487,17 @@ __device__ __forceinline__ void cp_async_wait() {
 }
 
 // k_visc_ev as a 2.5-D stencil: a VE_TX x VE_TY tile of (i, j) columns marches along a chunk of
-// VE_KC planes in k. The x / y neighbours of (u, v, w, T) come from a shared-memory copy of the
-// current plane with an HZ-point halo, the z neighbours from a ring of the tile's own columns, so
-// each value is read from global memory about twice per sweep instead of once per stencil use.
+// kc planes in k (VE_KC by default; the tile autotuner times the VE_KC_CHOICES). The x / y
+// neighbours of (u, v, w, T) come from a shared-memory copy of the current plane with an
+// HZ-point halo, the z neighbours from a ring of the tile's own columns, so each value is read
+// from global memory about (kc + 2 HZ) / kc times per sweep instead of once per stencil use.
 // The copies of plane k+1 (and ring plane k+HZ+1) are in flight while plane k is computed: the
 // halo plane is double-buffered and the ring has 2 HZ + 2 slots. HZ = 3 for CD6, 4 for CD8.
 #ifndef OCFD_VE_MINB
 #define OCFD_VE_MINB 2  // resident blocks per SM given to the register allocator
 #endif
 constexpr int VE_TX = 32, VE_TY = 8, VE_KC = 16, VE_THREADS = VE_TX * VE_TY;
+constexpr int VE_KC_CHOICES[4] = {8, 16, 32, 64};
 template <int HZ>
 struct VeTile {
   static constexpr int W = VE_TX + 2 * HZ, HH = VE_TY + 2 * HZ, PL = W * HH;  // halo plane
@@ -511,9 +513,9 @@ __global__ void __launch_bounds__(VE_THREADS, OCFD_VE_MINB) k_visc_ev(ViscArgs a
   double* pl = smem;                 // [2][4][HH][W]: u, v, w, T of planes k, k+1 with the halo
   double* ring = smem + 2 * 4 * PL;  // [RS][4][VE_THREADS]: planes k-HZ .. k+HZ+1, own columns
   const int tid = threadIdx.x, tx = tid % VE_TX, ty = tid / VE_TX;
-  const int i0 = blockIdx.x * VE_TX + 1, j0 = blockIdx.y * VE_TY + 1, k0 = blockIdx.z * VE_KC + 1;
+  const int i0 = blockIdx.x * VE_TX + 1, j0 = blockIdx.y * VE_TY + 1, k0 = blockIdx.z * a.kc + 1;
   const int i = i0 + tx, j = j0 + ty;
-  const int k1 = min(k0 + VE_KC - 1, cC.nz);
+  const int k1 = min(k0 + a.kc - 1, cC.nz);
   const int imax = cC.nx + OCFD_L, jmax = cC.ny + OCFD_L;  // last index of the halo arrays
   const bool in_array = i <= imax && j <= jmax;
   const bool active = i <= cC.nx && j <= cC.ny;
@@ -581,6 +583,7 @@ __global__ void __launch_bounds__(VE_THREADS, OCFD_VE_MINB) k_visc_ev(ViscArgs a
 struct DivArgs {
   const double* ev[12];  // Ev1 (4), Ev2 (4), Ev3 (4) halo arrays, periodic halos exchanged
   double* du;
+  int kc;                // k planes marched by one block
   Geo g;
 };
 
@@ -603,9 +606,9 @@ __global__ void __launch_bounds__(VE_THREADS, 2) k_visc_div(DivArgs a) {
   double* pb = smem;                        // [2][ [4][VE_TY][W] Ev1 | [4][HH][VE_TX] Ev2 ]
   double* ring = smem + 2 * 4 * (PX + PY);  // [RS][4][VE_THREADS]: Ev3 of planes k-HZ .. k+HZ+1
   const int tid = threadIdx.x, tx = tid % VE_TX, ty = tid / VE_TX;
-  const int i0 = blockIdx.x * VE_TX + 1, j0 = blockIdx.y * VE_TY + 1, k0 = blockIdx.z * VE_KC + 1;
+  const int i0 = blockIdx.x * VE_TX + 1, j0 = blockIdx.y * VE_TY + 1, k0 = blockIdx.z * a.kc + 1;
   const int i = i0 + tx, j = j0 + ty;
-  const int k1 = min(k0 + VE_KC - 1, cC.nz);
+  const int k1 = min(k0 + a.kc - 1, cC.nz);
   const int imax = cC.nx + OCFD_L, jmax = cC.ny + OCFD_L;
   const bool in_array = i <= imax && j <= jmax;
   const bool active = i <= cC.nx && j <= cC.ny;

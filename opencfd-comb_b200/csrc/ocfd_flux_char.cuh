@@ -90,7 +90,6 @@ __global__ void __launch_bounds__(FLUX_THREADS, 2) k_flux_char(FluxArgs a) {
   using T = CharTile<DIR>;
   constexpr int C = T::C, NL = T::NL, P = T::P, NI = T::NI, NQ = T::NQ;
   constexpr bool HYB = SCHEME == OCFD_SCHEME_HYBRID;
-  constexpr int VS = DIR == 0 ? 1 : NL;
   extern __shared__ double smem[];
   double* sf = smem;                // [10][P x NL]: F+ (5) then F- (5)
   double* sq = sf + 10 * P * NL;    // [NQ][P x NL]: point state

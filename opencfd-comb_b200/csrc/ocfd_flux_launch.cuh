@@ -7,23 +7,27 @@
 
 namespace ocfd {
 namespace flux_launch {
-template <int DIR, int SCHEME, int SPLIT, bool SEP, bool SCALAR, int G>
+template <int DIR, int TS>
+dim3 tile_grid(int nx, int ny, int nz) {
+  using T = Tile<DIR, TS>;
+  auto nb = [](int n, int b) { return (unsigned)((n + b - 1) / b); };
+  if (DIR == 0) return dim3(nb(nx, T::C), nb(ny, T::NL), nz);
+  if (DIR == 1) return dim3(nb(nx, T::NL), nb(ny, T::C), nz);
+  return dim3(nb(nx, T::NL), nb(nz, T::C), ny);
+}
+template <int DIR, int SCHEME, int SPLIT, bool SEP, bool SCALAR, int G, int TS = 0>
 void go(FluxArgs a, int ngroups, int nx, int ny, int nz, cudaStream_t st) {
-  constexpr size_t sm = flux_smem<DIR, SCALAR, G>();
+  constexpr size_t sm = flux_smem<DIR, SCALAR, G, TS>();
   static bool attr = false;
   if (!attr) {
-    cudaFuncSetAttribute(k_flux<DIR, SCHEME, SPLIT, SEP, SCALAR, G>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    cudaFuncSetAttribute(k_flux<DIR, SCHEME, SPLIT, SEP, SCALAR, G, TS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)sm);
     attr = true;
   }
-  auto nb = [](int n, int b) { return (unsigned)((n + b - 1) / b); };
-  dim3 grid;
-  if (DIR == 0) grid = dim3(nb(nx, Tile<0>::C), nb(ny, Tile<0>::NL), nz);
-  else if (DIR == 1) grid = dim3(nb(nx, Tile<1>::NL), nb(ny, Tile<1>::C), nz);
-  else grid = dim3(nb(nx, Tile<2>::NL), nb(nz, Tile<2>::C), ny);
+  dim3 grid = tile_grid<DIR, TS>(nx, ny, nz);
   a.nbz = (int)grid.z;
   grid.z *= (unsigned)ngroups;
-  k_flux<DIR, SCHEME, SPLIT, SEP, SCALAR, G><<<grid, FLUX_THREADS, sm, st>>>(a);
+  k_flux<DIR, SCHEME, SPLIT, SEP, SCALAR, G, TS><<<grid, FLUX_THREADS, sm, st>>>(a);
 }
 template <int DIR, int SCHEME, int SPLIT, bool SEP>
 void go_char(FluxArgs a, int nx, int ny, int nz, cudaStream_t st) {
@@ -33,11 +37,7 @@ void go_char(FluxArgs a, int nx, int ny, int nz, cudaStream_t st) {
     cudaFuncSetAttribute(k_flux_char<DIR, SCHEME, SPLIT, SEP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     attr = true;
   }
-  auto nb = [](int n, int b) { return (unsigned)((n + b - 1) / b); };
-  dim3 grid;
-  if (DIR == 0) grid = dim3(nb(nx, Tile<0>::C), nb(ny, Tile<0>::NL), nz);
-  else if (DIR == 1) grid = dim3(nb(nx, Tile<1>::NL), nb(ny, Tile<1>::C), nz);
-  else grid = dim3(nb(nx, Tile<2>::NL), nb(nz, Tile<2>::C), ny);
+  dim3 grid = tile_grid<DIR, 0>(nx, ny, nz);
   a.nbz = (int)grid.z;
   k_flux_char<DIR, SCHEME, SPLIT, SEP><<<grid, FLUX_THREADS, sm, st>>>(a);
 }
@@ -65,6 +65,24 @@ void launch(int scheme, int split, bool sep, int group, int ngroups, bool charac
   if (group != 0 && group != 1 && group != 3) throw std::runtime_error("species group");
   if (sep) pick<DIR, true>(scheme, split, group, ngroups, character, a, nx, ny, nz, st);
   else pick<DIR, false>(scheme, split, group, ngroups, character, a, nx, ny, nz, st);
+}
+// the flow fluxes (no species group, component-wise) with the alternative tile shape TS
+template <int DIR, int TS>
+void launch_tile(int scheme, int split, bool sep, const FluxArgs& a, int nx, int ny, int nz, cudaStream_t st) {
+#define FT(S)                                                                                           \
+  if (scheme == S) {                                                                                    \
+    if (sep) {                                                                                          \
+      if (split == OCFD_SPLIT_SW) go<DIR, S, OCFD_SPLIT_SW, true, false, 1, TS>(a, 1, nx, ny, nz, st);   \
+      else go<DIR, S, OCFD_SPLIT_LLF, true, false, 1, TS>(a, 1, nx, ny, nz, st);                        \
+    } else {                                                                                            \
+      if (split == OCFD_SPLIT_SW) go<DIR, S, OCFD_SPLIT_SW, false, false, 1, TS>(a, 1, nx, ny, nz, st);  \
+      else go<DIR, S, OCFD_SPLIT_LLF, false, false, 1, TS>(a, 1, nx, ny, nz, st);                       \
+    }                                                                                                   \
+    return;                                                                                             \
+  }
+  FT(OCFD_SCHEME_WENO5) FT(OCFD_SCHEME_WENO7) FT(OCFD_SCHEME_OMP6) FT(OCFD_SCHEME_UD7L) FT(OCFD_SCHEME_HYBRID)
+#undef FT
+  throw std::runtime_error("scheme");
 }
 }  // namespace flux_launch
 }  // namespace ocfd

@@ -7,7 +7,9 @@
 
 #include <cmath>
 #include <cstdio>
+#include <array>
 #include <cstring>
+#include <map>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -79,6 +81,10 @@ struct Lib {
   cudaGraphExec_t gexec = nullptr;
   double g_dt = 0;
   int g_ifr = -1, g_nsub = -1, g_par = -1, g_launches = 0;
+  // stencil tile choices (ocfd_gpu_set_tiles / ocfd_gpu_autotune): flow-flux tile shape per
+  // sweep direction, k planes per block of k_visc_ev and k_visc_div
+  int flux_ts[3] = {0, 0, 0};
+  int kc_ev = VE_KC, kc_div = VE_KC;
   // batched chemistry scratch
   double *b_di = nullptr, *b_e = nullptr, *b_dt = nullptr;
   int *b_nsub = nullptr, *b_perm = nullptr, *b_hist = nullptr, *b_counter = nullptr, *b_nfail = nullptr;
@@ -178,7 +184,14 @@ void launch_flux(int dir, const FluxArgs& a, int group = 0, int ngroups = 1) {
   KTimer t(group ? KC_SPECIES : KC_FLUX_X + dir);
   const ocfd_params& P = L->P;
   const bool ch = P.if_scheme_character == 1;
-  if (dir == 0) launch_flux_x(P.scheme_invis, P.flux_splitting, L->sep, group, ngroups, ch, a, P.nx, P.ny, P.nz, L->st);
+  const int ts = (group == 0 && !ch) ? L->flux_ts[dir] : 0;
+  if (ts != 0) {
+    using Fn = void (*)(int, int, bool, const FluxArgs&, int, int, int, cudaStream_t);
+    static const Fn tab[3][2] = {{launch_flux_x_t1, launch_flux_x_t2},
+                                 {launch_flux_y_t1, launch_flux_y_t2},
+                                 {launch_flux_z_t1, launch_flux_z_t2}};
+    tab[dir][ts - 1](P.scheme_invis, P.flux_splitting, L->sep, a, P.nx, P.ny, P.nz, L->st);
+  } else if (dir == 0) launch_flux_x(P.scheme_invis, P.flux_splitting, L->sep, group, ngroups, ch, a, P.nx, P.ny, P.nz, L->st);
   else if (dir == 1) launch_flux_y(P.scheme_invis, P.flux_splitting, L->sep, group, ngroups, ch, a, P.nx, P.ny, P.nz, L->st);
   else launch_flux_z(P.scheme_invis, P.flux_splitting, L->sep, group, ngroups, ch, a, P.nx, P.ny, P.nz, L->st);
   LAUNCH_CHECK();
@@ -323,7 +336,7 @@ void visc_ev_go(const ViscArgs& va) {
     attr = true;
   }
   const ocfd_params& P = L->P;
-  dim3 grid(nblk(P.nx, VE_TX), nblk(P.ny, VE_TY), nblk(P.nz, VE_KC));
+  dim3 grid(nblk(P.nx, VE_TX), nblk(P.ny, VE_TY), nblk(P.nz, va.kc));
   k_visc_ev<NS, SEP, HZ><<<grid, VE_THREADS, sm, L->st>>>(va);
 }
 
@@ -336,8 +349,52 @@ void visc_div_go(const DivArgs& da) {
     attr = true;
   }
   const ocfd_params& P = L->P;
-  dim3 grid(nblk(P.nx, VE_TX), nblk(P.ny, VE_TY), nblk(P.nz, VE_KC));
+  dim3 grid(nblk(P.nx, VE_TX), nblk(P.ny, VE_TY), nblk(P.nz, da.kc));
   k_visc_div<SEP, HZ><<<grid, VE_THREADS, sm, L->st>>>(da);
+}
+
+// kernel arguments of the stage's flow sweeps and viscous kernels on the current state
+FluxArgs flow_flux_args() {
+  FluxArgs fa{};
+  fa.d = L->d; fa.u = L->u; fa.v = L->v; fa.w = L->w; fa.p = L->p; fa.Et = L->Et[L->cur]; fa.Rh = L->Rh;
+  fa.out = L->du;
+  fa.g = L->geo;
+  return fa;
+}
+template <int NS>
+ViscArgs visc_args() {
+  ViscArgs va{};
+  va.d = L->d; va.u = L->u; va.v = L->v; va.w = L->w; va.T = L->T; va.di = L->di;
+  if (NS > 1) {
+    va.amu = L->amu; va.amk = L->amk;
+    va.qpx = L->qp[0]; va.qpy = L->qp[1]; va.qpz = L->qp[2];
+  }
+  for (int dd = 0; dd < 3; dd++)
+    for (int m = 0; m < 4; m++) va.ev[dd][m] = L->ev[4 * dd + m];
+  va.g = L->geo;
+  va.kc = L->kc_ev;
+  return va;
+}
+DivArgs div_args() {
+  DivArgs da{};
+  for (int m = 0; m < 12; m++) da.ev[m] = L->ev[m];
+  da.du = L->du;
+  da.g = L->geo;
+  da.kc = L->kc_div;
+  return da;
+}
+template <int NS>
+void visc_ev_launch(const ViscArgs& va) {
+  const bool cd8 = L->P.scheme_vis == OCFD_SCHEME_CD8;
+  if (L->sep) cd8 ? visc_ev_go<NS, true, 4>(va) : visc_ev_go<NS, true, 3>(va);
+  else cd8 ? visc_ev_go<NS, false, 4>(va) : visc_ev_go<NS, false, 3>(va);
+  LAUNCH_CHECK();
+}
+void visc_div_launch(const DivArgs& da) {
+  const bool cd8 = L->P.scheme_vis == OCFD_SCHEME_CD8;
+  if (L->sep) cd8 ? visc_div_go<true, 4>(da) : visc_div_go<true, 3>(da);
+  else cd8 ? visc_div_go<false, 4>(da) : visc_div_go<false, 3>(da);
+  LAUNCH_CHECK();
 }
 
 template <int NS>
@@ -359,9 +416,7 @@ void stage_t(int krk, double dt1) {
     sensor();
     exchange({L->Rh}, 7);
   }
-  FluxArgs fa{};
-  fa.d = L->d; fa.u = L->u; fa.v = L->v; fa.w = L->w; fa.p = L->p; fa.Et = Etc; fa.Rh = L->Rh;
-  fa.g = L->geo;
+  FluxArgs fa = flow_flux_args();
   if (NS > 1) {
     // every species at once (du_scaler_invis / du_scaler_viscous / Scalar_time_adv_RK3 of the
     // reference's species loop): Dus of species m is dus + m N
@@ -398,35 +453,16 @@ void stage_t(int krk, double dt1) {
   fa.out = L->du;
   for (int dd = 0; dd < 3; dd++) launch_flux(dd, fa);
   if (L->P.if_viscous == 1) {
-    ViscArgs va{};
-    va.d = L->d; va.u = L->u; va.v = L->v; va.w = L->w; va.T = L->T; va.di = L->di;
-    if (NS > 1) {
-      va.amu = L->amu; va.amk = L->amk;
-      va.qpx = L->qp[0]; va.qpy = L->qp[1]; va.qpz = L->qp[2];
-    }
-    for (int dd = 0; dd < 3; dd++)
-      for (int m = 0; m < 4; m++) va.ev[dd][m] = L->ev[4 * dd + m];
-    va.g = L->geo;
     {
       KTimer t(KC_VISC_EV);
-      const bool cd8 = L->P.scheme_vis == OCFD_SCHEME_CD8;
-      if (L->sep) cd8 ? visc_ev_go<NS, true, 4>(va) : visc_ev_go<NS, true, 3>(va);
-      else cd8 ? visc_ev_go<NS, false, 4>(va) : visc_ev_go<NS, false, 3>(va);
-      LAUNCH_CHECK();
+      visc_ev_launch<NS>(visc_args<NS>());
     }
     exchange({L->ev[0], L->ev[1], L->ev[2], L->ev[3]}, 1);
     exchange({L->ev[4], L->ev[5], L->ev[6], L->ev[7]}, 2);
     exchange({L->ev[8], L->ev[9], L->ev[10], L->ev[11]}, 4);
     {
       KTimer t(KC_VISC_DIV);
-      DivArgs da{};
-      for (int m = 0; m < 12; m++) da.ev[m] = L->ev[m];
-      da.du = L->du;
-      da.g = L->geo;
-      const bool cd8 = L->P.scheme_vis == OCFD_SCHEME_CD8;
-      if (L->sep) cd8 ? visc_div_go<true, 4>(da) : visc_div_go<true, 3>(da);
-      else cd8 ? visc_div_go<false, 4>(da) : visc_div_go<false, 3>(da);
-      LAUNCH_CHECK();
+      visc_div_launch(div_args());
     }
   }
   // N_SPEC = 1: di = d over the whole array (OCFD_Time_Adv.f90:45-52). Nothing between the stage
@@ -470,6 +506,97 @@ void chem_t(double dt2, int nsub) {
     launch_chem_cells(NS, L->hc.N, L->f, L->Et[L->cur], L->T, L->p, L->di, dt2, nsub, &L->sdev->newton_fail, L->st);
   }
   LAUNCH_CHECK();
+}
+
+// ---------------------------------------------------------------- stencil tile autotuner
+// Tile choices {flux x, y, z shape; k_visc_ev, k_visc_div k planes per block}. Every choice
+// gives bit-identical results (a tile decides which block computes a point, not how), so the
+// tuner is free to pick by time alone. Choices are remembered per configuration in the process.
+constexpr int TUNE_N = 5, TUNE_TIMES = 3 * FLUX_TILE_SHAPES + 8;
+std::map<std::string, std::array<int, TUNE_N>> g_tune_cache;
+
+std::string tune_key() {
+  const ocfd_params& P = L->P;
+  char b[200];
+  std::snprintf(b, sizeof b, "%d %d %d|%d %d %d %d|%d %d %d", P.nx, P.ny, P.nz, P.scheme_invis, P.flux_splitting,
+                P.if_scheme_character, (int)L->sep, L->NS, P.if_viscous, P.scheme_vis);
+  return b;
+}
+
+void apply_tiles(const int* c) {
+  for (int d = 0; d < 3; d++) L->flux_ts[d] = c[d];
+  L->kc_ev = c[3];
+  L->kc_div = c[4];
+  if (L->gexec) {  // the captured step holds the old launches
+    CK(cudaGraphExecDestroy(L->gexec));
+    L->gexec = nullptr;
+  }
+}
+
+// times every candidate of each family on the current state (one warm-up launch, then reps
+// launches between two events) and applies the fastest; the launches write only scratch arrays
+// (du, Ev, the hybrid sensor) that every stage recomputes before it reads them
+template <int NS>
+void tune_t(int reps, int* best, double* ms) {
+  cudaEvent_t e0, e1;
+  CK(cudaEventCreate(&e0));
+  CK(cudaEventCreate(&e1));
+  auto timed = [&](auto&& launch) {
+    launch();
+    CK(cudaEventRecord(e0, L->st));
+    for (int r = 0; r < reps; r++) launch();
+    CK(cudaEventRecord(e1, L->st));
+    CK(cudaEventSynchronize(e1));
+    float t = 0.f;
+    CK(cudaEventElapsedTime(&t, e0, e1));
+    return (double)t / reps;
+  };
+  try {
+    const ocfd_params& P = L->P;
+    if (P.scheme_invis == OCFD_SCHEME_HYBRID) {
+      sensor();
+      exchange({L->Rh}, 7);
+    }
+    const FluxArgs fa = flow_flux_args();
+    const bool ch = P.if_scheme_character == 1;
+    for (int d = 0; d < 3; d++) {
+      double tmin = 1e300;
+      best[d] = 0;
+      for (int ts = 0; ts < FLUX_TILE_SHAPES; ts++) {
+        if (ch && ts > 0) { ms[d * FLUX_TILE_SHAPES + ts] = -1.0; continue; }  // one characteristic tile
+        L->flux_ts[d] = ts;
+        const double t = timed([&] { launch_flux(d, fa); });
+        ms[d * FLUX_TILE_SHAPES + ts] = t;
+        if (t < tmin) { tmin = t; best[d] = ts; }
+      }
+      L->flux_ts[d] = best[d];
+    }
+    best[3] = best[4] = VE_KC;
+    for (int m = 0; m < 4; m++) ms[3 * FLUX_TILE_SHAPES + m] = ms[3 * FLUX_TILE_SHAPES + 4 + m] = -1.0;
+    if (P.if_viscous == 1) {
+      double t_ev = 1e300, t_div = 1e300;
+      for (int m = 0; m < 4; m++) {
+        ViscArgs va = visc_args<NS>();
+        va.kc = VE_KC_CHOICES[m];
+        const double t = timed([&] { visc_ev_launch<NS>(va); });
+        ms[3 * FLUX_TILE_SHAPES + m] = t;
+        if (t < t_ev) { t_ev = t; best[3] = va.kc; }
+      }
+      for (int m = 0; m < 4; m++) {
+        DivArgs da = div_args();
+        da.kc = VE_KC_CHOICES[m];
+        const double t = timed([&] { visc_div_launch(da); });
+        ms[3 * FLUX_TILE_SHAPES + 4 + m] = t;
+        if (t < t_div) { t_div = t; best[4] = da.kc; }
+      }
+    }
+  } catch (...) {
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    throw;
+  }
+  CK(cudaEventDestroy(e0));
+  CK(cudaEventDestroy(e1));
 }
 
 double wall_ht(double tt) {
@@ -622,10 +749,8 @@ __global__ void k_shift(double* X, double* Y, double* Z, int dir, double sx, dou
   int n = dir == 0 ? cC.nx : (dir == 1 ? cC.ny : cC.nz);
   int s = side == 0 ? 1 - L + l : n + 1 + l;
   int q = dir == 0 ? hidx(s, a, b) : (dir == 1 ? hidx(a, s, b) : hidx(a, b, s));
-  double sg = side == 0 ? -1.0 : 1.0;
   if (side == 0) { X[q] = X[q] - sx; Y[q] = Y[q] - sy; Z[q] = Z[q] - sz; }
   else { X[q] = X[q] + sx; Y[q] = Y[q] + sy; Z[q] = Z[q] + sz; }
-  (void)sg;
 }
 // comput_Jacobian3d (OCFD_mesh.f90:60-107) for general grids
 __global__ void k_jacobian(const double* X, const double* Y, const double* Z, double* const* m) {
@@ -799,8 +924,6 @@ __global__ void k_expand_metrics(Geo g, double* out, long long H) {
   int i = (int)(t % cC.HX) - OCFD_L + 1;
   int j = (int)((t / cC.HX) % cC.HY) - OCFD_L + 1;
   int k = (int)(t / cC.HX / cC.HY) - OCFD_L + 1;
-  bool ox = i < 1 || i > cC.nx, oy = j < 1 || j > cC.ny, oz = k < 1 || k > cC.nz;
-  (void)ox; (void)oy; (void)oz;
   if (metric_unfilled(i, j, k)) {
     for (int m = 0; m < 10; m++) out[m * H + t] = 1.0;
     return;
@@ -1583,6 +1706,56 @@ int ocfd_gpu_stats(long long* neg_et, long long* newton_fail) {
     if (neg_et) *neg_et = (long long)L->shost->neg_total;
     if (newton_fail) *newton_fail = L->shost->newton_fail;
     return 0;
+  });
+}
+
+int ocfd_gpu_set_tiles(const int* choice) {
+  return guarded([&]() -> int {
+    if (!L || !L->flow_ready) { g_err = "state not initialised"; return OCFD_ERR_STATE; }
+    if (!choice) { g_err = "choice is NULL"; return OCFD_ERR_PARAM; }
+    for (int d = 0; d < 3; d++)
+      if (choice[d] < 0 || choice[d] >= FLUX_TILE_SHAPES) { g_err = "flux tile shape must be 0, 1 or 2"; return OCFD_ERR_PARAM; }
+    if (L->P.if_scheme_character == 1 && (choice[0] | choice[1] | choice[2]) != 0) {
+      g_err = "the characteristic flux has one tile shape (0)";
+      return OCFD_ERR_PARAM;
+    }
+    if (choice[3] < 1 || choice[4] < 1) { g_err = "k planes per block must be >= 1"; return OCFD_ERR_PARAM; }
+    apply_tiles(choice);
+    return 0;
+  });
+}
+
+int ocfd_gpu_get_tiles(int* choice) {
+  if (!L || !choice) return OCFD_ERR_STATE;
+  for (int d = 0; d < 3; d++) choice[d] = L->flux_ts[d];
+  choice[3] = L->kc_ev;
+  choice[4] = L->kc_div;
+  return 0;
+}
+
+int ocfd_gpu_autotune(int reps, int* choice, double* ms) {
+  return guarded([&]() -> int {
+    if (!L || !L->flow_ready) { g_err = "state not initialised"; return OCFD_ERR_STATE; }
+    if (reps < 0) { g_err = "reps must be >= 0"; return OCFD_ERR_PARAM; }
+    int best[TUNE_N];
+    double t[TUNE_TIMES];
+    const std::string key = tune_key();
+    auto it = g_tune_cache.find(key);
+    if (reps == 0 && it != g_tune_cache.end()) {
+      for (int m = 0; m < TUNE_N; m++) best[m] = it->second[m];
+      for (int m = 0; m < TUNE_TIMES; m++) t[m] = -1.0;
+    } else {
+      NS_DISPATCH(L->NS, tune_t<NSV>(reps > 0 ? reps : 3, best, t));
+      std::array<int, TUNE_N> a;
+      for (int m = 0; m < TUNE_N; m++) a[m] = best[m];
+      g_tune_cache[key] = a;
+    }
+    apply_tiles(best);
+    if (choice)
+      for (int m = 0; m < TUNE_N; m++) choice[m] = best[m];
+    if (ms)
+      for (int m = 0; m < TUNE_TIMES; m++) ms[m] = t[m];
+    return check_status();
   });
 }
 

@@ -127,6 +127,9 @@ GPU_SIGNATURES = {
     "ocfd_gpu_init_state": (I, [PD, PD, D]),
     "ocfd_gpu_run": (I, [D, D, I, I, I]),
     "ocfd_gpu_chem_setup": (I, [C.POINTER(Thermo), C.POINTER(Kinetics), I, I]),
+    "ocfd_gpu_autotune": (I, [I, PI, PD]),
+    "ocfd_gpu_set_tiles": (I, [PI]),
+    "ocfd_gpu_get_tiles": (I, [PI]),
     "ocfd_gpu_profile": (I, [I]),
     "ocfd_gpu_profile_read": (I, [I, PD, C.POINTER(C.c_longlong)]),
     "ocfd_gpu_profile_name": (C.c_char_p, [I]),

@@ -21,6 +21,7 @@ generated here from a fixed NumPy seed:
 Arrays use the reference's Fortran layout: a halo array (1-LAP:nx+LAP, ...) is a numpy array of
 shape (nz+2L, ny+2L, nx+2L); an interior array is (nz, ny, nx); f is (5, nz, ny, nx).
 """
+import ctypes as C
 import json
 import math
 import os
@@ -65,6 +66,39 @@ class Case:
     def halo_shape(self):
         p = self.params
         return (p.nz + 2 * LAP, p.ny + 2 * LAP, p.nx + 2 * LAP)
+
+    def save(self, path):
+        """Writes the case file read by the compiled host driver (host/ns_solver.cpp): the ABI
+        records as bytes, then dt / nsteps / chemistry switch / sub-steps, grid, initial
+        primitives, species densities and the boundary tables."""
+        import struct
+        with open(path, "wb") as fh:
+            fh.write(b"OCFDCASE")
+            fh.write(struct.pack("<5i", 1, C.sizeof(abi.Params), C.sizeof(abi.Thermo), C.sizeof(abi.Kinetics),
+                                 C.sizeof(abi.Transport)))
+            fh.write(bytes(self.params))
+            fh.write(bytes(self.thermo))
+            fh.write(struct.pack("<i", 1 if self.kin is not None else 0))
+            if self.kin is not None:
+                fh.write(bytes(self.kin))
+            fh.write(bytes(self.trans))
+            fh.write(struct.pack("<d3i", self.dt, self.nsteps, self.if_reaction, self.nsub))
+            coords = np.ascontiguousarray(self.coords, dtype=np.float64)
+            fh.write(struct.pack("<q", coords.size // 3))
+            fh.write(coords.tobytes())
+            prim = np.ascontiguousarray(self.prim5, dtype=np.float64)
+            fh.write(struct.pack("<q", prim.size // 5))
+            fh.write(prim.tobytes())
+            di = np.ascontiguousarray(self.di, dtype=np.float64)
+            fh.write(struct.pack("<i", self.params.n_spec))
+            fh.write(di.tobytes())
+            fh.write(struct.pack("<i", 1 if self.bc is not None else 0))
+            if self.bc is not None:
+                for key in ("inlet", "upper", "wall_pertb", "tm", "fait"):
+                    a = self.bc.get(key)
+                    a = np.zeros(0) if a is None else np.ascontiguousarray(a, dtype=np.float64).ravel()
+                    fh.write(struct.pack("<q", a.size))
+                    fh.write(a.tobytes())
 
     def bcdata(self):
         """abi.BcData pointing at this case's arrays (kept alive by the case)."""

@@ -114,6 +114,24 @@ class Solver:
         _chk(lib().ocfd_gpu_stats(C.byref(a), C.byref(b)))
         return a.value, b.value
 
+    # ---- stencil tiles ----
+    def autotune(self, reps=5):
+        """Times the candidate tile shapes on the current state and applies the fastest; returns
+        (choice, ms per launch of each candidate)."""
+        ch = (C.c_int * 5)()
+        ms = (C.c_double * 17)()
+        _chk(lib().ocfd_gpu_autotune(reps, ch, ms))
+        return list(ch), list(ms)
+
+    def set_tiles(self, choice):
+        ch = (C.c_int * 5)(*choice)
+        _chk(lib().ocfd_gpu_set_tiles(ch))
+
+    def tiles(self):
+        ch = (C.c_int * 5)()
+        _chk(lib().ocfd_gpu_get_tiles(ch))
+        return list(ch)
+
     # ---- measurement helpers ----
     @staticmethod
     def profile(enable):
