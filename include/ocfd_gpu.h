@@ -78,7 +78,7 @@ typedef struct ocfd_params {
   int scheme_invis, scheme_vis;
   int scheme_boundary[6];  /* i-, i+, j-, j+, k-, k+ : 0 WENO5 deleted-stencil, 1 WENO5 full, -1 none */
   int ghost_cell[6];       /* 0 none, 1/2 second-order extrapolation (OCFD_GhostCell.f90:166-364) */
-  int if_scheme_character; /* must be 0 (characteristic flux not built) */
+  int if_scheme_character; /* 0 component-wise, 1 characteristic-space flux */
   int if_viscous;
   int flux_splitting;      /* OCFD_SPLIT_SW / OCFD_SPLIT_LLF */
   int if_mass_force;
@@ -204,6 +204,38 @@ int ocfd_gpu_chem_batch_device(int n, double* d_di, double* d_e, const double* d
 /* Sets up the chemistry tables alone (no grid) for ocfd_gpu_chem_batch: read_Spec + read_Reac
  * content, IF_RealGas and CHEM_TimeAdv. */
 int ocfd_gpu_chem_setup(const ocfd_thermo* th, const ocfd_kinetics* kin, int realgas, int timeadv);
+
+/* filtering (code/others/OCFD_filtering.f90:4-72), the reference's call after every step
+ * (OCFD_NS_Solver.f90:48) with Istep already advanced. filter = Para%Filter(100,10) column-major
+ * (group m's parameters at filter[100*(m-1) + 0..12]: step interval, filter x/y/z, ib, ie, jb, je,
+ * kb, ke (global indices), scheme 1 = 9-point Bogey-Bailly Fo9p, 2 = shock-capturing, amplitude
+ * s0, threshold rth), nfiltering = Para%NFiltering (0..10). Each due group filters f in x, then
+ * y, then z; the primitives keep their values (the shock filter recomputes them from f first,
+ * comput_flow_variables, as the reference does). applied (may be NULL) = 1 when a group ran. */
+int ocfd_gpu_filtering(int istep, int nfiltering, const double* filter, int* applied);
+
+/* Keeps the mixture viscosity Amu of every RK stage (comput_Amu_Amk_AMD at the stage start,
+ * OCFD_Time_Adv.f90:35) on the device so that ocfd_gpu_ana_box can average it. With N_SPEC > 1
+ * it is always kept; a single-species run computes it inline and needs this switch on before
+ * the steps whose last stage ana_box reads. */
+int ocfd_gpu_keep_viscosity(int on);
+
+/* ana_box (code/others/OCFD_ANA.f90:197-303), isotropic-turbulence statistics of the current
+ * state: out[19] = tt, Re_lamda, Re_lamdax, Amt, vv_rms, u_rms, v_rms, w_rms, u_skewness,
+ * u_flatness, ux_skewness, ux_flatness, E_kinetic, d_rms, T_aver, Amu_aver, d_aver, Ux_rms,
+ * Alamdax (the row the reference appends to statistics.dat). Sums are fixed-order trees. */
+int ocfd_gpu_ana_box(double tt, double* out);
+
+/* ana_getQ (OCFD_ANA.f90:143-190): Q, the second invariant of the velocity gradient, into q
+ * (N interior doubles, the array the reference writes to Q-<Istep>.dat). */
+int ocfd_gpu_ana_q(double* q);
+
+/* ana_time_average (OCFD_ANA.f90:39-140): one accumulation of the running means of d, u, v, w,
+ * T and every di on the device; K_average and t_average after it are returned (may be NULL).
+ * ocfd_gpu_ana_average downloads (upload = 0) or restores (upload = 1, from a
+ * opencfd-comb.dat.average restart) the (5 + N_SPEC) interior arrays with K_average, t_average. */
+int ocfd_gpu_ana_time_average(double dt, int* k_average, double* t_average);
+int ocfd_gpu_ana_average(int upload, double* fields, int* k_average, double* t_average);
 
 /* Stencil tile autotuner (no counterpart in the reference, whose loops have no tiles). A tile
  * choice is int[5] = {flux tile shape of the x, y, z flow sweeps (0, 1, 2); k planes per block of

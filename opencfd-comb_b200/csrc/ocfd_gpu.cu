@@ -18,6 +18,7 @@
 #include "ocfd_chem.cuh"
 #include "ocfd_device.cuh"
 #include "ocfd_flow.cuh"
+#include "ocfd_post.cuh"
 
 namespace ocfd {
 // the surrogate's flow-cell chemistry (ocfd_surrogate.cu)
@@ -85,6 +86,13 @@ struct Lib {
   // sweep direction, k planes per block of k_visc_ev and k_visc_div
   int flux_ts[3] = {0, 0, 0};
   int kc_ev = VE_KC, kc_div = VE_KC;
+  // analysis (ocfd_gpu_keep_viscosity, ocfd_gpu_ana_*): the single-species stage viscosity kept
+  // for ana_box, reduction partials, time-average accumulators
+  bool keep_amu = false;
+  double *amu_keep = nullptr, *ana_part = nullptr, *avg = nullptr;
+  size_t ana_part_n = 0;
+  int k_average = 0;
+  double t_average = 0.0;
   // batched chemistry scratch
   double *b_di = nullptr, *b_e = nullptr, *b_dt = nullptr;
   int *b_nsub = nullptr, *b_perm = nullptr, *b_hist = nullptr, *b_counter = nullptr, *b_nfail = nullptr;
@@ -401,6 +409,11 @@ template <int NS>
 void stage_t(int krk, double dt1) {
   const long long N = L->hc.N, H = L->hc.H;
   double* Etc = L->Et[L->cur];
+  if (NS == 1 && L->keep_amu) {  // comput_Amu_Amk_AMD's Amu at the stage start, for ana_box
+    KTimer t(KC_OTHER);
+    k_amu1<<<nblk(N, 256), 256, 0, L->st>>>(L->T, L->di, L->amu_keep);
+    LAUNCH_CHECK();
+  }
   if (NS > 1) {
     KTimer t(KC_SPECIES);
     k_transport<NS><<<nblk(N, 32), dim3(32, NS), 0, L->st>>>(L->d, L->T, L->p, L->di, L->amu, L->amk, L->amd);
@@ -599,6 +612,69 @@ void tune_t(int reps, int* best, double* ms) {
   CK(cudaEventDestroy(e1));
 }
 
+// ---------------------------------------------------------------- filtering and analysis
+// filtering (OCFD_filtering.f90:4-72) for the groups whose step interval divides istep; F is
+// Para%Filter(100,10) column-major. Every pass filters the five conserved variables from an
+// unfiltered copy (fn, free between steps) and leaves the primitives as they are, as the
+// reference does; the shock filter first runs comput_flow_variables (krk = 0 of k_rk_prims).
+template <int NS>
+void filter_t(int istep, int nf, const double* F) {
+  const ocfd_params& P = L->P;
+  const int nn3[3] = {P.nx, P.ny, P.nz};
+  const long long N = L->hc.N;
+  for (int m = 0; m < nf; m++) {
+    const double* c = F + 100 * m;
+    if (istep % (int)std::lround(c[0]) != 0) continue;
+    int b[3][2];
+    for (int d = 0; d < 3; d++) {  // global -> local index of the single rank (:34-39)
+      b[d][0] = std::max((int)std::lround(c[4 + 2 * d]), 1);
+      b[d][1] = std::min((int)std::lround(c[5 + 2 * d]), nn3[d]);
+    }
+    const int scheme = (int)std::lround(c[10]);
+    const double s0 = c[11], rth = c[12];
+    for (int d = 0; d < 3; d++) {
+      if (std::lround(c[1 + d]) != 1 || (scheme != 1 && scheme != 2)) continue;
+      // the filtered direction keeps 5 (Fo9p) or 3 (shock) points off a non-periodic end
+      const int edge = scheme == 1 ? 5 : 3;
+      FilterBox fb;
+      for (int e = 0; e < 3; e++) { fb.lo[e] = b[e][0]; fb.hi[e] = b[e][1]; }
+      if (P.iperiodic[d] != 1) {
+        fb.lo[d] = std::max(fb.lo[d], edge + 1);
+        fb.hi[d] = std::min(fb.hi[d], nn3[d] - edge);
+      }
+      if (scheme == 2) prims_t<NS>(0, 0.0);  // comput_flow_variables (:208)
+      const long long cells = (long long)std::max(0, fb.hi[0] - fb.lo[0] + 1) *
+                              std::max(0, fb.hi[1] - fb.lo[1] + 1) * std::max(0, fb.hi[2] - fb.lo[2] + 1);
+      if (cells == 0) continue;
+      CK(cudaMemcpyAsync(L->fn, L->f, sizeof(double) * 5 * N, cudaMemcpyDeviceToDevice, L->st));
+      KTimer t(KC_OTHER);
+      const unsigned nb = nblk(cells, 256);
+      if (scheme == 1) {
+        if (d == 0) k_filter_fo9p<0><<<nb, 256, 0, L->st>>>(L->f, L->fn, fb, s0);
+        else if (d == 1) k_filter_fo9p<1><<<nb, 256, 0, L->st>>>(L->f, L->fn, fb, s0);
+        else k_filter_fo9p<2><<<nb, 256, 0, L->st>>>(L->f, L->fn, fb, s0);
+      } else {
+        if (d == 0) k_filter_shock<0><<<nb, 256, 0, L->st>>>(L->f, L->fn, L->p, fb, s0, rth);
+        else if (d == 1) k_filter_shock<1><<<nb, 256, 0, L->st>>>(L->f, L->fn, L->p, fb, s0, rth);
+        else k_filter_shock<2><<<nb, 256, 0, L->st>>>(L->f, L->fn, L->p, fb, s0, rth);
+      }
+      LAUNCH_CHECK();
+    }
+  }
+}
+
+double* ana_partials(size_t n) {
+  if (L->ana_part_n < n) {
+    if (L->ana_part) CK(cudaFree(L->ana_part));
+    L->ana_part = nullptr;
+    CK(cudaMalloc(&L->ana_part, sizeof(double) * n));
+    L->ana_part_n = n;
+  }
+  return L->ana_part;
+}
+inline double hp3(double x) { double a = x * x; return a * x; }
+inline double hp4(double x) { double a = x * x; return a * a; }
+
 double wall_ht(double tt) {
   // get_ht_multifrequancy (OCFD_BC_Boundarylayers.f90:579-618), evaluated on the host
   const double PI = 3.14159265358979;
@@ -714,6 +790,9 @@ void release() {
   if (L->gexec) cudaGraphExecDestroy(L->gexec);
   for (auto& e : L->ev_pool) { cudaEventDestroy(e.first); cudaEventDestroy(e.second); }
   if (L->arena) cudaFree(L->arena);
+  if (L->amu_keep) cudaFree(L->amu_keep);
+  if (L->ana_part) cudaFree(L->ana_part);
+  if (L->avg) cudaFree(L->avg);
   if (L->shost) cudaFreeHost(L->shost);
   if (L->ht_host) cudaFreeHost(L->ht_host);
   if (L->b_di) cudaFree(L->b_di);
@@ -1705,6 +1784,155 @@ int ocfd_gpu_stats(long long* neg_et, long long* newton_fail) {
     CK(cudaStreamSynchronize(L->st));
     if (neg_et) *neg_et = (long long)L->shost->neg_total;
     if (newton_fail) *newton_fail = L->shost->newton_fail;
+    return 0;
+  });
+}
+
+int ocfd_gpu_filtering(int istep, int nfiltering, const double* filter, int* applied) {
+  return guarded([&]() -> int {
+    if (applied) *applied = 0;
+    if (!L || !L->flow_ready) { g_err = "state not initialised"; return OCFD_ERR_STATE; }
+    if (nfiltering < 0 || nfiltering > 10 || (nfiltering > 0 && !filter)) {
+      g_err = "NFiltering must be 0..10 with a Filter table";
+      return OCFD_ERR_PARAM;
+    }
+    bool any = false;
+    for (int m = 0; m < nfiltering; m++) {
+      const long cad = std::lround(filter[100 * m]);
+      if (cad < 1) { g_err = "filter step interval Filter(1,m) must be >= 1"; return OCFD_ERR_PARAM; }
+      if (istep % cad == 0) any = true;
+    }
+    if (!any) return 0;
+    NS_DISPATCH(L->NS, filter_t<NSV>(istep, nfiltering, filter));
+    if (applied) *applied = 1;
+    return check_status();
+  });
+}
+
+int ocfd_gpu_keep_viscosity(int on) {
+  return guarded([&]() -> int {
+    if (!L || !L->d) { g_err = "ocfd_gpu_init first"; return OCFD_ERR_STATE; }
+    const bool want = on != 0;
+    if (want && L->NS == 1 && !L->amu_keep) {
+      CK(cudaMalloc(&L->amu_keep, sizeof(double) * L->hc.N));
+      CK(cudaMemsetAsync(L->amu_keep, 0, sizeof(double) * L->hc.N, L->st));
+    }
+    if (L->keep_amu != want) {
+      L->keep_amu = want;
+      if (L->gexec) { CK(cudaGraphExecDestroy(L->gexec)); L->gexec = nullptr; }
+    }
+    return 0;
+  });
+}
+
+int ocfd_gpu_ana_box(double tt, double* out) {
+  return guarded([&]() -> int {
+    if (!L || !L->flow_ready) { g_err = "state not initialised"; return OCFD_ERR_STATE; }
+    if (!out) { g_err = "out is NULL"; return OCFD_ERR_PARAM; }
+    if (L->NS == 1 && !L->keep_amu) {
+      g_err = "ana_box averages the stage viscosity: call ocfd_gpu_keep_viscosity(1) before the steps";
+      return OCFD_ERR_STATE;
+    }
+    const long long N = L->hc.N;
+    const unsigned nb = nblk(N, 256);
+    double* part = ana_partials((size_t)13 * nb);
+    exchange({L->u}, 7);  // exchange_boundary_xyz(u) (OCFD_ANA.f90:214)
+    const double* amu = L->NS == 1 ? L->amu_keep : L->amu;
+    if (L->sep) k_ana_box<true><<<nb, 256, 0, L->st>>>(L->d, L->u, L->v, L->w, L->T, L->p, L->Et[L->cur], amu, part, L->geo);
+    else k_ana_box<false><<<nb, 256, 0, L->st>>>(L->d, L->u, L->v, L->w, L->T, L->p, L->Et[L->cur], amu, part, L->geo);
+    LAUNCH_CHECK();
+    std::vector<double> h((size_t)13 * nb);
+    CK(cudaMemcpyAsync(h.data(), part, sizeof(double) * h.size(), cudaMemcpyDeviceToHost, L->st));
+    CK(cudaStreamSynchronize(L->st));
+    double sm[13] = {};
+    for (unsigned b = 0; b < nb; b++)
+      for (int m = 0; m < 13; m++) sm[m] = sm[m] + h[(size_t)13 * b + m];
+    const double nn = (double)L->P.nx * L->P.ny * L->P.nz;
+    for (double& x : sm) x = x / nn;
+    k_ana_drms<<<nb, 256, 0, L->st>>>(L->d, sm[6], part);
+    LAUNCH_CHECK();
+    CK(cudaMemcpyAsync(h.data(), part, sizeof(double) * nb, cudaMemcpyDeviceToHost, L->st));
+    CK(cudaStreamSynchronize(L->st));
+    double drs = 0.0;
+    for (unsigned b = 0; b < nb; b++) drs = drs + h[b];
+    // OCFD_ANA.f90:260-286
+    double u_rms = sm[0], v_rms = sm[1], w_rms = sm[2], ux_rms = sm[3], ux_sk = sm[4], ux_fl = sm[5];
+    const double d_aver = sm[6], c_aver = sm[7], amu_aver = sm[8], ek = sm[9], T_aver = sm[10];
+    double u_sk = sm[11], u_fl = sm[12];
+    const double vv_rms = std::sqrt((u_rms + v_rms + w_rms) / 3.0);
+    const double amt = std::sqrt(u_rms + v_rms + w_rms) / c_aver;
+    u_rms = std::sqrt(u_rms); v_rms = std::sqrt(v_rms); w_rms = std::sqrt(w_rms); ux_rms = std::sqrt(ux_rms);
+    const double alamda = vv_rms / ux_rms, alamdax = u_rms / ux_rms;
+    const double re_l = vv_rms * alamda * d_aver / amu_aver, re_lx = vv_rms * alamdax * d_aver / amu_aver;
+    ux_sk = ux_sk / hp3(ux_rms); ux_fl = ux_fl / hp4(ux_rms);
+    u_sk = u_sk / hp3(u_rms); u_fl = u_fl / hp4(u_rms);
+    const double d_rms = std::sqrt(drs / nn);
+    const double o[19] = {tt, re_l, re_lx, amt, vv_rms, u_rms, v_rms, w_rms, u_sk, u_fl, ux_sk, ux_fl, ek, d_rms,
+                          T_aver, amu_aver, d_aver, ux_rms, alamdax};
+    for (int m = 0; m < 19; m++) out[m] = o[m];
+    return check_status();
+  });
+}
+
+int ocfd_gpu_ana_q(double* q) {
+  return guarded([&]() -> int {
+    if (!L || !L->flow_ready) { g_err = "state not initialised"; return OCFD_ERR_STATE; }
+    if (!q) { g_err = "q is NULL"; return OCFD_ERR_PARAM; }
+    const long long N = L->hc.N;
+    exchange({L->u, L->v, L->w}, 7);
+    // du is scratch between steps
+    if (L->sep) k_ana_q<true><<<nblk(N, 256), 256, 0, L->st>>>(L->u, L->v, L->w, L->du, L->geo);
+    else k_ana_q<false><<<nblk(N, 256), 256, 0, L->st>>>(L->u, L->v, L->w, L->du, L->geo);
+    LAUNCH_CHECK();
+    CK(cudaMemcpyAsync(q, L->du, sizeof(double) * N, cudaMemcpyDeviceToHost, L->st));
+    CK(cudaStreamSynchronize(L->st));
+    return 0;
+  });
+}
+
+int ocfd_gpu_ana_time_average(double dt, int* k_average, double* t_average) {
+  return guarded([&]() -> int {
+    if (!L || !L->flow_ready) { g_err = "state not initialised"; return OCFD_ERR_STATE; }
+    const long long N = L->hc.N;
+    const size_t n = (size_t)(5 + L->NS) * N;
+    if (!L->avg) {  // first call with nothing uploaded: start from zero (:80-88)
+      CK(cudaMalloc(&L->avg, sizeof(double) * n));
+      CK(cudaMemsetAsync(L->avg, 0, sizeof(double) * n, L->st));
+      L->k_average = 0;
+      L->t_average = 0.0;
+    }
+    const double K = (double)L->k_average;
+    NS_DISPATCH(L->NS, (k_ana_average<NSV><<<nblk(N, 256), 256, 0, L->st>>>(L->d, L->u, L->v, L->w, L->T, L->di,
+                                                                              L->avg, K)));
+    LAUNCH_CHECK();
+    L->k_average = L->k_average + 1;
+    L->t_average = L->t_average + dt;
+    if (k_average) *k_average = L->k_average;
+    if (t_average) *t_average = L->t_average;
+    return 0;
+  });
+}
+
+int ocfd_gpu_ana_average(int upload, double* fields, int* k_average, double* t_average) {
+  return guarded([&]() -> int {
+    if (!L || !L->flow_ready) { g_err = "state not initialised"; return OCFD_ERR_STATE; }
+    const size_t n = (size_t)(5 + L->NS) * L->hc.N;
+    if (upload) {
+      if (!fields || !k_average || !t_average) { g_err = "upload needs fields, K_average and t_average"; return OCFD_ERR_PARAM; }
+      if (!L->avg) CK(cudaMalloc(&L->avg, sizeof(double) * n));
+      CK(cudaMemcpyAsync(L->avg, fields, sizeof(double) * n, cudaMemcpyHostToDevice, L->st));
+      CK(cudaStreamSynchronize(L->st));
+      L->k_average = *k_average;
+      L->t_average = *t_average;
+      return 0;
+    }
+    if (!L->avg) { g_err = "no time average accumulated"; return OCFD_ERR_STATE; }
+    if (fields) {
+      CK(cudaMemcpyAsync(fields, L->avg, sizeof(double) * n, cudaMemcpyDeviceToHost, L->st));
+      CK(cudaStreamSynchronize(L->st));
+    }
+    if (k_average) *k_average = L->k_average;
+    if (t_average) *t_average = L->t_average;
     return 0;
   });
 }

@@ -127,6 +127,12 @@ GPU_SIGNATURES = {
     "ocfd_gpu_init_state": (I, [PD, PD, D]),
     "ocfd_gpu_run": (I, [D, D, I, I, I]),
     "ocfd_gpu_chem_setup": (I, [C.POINTER(Thermo), C.POINTER(Kinetics), I, I]),
+    "ocfd_gpu_filtering": (I, [I, I, PD, PI]),
+    "ocfd_gpu_keep_viscosity": (I, [I]),
+    "ocfd_gpu_ana_box": (I, [D, PD]),
+    "ocfd_gpu_ana_q": (I, [PD]),
+    "ocfd_gpu_ana_time_average": (I, [D, PI, PD]),
+    "ocfd_gpu_ana_average": (I, [I, PD, PI, PD]),
     "ocfd_gpu_autotune": (I, [I, PI, PD]),
     "ocfd_gpu_set_tiles": (I, [PI]),
     "ocfd_gpu_get_tiles": (I, [PI]),

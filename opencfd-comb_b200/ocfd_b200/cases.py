@@ -53,6 +53,8 @@ class Case:
         self.nsteps = 1
         self.if_reaction = 0
         self.nsub = 1
+        self.filters = []    # filter groups (post.filter_table), applied after every step
+        self.analysis = []   # analysis entries (post.ana_table), OCFD_analysis after every step
 
     @property
     def shape(self):
@@ -70,11 +72,12 @@ class Case:
     def save(self, path):
         """Writes the case file read by the compiled host driver (host/ns_solver.cpp): the ABI
         records as bytes, then dt / nsteps / chemistry switch / sub-steps, grid, initial
-        primitives, species densities and the boundary tables."""
+        primitives, species densities, the boundary tables, and the filter and analysis tables
+        (Para%Filter, Para%ANA_Para)."""
         import struct
         with open(path, "wb") as fh:
             fh.write(b"OCFDCASE")
-            fh.write(struct.pack("<5i", 1, C.sizeof(abi.Params), C.sizeof(abi.Thermo), C.sizeof(abi.Kinetics),
+            fh.write(struct.pack("<5i", 2, C.sizeof(abi.Params), C.sizeof(abi.Thermo), C.sizeof(abi.Kinetics),
                                  C.sizeof(abi.Transport)))
             fh.write(bytes(self.params))
             fh.write(bytes(self.thermo))
@@ -99,6 +102,13 @@ class Case:
                     a = np.zeros(0) if a is None else np.ascontiguousarray(a, dtype=np.float64).ravel()
                     fh.write(struct.pack("<q", a.size))
                     fh.write(a.tobytes())
+            from . import post
+            ft, nf = post.filter_table(self.filters)
+            at, na = post.ana_table(self.analysis)
+            fh.write(struct.pack("<i", nf))
+            fh.write(np.ascontiguousarray(ft).tobytes())
+            fh.write(struct.pack("<i", na))
+            fh.write(np.ascontiguousarray(at).tobytes())
 
     def bcdata(self):
         """abi.BcData pointing at this case's arrays (kept alive by the case)."""

@@ -227,3 +227,39 @@ def read_restart(path, nx, ny, nz, nfields):
             arr[:, :, k] = np.frombuffer(recs[1 + m * nz + k], dtype=np.float64).reshape((nx, ny), order="F")
         fields.append(arr)
     return istep, tt, fields
+
+
+def _write_planes(fh, a):
+    """write_3d (OCFD_IO_mpi.f90:232): one record of nx*ny doubles per k plane; a is (nz, ny, nx)
+    in C order, whose planes are the Fortran (nx, ny) column-major planes."""
+    a = np.ascontiguousarray(a, dtype=np.float64)
+    for k in range(a.shape[0]):
+        b = a[k].tobytes()
+        fh.write(struct.pack("<i", len(b))); fh.write(b); fh.write(struct.pack("<i", len(b)))
+
+
+def write_3d_records(path, arrays):
+    """Files written by write_3d alone, e.g. Q-<Istep>.dat of ana_getQ (OCFD_ANA.f90:183-188)."""
+    with open(path, "wb") as fh:
+        for a in arrays:
+            _write_planes(fh, a)
+
+
+def write_average(path, k_average, t_average, fields):
+    """OCFD-comb<Istep>.dat.average of ana_time_average (OCFD_ANA.f90:119-139): header record
+    (int32 K_average, real64 t_average), then dm, um, vm, wm, Tm and every diav as write_3d."""
+    with open(path, "wb") as fh:
+        hdr = struct.pack("<id", k_average, t_average)
+        fh.write(struct.pack("<i", len(hdr))); fh.write(hdr); fh.write(struct.pack("<i", len(hdr)))
+        for a in fields:
+            _write_planes(fh, a)
+
+
+def read_average(path, nx, ny, nz, nfields):
+    recs = read_records(path)
+    k_average, t_average = struct.unpack("<id", recs[0])
+    out = np.empty((nfields, nz, ny, nx))
+    for m in range(nfields):
+        for k in range(nz):
+            out[m, k] = np.frombuffer(recs[1 + m * nz + k], dtype=np.float64).reshape(ny, nx)
+    return k_average, t_average, out

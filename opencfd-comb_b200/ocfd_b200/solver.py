@@ -114,6 +114,48 @@ class Solver:
         _chk(lib().ocfd_gpu_stats(C.byref(a), C.byref(b)))
         return a.value, b.value
 
+    # ---- filtering and analysis (code/others/OCFD_filtering.f90, OCFD_ANA.f90) ----
+    def filtering(self, istep, table, nfiltering):
+        """filtering after step istep (OCFD_NS_Solver.f90:48); table from post.filter_table.
+        Returns 1 when a filter group ran."""
+        t = np.ascontiguousarray(table, dtype=np.float64)
+        applied = C.c_int()
+        _chk(lib().ocfd_gpu_filtering(istep, nfiltering, abi.dptr(t), C.byref(applied)))
+        return applied.value
+
+    def keep_viscosity(self, on=True):
+        _chk(lib().ocfd_gpu_keep_viscosity(1 if on else 0))
+
+    def ana_box(self, tt=None):
+        out = np.empty(19)
+        _chk(lib().ocfd_gpu_ana_box(self.tt if tt is None else tt, abi.dptr(out)))
+        return out
+
+    def ana_q(self):
+        nx, ny, nz = self.case.shape
+        q = np.empty((nz, ny, nx))
+        _chk(lib().ocfd_gpu_ana_q(abi.dptr(q)))
+        return q
+
+    def ana_time_average(self, dt):
+        k, t = C.c_int(), C.c_double()
+        _chk(lib().ocfd_gpu_ana_time_average(dt, C.byref(k), C.byref(t)))
+        return k.value, t.value
+
+    def ana_average(self, upload=None):
+        """Downloads (fields, K_average, t_average); upload=(fields, K, t) restores them."""
+        nx, ny, nz = self.case.shape
+        nf = 5 + self.case.params.n_spec
+        if upload is not None:
+            f = np.ascontiguousarray(upload[0], dtype=np.float64).reshape(nf, nz, ny, nx)
+            k, t = C.c_int(int(upload[1])), C.c_double(float(upload[2]))
+            _chk(lib().ocfd_gpu_ana_average(1, abi.dptr(f), C.byref(k), C.byref(t)))
+            return None
+        a = np.empty((nf, nz, ny, nx))
+        k, t = C.c_int(), C.c_double()
+        _chk(lib().ocfd_gpu_ana_average(0, abi.dptr(a), C.byref(k), C.byref(t)))
+        return a, k.value, t.value
+
     # ---- stencil tiles ----
     def autotune(self, reps=5):
         """Times the candidate tile shapes on the current state and applies the fastest; returns

@@ -25,7 +25,10 @@
  *   code/flow-solver/OCFD_mesh.f90          init_mesh :1-57, comput_Jacobian3d :60-107, updata_Axyz_periodic :109-185
  *   code/mpi-io/OCFD_mpi.f90                exchange_boundary_x/y/z :201-236 (single rank: periodic copy)
  *   code/mpi-io/OCFD_readpara.f90           set_parameters :347-409, set_scheme_para :424-431
+ *   code/others/OCFD_filtering.f90          filtering :4-72, Fo9p filters :78-189, shock filters :194-360
+ *   code/others/OCFD_ANA.f90                ana_time_average :39-140, ana_getQ :143-190, ana_box :197-303
  */
+#include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <string>
@@ -1195,6 +1198,217 @@ struct Oracle {
     return 0;
   }
 
+  /* ---------------- filtering (code/others/OCFD_filtering.f90) ---------------- */
+  /* F = Para%Filter(100,10) column-major: group m's parameters at F[100 m + 0..12] */
+  int filtering(int istep, int nfilt, const double* F, int* applied) {
+    if (applied) *applied = 0;
+    if (nfilt < 0 || nfilt > 10) { err = "NFiltering must be 0..10"; return OCFD_ERR_PARAM; }
+    for (int m = 0; m < nfilt; m++)
+      if (std::lround(F[100 * m]) < 1) { err = "filter step interval must be >= 1"; return OCFD_ERR_PARAM; }
+    int any = 0;
+    for (int m = 0; m < nfilt; m++)
+      if (istep % (int)std::lround(F[100 * m]) == 0) any = 1;
+    if (!any) return 0;
+    if (applied) *applied = 1;
+    for (int m = 0; m < nfilt; m++) {
+      const double* c = F + 100 * m;
+      if (istep % (int)std::lround(c[0]) != 0) continue;
+      const int fdir[3] = {(int)std::lround(c[1]), (int)std::lround(c[2]), (int)std::lround(c[3])};
+      int b[3][2];
+      const int nn3[3] = {nx, ny, nz};
+      for (int d = 0; d < 3; d++) {
+        b[d][0] = std::max((int)std::lround(c[4 + 2 * d]), 1);
+        b[d][1] = std::min((int)std::lround(c[5 + 2 * d]), nn3[d]);
+      }
+      const int scheme = (int)std::lround(c[10]);
+      const double s0 = c[11], rth = c[12];
+      for (int d = 0; d < 3; d++) {
+        if (fdir[d] != 1) continue;
+        if (scheme == 1) filter_fo9p(d, s0, b);
+        else if (scheme == 2) {
+          int e = filter_shock(d, s0, rth, b);
+          if (e) return e;
+        }
+      }
+    }
+    return 0;
+  }
+  /* filter_x3d / filter_y3d / filter_z3d (:78-189): f0 is a fresh halo array (its halo is only
+   * read where the exchange filled it), f is overwritten component by component */
+  void filter_fo9p(int dir, double s0, const int (&b)[3][2]) {
+    const double d0 = 0.243527493120, d1 = -0.204788880640, d2 = 0.120007591680, d3 = -0.045211119360,
+                 d4 = 0.008228661760;
+    const int n = dir == 0 ? nx : (dir == 1 ? ny : nz);
+    int lo[3] = {b[0][0], b[1][0], b[2][0]}, hi[3] = {b[0][1], b[1][1], b[2][1]};
+    if (P.iperiodic[dir] != 1) { lo[dir] = std::max(lo[dir], 6); hi[dir] = std::min(hi[dir], n - 5); }
+    const long s = dir == 0 ? 1 : (dir == 1 ? HX : HX * HY);
+    std::vector<double> f0(H, std::nan(""));
+    for (int m = 0; m < 5; m++) {
+      for (int k = 1; k <= nz; k++)
+        for (int j = 1; j <= ny; j++)
+          for (int i = 1; i <= nx; i++) f0[ih(i, j, k)] = f[(long)m * N + in(i, j, k)];
+      if (dir == 0) exch_x(f0.data());
+      else if (dir == 1) exch_y(f0.data());
+      else exch_z(f0.data());
+      for (int k = lo[2]; k <= hi[2]; k++)
+        for (int j = lo[1]; j <= hi[1]; j++)
+          for (int i = lo[0]; i <= hi[0]; i++) {
+            const double* q = f0.data() + ih(i, j, k);
+            f[(long)m * N + in(i, j, k)] =
+                q[0] - s0 * (d0 * q[0] + d1 * (q[-s] + q[s]) + d2 * (q[-2 * s] + q[2 * s]) + d3 * (q[-3 * s] + q[3 * s]) +
+                             d4 * (q[-4 * s] + q[4 * s]));
+          }
+    }
+  }
+  /* filter_x3d_shock / _y3d_ / _z3d_ (:194-360) */
+  int filter_shock(int dir, double s0, double rth, const int (&b)[3][2]) {
+    const double c1 = -0.210383, c2 = 0.039617;
+    const int n = dir == 0 ? nx : (dir == 1 ? ny : nz);
+    int lo[3] = {b[0][0], b[1][0], b[2][0]}, hi[3] = {b[0][1], b[1][1], b[2][1]};
+    if (P.iperiodic[dir] != 1) { lo[dir] = std::max(lo[dir], 4); hi[dir] = std::min(hi[dir], n - 3); }
+    int e = comput_flow_variables();
+    if (e) return e;
+    if (dir == 0) exch_x(p.data());
+    else if (dir == 1) exch_y(p.data());
+    else exch_z(p.data());
+    const long s = dir == 0 ? 1 : (dir == 1 ? HX : HX * HY);
+    std::vector<double> f0(H, std::nan("")), sc0(n + 2);
+    for (int m = 0; m < 5; m++) {
+      for (int k = 1; k <= nz; k++)
+        for (int j = 1; j <= ny; j++)
+          for (int i = 1; i <= nx; i++) f0[ih(i, j, k)] = f[(long)m * N + in(i, j, k)];
+      if (dir == 0) exch_x(f0.data());
+      else if (dir == 1) exch_y(f0.data());
+      else exch_z(f0.data());
+      /* one line at a time: the two cross indices run over the box, the line index over
+       * lo-1 .. hi+1 for sc0 and lo .. hi for the update */
+      const int a0 = dir == 0 ? 1 : 0, a1 = dir == 2 ? 1 : 2;
+      for (int cb = lo[a1]; cb <= hi[a1]; cb++)
+        for (int ca = lo[a0]; ca <= hi[a0]; ca++) {
+          auto at = [&](int t) {
+            int ijk[3];
+            ijk[dir] = t; ijk[a0] = ca; ijk[a1] = cb;
+            return ih(ijk[0], ijk[1], ijk[2]);
+          };
+          for (int t = lo[dir] - 1; t <= hi[dir] + 1; t++) {
+            const double* pq = p.data() + at(t);
+            double dp0 = 0.25 * (-pq[s] + 2.0 * pq[0] - pq[-s]);
+            double dp1 = 0.25 * (-pq[2 * s] + 2.0 * pq[s] - pq[0]);
+            double dp2 = 0.25 * (-pq[0] + 2.0 * pq[-s] - pq[-2 * s]);
+            double ri = 0.5 * (p2(dp0 - dp1) + p2(dp0 - dp2)) / (pq[0] * pq[0]) + 1.0e-16;
+            sc0[t] = 0.5 * (1.0 - rth / ri + std::fabs(1.0 - rth / ri));
+          }
+          for (int t = lo[dir]; t <= hi[dir]; t++) {
+            double sc1 = 0.5 * (sc0[t] + sc0[t + 1]);
+            double sc2 = 0.5 * (sc0[t] + sc0[t - 1]);
+            const long qh = at(t);
+            const double* q = f0.data() + qh;
+            int ijk[3];
+            ijk[dir] = t; ijk[a0] = ca; ijk[a1] = cb;
+            f[(long)m * N + in(ijk[0], ijk[1], ijk[2])] =
+                q[0] - s0 * (sc1 * (c1 * (q[s] - q[0]) + c2 * (q[2 * s] - q[-s])) -
+                             sc2 * (c1 * (q[0] - q[-s]) + c2 * (q[s] - q[-2 * s])));
+          }
+        }
+    }
+    return 0;
+  }
+
+  /* ---------------- OCFD_analysis pieces (code/others/OCFD_ANA.f90) ---------------- */
+  /* ana_box (:197-303): out = tt, Re_lamda, Re_lamdax, Amt, vv_rms, u_rms, v_rms, w_rms,
+   * u_skewness, u_flatness, ux_skewness, ux_flatness, E_kinetic, d_rms, T_aver, Amu_aver, d_aver,
+   * Ux_rms, Alamdax; sums in the reference's serial loop order */
+  void ana_box(double tt, double* out) {
+    exch(u.data());
+    std::vector<double> uk(N), ui(N), us(N);
+    dxyz(0, u.data(), uk.data()); dxyz(1, u.data(), ui.data()); dxyz(2, u.data(), us.data());
+    double c_aver = 0, d_aver = 0, amu_aver = 0, T_aver = 0, u_rms = 0, v_rms = 0, w_rms = 0, ux_rms = 0,
+           ux_sk = 0, ux_fl = 0, u_sk = 0, u_fl = 0, ek = 0;
+    for (int k = 1; k <= nz; k++)
+      for (int j = 1; j <= ny; j++)
+        for (int i = 1; i <= nx; i++) {
+          long q = ih(i, j, k), a = in(i, j, k);
+          double ux = uk[a] * M[M_AKX][q] + ui[a] * M[M_AIX][q] + us[a] * M[M_ASX][q];
+          double gamma = p[q] / Et[q] + 1.0;
+          double c1 = std::sqrt(gamma * p[q] / d[q]);
+          c_aver = c_aver + c1;
+          d_aver = d_aver + d[q];
+          amu_aver = amu_aver + Amu[a];
+          T_aver = T_aver + T[q];
+          u_rms = u_rms + u[q] * u[q];
+          v_rms = v_rms + v[q] * v[q];
+          w_rms = w_rms + w[q] * w[q];
+          ux_rms = ux_rms + ux * ux;
+          ux_sk = ux_sk + p3(ux);
+          ux_fl = ux_fl + p4(ux);
+          u_sk = u_sk + p3(u[q]);
+          u_fl = u_fl + p4(u[q]);
+          ek = ek + (u[q] * u[q] + v[q] * v[q] + w[q] * w[q]) * d[q] * 0.5;
+        }
+    double sums[13] = {u_rms, v_rms, w_rms, ux_rms, ux_sk, ux_fl, d_aver, c_aver, amu_aver, ek, T_aver, u_sk, u_fl};
+    const double nn = (double)((long)nx * ny * nz);
+    for (double& x : sums) x = x / nn;
+    double d_rms = 0.0;
+    for (int k = 1; k <= nz; k++)
+      for (int j = 1; j <= ny; j++)
+        for (int i = 1; i <= nx; i++) d_rms = d_rms + p2(d[ih(i, j, k)] - sums[6]);
+    ana_box_finish(tt, sums, d_rms, nn, out);
+  }
+  static void ana_box_finish(double tt, const double* s, double d_rms_sum, double nn, double* out) {
+    double u_rms = s[0], v_rms = s[1], w_rms = s[2], ux_rms = s[3], ux_sk = s[4], ux_fl = s[5], d_aver = s[6],
+           c_aver = s[7], amu_aver = s[8], ek = s[9], T_aver = s[10], u_sk = s[11], u_fl = s[12];
+    double vv_rms = std::sqrt((u_rms + v_rms + w_rms) / 3.0);
+    double amt = std::sqrt(u_rms + v_rms + w_rms) / c_aver;
+    u_rms = std::sqrt(u_rms); v_rms = std::sqrt(v_rms); w_rms = std::sqrt(w_rms); ux_rms = std::sqrt(ux_rms);
+    double alamda = vv_rms / ux_rms, alamdax = u_rms / ux_rms;
+    double re_l = vv_rms * alamda * d_aver / amu_aver, re_lx = vv_rms * alamdax * d_aver / amu_aver;
+    ux_sk = ux_sk / p3(ux_rms); ux_fl = ux_fl / p4(ux_rms);
+    u_sk = u_sk / p3(u_rms); u_fl = u_fl / p4(u_rms);
+    double d_rms = std::sqrt(d_rms_sum / nn);
+    const double o[19] = {tt, re_l, re_lx, amt, vv_rms, u_rms, v_rms, w_rms, u_sk, u_fl, ux_sk, ux_fl, ek, d_rms,
+                          T_aver, amu_aver, d_aver, ux_rms, alamdax};
+    for (int m = 0; m < 19; m++) out[m] = o[m];
+  }
+  /* ana_getQ (:143-190): Q = II of the velocity gradient, interior array */
+  void ana_q(double* tk) {
+    exch(u.data()); exch(v.data()); exch(w.data());
+    std::vector<double> g[9];
+    for (auto& x : g) x.resize(N);
+    const double* vel[3] = {u.data(), v.data(), w.data()};
+    for (int c = 0; c < 3; c++)
+      for (int d = 0; d < 3; d++) dxyz(d, vel[c], g[3 * c + d].data());
+    for (int k = 1; k <= nz; k++)
+      for (int j = 1; j <= ny; j++)
+        for (int i = 1; i <= nx; i++) {
+          long q = ih(i, j, k), a = in(i, j, k);
+          auto dd = [&](int c, int x) {  /* d(vel c)/d(x): uk*Akx + ui*Aix + us*Asx for x */
+            return g[3 * c][a] * M[M_AKX + x][q] + g[3 * c + 1][a] * M[M_AIX + x][q] + g[3 * c + 2][a] * M[M_ASX + x][q];
+          };
+          double ux = dd(0, 0), vx = dd(1, 0), wx = dd(2, 0), uy = dd(0, 1), vy = dd(1, 1), wy = dd(2, 1);
+          double uz = dd(0, 2), vz = dd(1, 2), wz = dd(2, 2);
+          tk[a] = ux * vy + ux * wz + vy * wz - uy * vx - uz * wx - vz * wy;
+        }
+  }
+  /* ana_time_average (:39-140): running means of d, u, v, w, T, di(m), interior arrays */
+  std::vector<double> avg;
+  int k_average = 0;
+  double t_average = 0.0;
+  void ana_time_average(double dt) {
+    if (avg.empty()) avg.assign((size_t)(5 + NS) * N, 0.0);
+    const double K = (double)k_average;
+    for (int k = 1; k <= nz; k++)
+      for (int j = 1; j <= ny; j++)
+        for (int i = 1; i <= nx; i++) {
+          long q = ih(i, j, k), a = in(i, j, k);
+          const double* src[5] = {d.data(), u.data(), v.data(), w.data(), T.data()};
+          for (int m = 0; m < 5; m++) avg[(long)m * N + a] = (K * avg[(long)m * N + a] + src[m][q]) / (K + 1.0);
+          for (int m = 0; m < NS; m++)
+            avg[(long)(5 + m) * N + a] = (K * avg[(long)(5 + m) * N + a] + di[(long)m * H + q]) / (K + 1.0);
+        }
+    k_average = k_average + 1;
+    t_average = t_average + dt;
+  }
+
   /* nsub x Chemical_time_advance + comput_T_P */
   int chem_advance(double dt2, int nsub) {
     if (!ch.have_kin) { err = "no kinetics"; return OCFD_ERR_PARAM; }
@@ -1405,6 +1619,37 @@ int ocfd_cpu_set_threads(int n) {
 
 long long ocfd_cpu_neg_et(void) { return g ? g->neg_et : 0; }
 const char* ocfd_cpu_last_error(void) { return g_err.c_str(); }
+/* filtering after step istep (OCFD_NS_Solver.f90:48); filter = Para%Filter(100,10) */
+int ocfd_cpu_filtering(int istep, int nfiltering, const double* filter, int* applied) {
+  if (!g) return OCFD_ERR_STATE;
+  int e = g->filtering(istep, nfiltering, filter, applied);
+  if (e) g_err = g->err;
+  return e;
+}
+int ocfd_cpu_ana_box(double tt, double* out) {
+  if (!g) return OCFD_ERR_STATE;
+  g->ana_box(tt, out);
+  return 0;
+}
+int ocfd_cpu_ana_q(double* q) {
+  if (!g) return OCFD_ERR_STATE;
+  g->ana_q(q);
+  return 0;
+}
+int ocfd_cpu_ana_time_average(double dt, int* k_average, double* t_average) {
+  if (!g) return OCFD_ERR_STATE;
+  g->ana_time_average(dt);
+  if (k_average) *k_average = g->k_average;
+  if (t_average) *t_average = g->t_average;
+  return 0;
+}
+int ocfd_cpu_ana_average_download(double* fields) {
+  if (!g) return OCFD_ERR_STATE;
+  if (g->avg.empty()) return OCFD_ERR_STATE;
+  std::memcpy(fields, g->avg.data(), sizeof(double) * g->avg.size());
+  return 0;
+}
+
 int ocfd_cpu_finalize(void) {
   delete g;
   g = nullptr;

@@ -51,6 +51,11 @@ def lib():
                                              C.c_double, C.c_double, C.c_double, PD]),
             "ocfd_cpu_split": (C.c_int, [C.c_int, PD, PD, PD]),
             "ocfd_cpu_gauss": (C.c_int, [C.c_int, PD, PD, PD]),
+            "ocfd_cpu_filtering": (C.c_int, [C.c_int, C.c_int, PD, PI]),
+            "ocfd_cpu_ana_box": (C.c_int, [C.c_double, PD]),
+            "ocfd_cpu_ana_q": (C.c_int, [PD]),
+            "ocfd_cpu_ana_time_average": (C.c_int, [C.c_double, PI, PD]),
+            "ocfd_cpu_ana_average_download": (C.c_int, [PD]),
             "ocfd_cpu_neg_et": (C.c_longlong, []),
             "ocfd_cpu_last_error": (C.c_char_p, []),
             "ocfd_cpu_finalize": (C.c_int, []),
@@ -127,6 +132,36 @@ class OracleSolver:
         e, k = C.c_double(), C.c_double()
         _chk(lib().ocfd_cpu_diag(C.byref(e), C.byref(k)))
         return e.value, k.value
+
+    # ---- filtering and analysis (code/others/OCFD_filtering.f90, OCFD_ANA.f90) ----
+    def filtering(self, istep, table, nfiltering):
+        """table: Para%Filter as a (10, 100) array (row m = filter group m), see post.filter_table."""
+        t = np.ascontiguousarray(table, dtype=np.float64)
+        applied = C.c_int()
+        _chk(lib().ocfd_cpu_filtering(istep, nfiltering, abi.dptr(t), C.byref(applied)))
+        return applied.value
+
+    def ana_box(self, tt):
+        out = np.empty(19)
+        _chk(lib().ocfd_cpu_ana_box(tt, abi.dptr(out)))
+        return out
+
+    def ana_q(self):
+        nx, ny, nz = self.case.shape
+        q = np.empty((nz, ny, nx))
+        _chk(lib().ocfd_cpu_ana_q(abi.dptr(q)))
+        return q
+
+    def ana_time_average(self, dt):
+        k, t = C.c_int(), C.c_double()
+        _chk(lib().ocfd_cpu_ana_time_average(dt, C.byref(k), C.byref(t)))
+        return k.value, t.value
+
+    def ana_average(self):
+        nx, ny, nz = self.case.shape
+        a = np.empty((5 + self.case.params.n_spec, nz, ny, nx))
+        _chk(lib().ocfd_cpu_ana_average_download(abi.dptr(a)))
+        return a
 
     def close(self):
         lib().ocfd_cpu_finalize()

@@ -107,3 +107,45 @@ def test_host_driver_matches_python_driver(tmp_path, make):
     for ln, (e, k) in zip(lines, msgs):
         d = _fields(ln)
         assert float("%.15e" % e) == d["E_mean"] and float("%.15e" % k) == d["K_mean"]
+
+
+@pytest.mark.gpu
+def test_host_driver_filtering_and_analysis(tmp_path):
+    """NS_solver's filtering (:48) and OCFD_analysis (:55) calls from the compiled driver: the
+    final state equals the Python sequence with the same calls, and the statistics rows and the
+    Q / average files match what post.analysis writes for that sequence."""
+    import filecmp
+    from ocfd_b200 import post, solver
+    _need_exe()
+    c = cases.isotropic(n=16)
+    c.nsteps = 4
+    c.filters = [dict(step=2, x=1, y=1, z=1, scheme=post.FILTER_FO9P, s0=0.3),
+                 dict(step=3, z=1, scheme=post.FILTER_SHOCK, s0=1.0, rth=1e-6)]
+    c.analysis = [(post.ANA_BOX, 1), (post.ANA_Q, 4), (post.ANA_TIME_AVERAGE, 1, [2])]
+    run_dir, py_dir = tmp_path / "c", tmp_path / "py"
+    run_dir.mkdir(); py_dir.mkdir()
+    c.save(str(run_dir / "case.bin"))
+    r = subprocess.run([EXE, "case.bin", "state.bin"], capture_output=True, text=True, timeout=600, cwd=str(run_dir))
+    assert r.returncode == 0, r.stderr
+    ft, nf = post.filter_table(c.filters)
+    at, na = post.ana_table(c.analysis)
+    g = solver.Solver(c)
+    g.init_state()
+    g.keep_viscosity(True)
+    tt = 0.0
+    for istep in range(1, c.nsteps + 1):
+        g.flow_time_advance(0.5 * c.dt, tt)
+        g.flow_time_advance(0.5 * c.dt, tt)
+        tt = tt + c.dt
+        g.filtering(istep, ft, nf)
+        post.analysis(g, istep, tt, at, na, outdir=str(py_dir))
+    f, di, prims = g.download_state()
+    g.close()
+    raw = np.fromfile(str(run_dir / "state.bin"), dtype=np.float64)
+    assert np.array_equal(raw[:f.size].reshape(f.shape), f)
+    assert np.array_equal(raw[f.size + di.size:].reshape(prims.shape), prims)
+    for name in ("Q-0000004.dat", "OCFD-comb00000002.dat.average", "OCFD-comb00000004.dat.average"):
+        assert filecmp.cmp(str(run_dir / name), str(py_dir / name), shallow=False), name
+    rows_c = [[float(x) for x in ln.split()] for ln in (run_dir / "statistics.dat").read_text().splitlines()]
+    rows_p = [[float(x) for x in ln.split()] for ln in (py_dir / "statistics.dat").read_text().splitlines()]
+    assert rows_c == rows_p and len(rows_c) == c.nsteps
