@@ -185,6 +185,21 @@ int ocfd_gpu_download_state(double* f, double* di, double* prims);
 /* show_flow_msg reductions (OCFD_Time_Adv.f90:210-223): mean total and kinetic energy. */
 int ocfd_gpu_diag(double* e_mean, double* k_mean);
 
+/* The same without stalling the time loop: _begin enqueues the sums and their copy to pinned
+ * host memory (a copy stream), _end waits for them; steps may run in between (the sums are of
+ * the state at _begin). ocfd_gpu_diag = _begin + _end. */
+int ocfd_gpu_diag_begin(void);
+int ocfd_gpu_diag_end(double* e_mean, double* k_mean);
+
+/* save_flow_data (OCFD_IO.f90:39-64) without a host sync: ocfd_gpu_snapshot packs d, u, v, w, T
+ * and every di (interior arrays, the file's field order) on the device and copies them to pinned
+ * host memory on a copy stream while the next steps run. ocfd_gpu_snapshot_wait waits for the
+ * oldest snapshot in flight and returns its Istep, tt and a pointer to its (5 + N_SPEC) * N doubles;
+ * the pointer stays valid until the second-next ocfd_gpu_snapshot (two slots). A third snapshot
+ * while two are in flight is OCFD_ERR_STATE. */
+int ocfd_gpu_snapshot(int istep, double tt);
+int ocfd_gpu_snapshot_wait(int* istep, double* tt, const double** fields);
+
 /* Downloads the hybrid-scheme sensor Rhybrid (halo array) for decision-map comparisons. */
 int ocfd_gpu_download_rhybrid(double* rhybrid);
 

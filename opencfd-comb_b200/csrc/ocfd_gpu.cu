@@ -93,6 +93,18 @@ struct Lib {
   size_t ana_part_n = 0;
   int k_average = 0;
   double t_average = 0.0;
+  // asynchronous save / show (ocfd_gpu_snapshot*, ocfd_gpu_diag_begin/end): a copy stream, two
+  // snapshot slots (device pack buffer + pinned host buffer; state 0 free, 1 in flight or
+  // unread, 2 handed out), the show_flow_msg sums
+  cudaStream_t cst = nullptr;
+  double *snap_dev[2] = {}, *snap_host[2] = {};
+  cudaEvent_t snap_ready[2] = {}, snap_done[2] = {};
+  int snap_state[2] = {0, 0}, snap_istep[2] = {0, 0};
+  double snap_tt[2] = {0.0, 0.0};
+  long long snap_seq[2] = {0, 0}, snap_counter = 0;
+  double *diag_dev = nullptr, *diag_host = nullptr;
+  cudaEvent_t diag_ready = nullptr, diag_done = nullptr;
+  bool diag_pending = false;
   // batched chemistry scratch
   double *b_di = nullptr, *b_e = nullptr, *b_dt = nullptr;
   int *b_nsub = nullptr, *b_perm = nullptr, *b_hist = nullptr, *b_counter = nullptr, *b_nfail = nullptr;
@@ -663,6 +675,20 @@ void filter_t(int istep, int nf, const double* F) {
   }
 }
 
+// copy stream, events and the show_flow_msg buffers of the asynchronous save / show calls
+void async_setup() {
+  if (L->cst) return;
+  CK(cudaStreamCreateWithFlags(&L->cst, cudaStreamNonBlocking));
+  for (int m = 0; m < 2; m++) {
+    CK(cudaEventCreateWithFlags(&L->snap_ready[m], cudaEventDisableTiming));
+    CK(cudaEventCreateWithFlags(&L->snap_done[m], cudaEventDisableTiming));
+  }
+  CK(cudaEventCreateWithFlags(&L->diag_ready, cudaEventDisableTiming));
+  CK(cudaEventCreateWithFlags(&L->diag_done, cudaEventDisableTiming));
+  CK(cudaMalloc(&L->diag_dev, sizeof(double) * 2));
+  CK(cudaMallocHost(&L->diag_host, sizeof(double) * 2));
+}
+
 double* ana_partials(size_t n) {
   if (L->ana_part_n < n) {
     if (L->ana_part) CK(cudaFree(L->ana_part));
@@ -791,6 +817,18 @@ void release() {
   for (auto& e : L->ev_pool) { cudaEventDestroy(e.first); cudaEventDestroy(e.second); }
   if (L->arena) cudaFree(L->arena);
   if (L->amu_keep) cudaFree(L->amu_keep);
+  if (L->cst) cudaStreamSynchronize(L->cst);
+  for (int m = 0; m < 2; m++) {
+    if (L->snap_dev[m]) cudaFree(L->snap_dev[m]);
+    if (L->snap_host[m]) cudaFreeHost(L->snap_host[m]);
+    if (L->snap_ready[m]) cudaEventDestroy(L->snap_ready[m]);
+    if (L->snap_done[m]) cudaEventDestroy(L->snap_done[m]);
+  }
+  if (L->diag_dev) cudaFree(L->diag_dev);
+  if (L->diag_host) cudaFreeHost(L->diag_host);
+  if (L->diag_ready) cudaEventDestroy(L->diag_ready);
+  if (L->diag_done) cudaEventDestroy(L->diag_done);
+  if (L->cst) cudaStreamDestroy(L->cst);
   if (L->ana_part) cudaFree(L->ana_part);
   if (L->avg) cudaFree(L->avg);
   if (L->shost) cudaFreeHost(L->shost);
@@ -1563,22 +1601,86 @@ int ocfd_gpu_download_state(double* f, double* di, double* prims) {
   });
 }
 
-int ocfd_gpu_diag(double* e_mean, double* k_mean) {
+int ocfd_gpu_diag_begin(void) {
   return guarded([&]() -> int {
     if (!L || !L->flow_ready) { g_err = "state not initialised"; return OCFD_ERR_STATE; }
+    async_setup();
     const long long N = L->hc.N;
-    unsigned nb = nblk(N, 256);
+    const unsigned nb = nblk(N, 256);
     if (L->sep) k_diag<true><<<nb, 256, 0, L->st>>>(L->f, L->d, L->u, L->v, L->w, L->partial, L->geo);
     else k_diag<false><<<nb, 256, 0, L->st>>>(L->f, L->d, L->u, L->v, L->w, L->partial, L->geo);
     LAUNCH_CHECK();
-    std::vector<double> h(2 * nb);
-    CK(cudaMemcpyAsync(h.data(), L->partial, sizeof(double) * 2 * nb, cudaMemcpyDeviceToHost, L->st));
-    CK(cudaStreamSynchronize(L->st));
-    double e = 0.0, k = 0.0;
-    for (unsigned b = 0; b < nb; b++) { e = e + h[2 * b]; k = k + h[2 * b + 1]; }
-    double nn = (double)L->P.nx * L->P.ny * L->P.nz;
-    *e_mean = e / nn;
-    *k_mean = k / nn;
+    k_sum_partials<2><<<1, 256, 0, L->st>>>(L->partial, (int)nb, L->diag_dev);
+    LAUNCH_CHECK();
+    CK(cudaEventRecord(L->diag_ready, L->st));
+    CK(cudaStreamWaitEvent(L->cst, L->diag_ready, 0));
+    CK(cudaMemcpyAsync(L->diag_host, L->diag_dev, sizeof(double) * 2, cudaMemcpyDeviceToHost, L->cst));
+    CK(cudaEventRecord(L->diag_done, L->cst));
+    L->diag_pending = true;
+    return 0;
+  });
+}
+
+int ocfd_gpu_diag_end(double* e_mean, double* k_mean) {
+  return guarded([&]() -> int {
+    if (!L || !L->diag_pending) { g_err = "no ocfd_gpu_diag_begin pending"; return OCFD_ERR_STATE; }
+    CK(cudaEventSynchronize(L->diag_done));
+    L->diag_pending = false;
+    const double nn = (double)L->P.nx * L->P.ny * L->P.nz;
+    if (e_mean) *e_mean = L->diag_host[0] / nn;
+    if (k_mean) *k_mean = L->diag_host[1] / nn;
+    return check_status();
+  });
+}
+
+int ocfd_gpu_diag(double* e_mean, double* k_mean) {
+  int rc = ocfd_gpu_diag_begin();
+  return rc != 0 ? rc : ocfd_gpu_diag_end(e_mean, k_mean);
+}
+
+int ocfd_gpu_snapshot(int istep, double tt) {
+  return guarded([&]() -> int {
+    if (!L || !L->flow_ready) { g_err = "state not initialised"; return OCFD_ERR_STATE; }
+    async_setup();
+    int slot = -1;  // a free slot, else the older of the handed-out ones
+    for (int m = 0; m < 2 && slot < 0; m++)
+      if (L->snap_state[m] == 0) slot = m;
+    if (slot < 0)
+      for (int m = 0; m < 2; m++)
+        if (L->snap_state[m] == 2 && (slot < 0 || L->snap_seq[m] < L->snap_seq[slot])) slot = m;
+    if (slot < 0) { g_err = "two snapshots in flight: call ocfd_gpu_snapshot_wait first"; return OCFD_ERR_STATE; }
+    const long long N = L->hc.N;
+    const size_t n = (size_t)(5 + L->NS) * N;
+    if (!L->snap_dev[slot]) {
+      CK(cudaMalloc(&L->snap_dev[slot], sizeof(double) * n));
+      CK(cudaMallocHost(&L->snap_host[slot], sizeof(double) * n));
+    }
+    k_pack_snapshot<<<nblk(N, 256), 256, 0, L->st>>>(L->d, L->u, L->v, L->w, L->T, L->di, L->NS, L->snap_dev[slot]);
+    LAUNCH_CHECK();
+    CK(cudaEventRecord(L->snap_ready[slot], L->st));
+    CK(cudaStreamWaitEvent(L->cst, L->snap_ready[slot], 0));
+    CK(cudaMemcpyAsync(L->snap_host[slot], L->snap_dev[slot], sizeof(double) * n, cudaMemcpyDeviceToHost, L->cst));
+    CK(cudaEventRecord(L->snap_done[slot], L->cst));
+    L->snap_state[slot] = 1;
+    L->snap_seq[slot] = ++L->snap_counter;
+    L->snap_istep[slot] = istep;
+    L->snap_tt[slot] = tt;
+    return 0;
+  });
+}
+
+int ocfd_gpu_snapshot_wait(int* istep, double* tt, const double** fields) {
+  return guarded([&]() -> int {
+    if (!L) { g_err = "not initialised"; return OCFD_ERR_STATE; }
+    int slot = -1;
+    for (int m = 0; m < 2; m++)
+      if (L->snap_state[m] == 1 && (slot < 0 || L->snap_seq[m] < L->snap_seq[slot])) slot = m;
+    if (slot < 0) { g_err = "no snapshot in flight"; return OCFD_ERR_STATE; }
+    CK(cudaEventSynchronize(L->snap_done[slot]));
+    L->snap_state[slot] = 2;
+    if (istep) *istep = L->snap_istep[slot];
+    if (tt) *tt = L->snap_tt[slot];
+    if (fields) *fields = L->snap_host[slot];
     return 0;
   });
 }

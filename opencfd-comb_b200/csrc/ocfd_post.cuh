@@ -212,4 +212,34 @@ __global__ void k_ana_average(const double* d, const double* u, const double* v,
     avg[(size_t)(5 + m) * N + nn] = (K * avg[(size_t)(5 + m) * N + nn] + di[(size_t)m * cC.H + q]) / (K + 1.0);
 }
 
+// save_flow_data's content (OCFD_IO.f90:39-64): d, u, v, w, T and every di, as interior arrays,
+// packed into one buffer for a single device-to-host copy
+__global__ void k_pack_snapshot(const double* d, const double* u, const double* v, const double* w, const double* T,
+                                const double* di, int ns, double* out) {
+  int i, j, k;
+  if (!cell_of((long long)blockIdx.x * blockDim.x + threadIdx.x, i, j, k)) return;
+  const int q = hidx(i, j, k), nn = nidx(i, j, k);
+  const long long N = cC.N;
+  out[nn] = d[q];
+  out[N + nn] = u[q];
+  out[2 * N + nn] = v[q];
+  out[3 * N + nn] = w[q];
+  out[4 * N + nn] = T[q];
+  for (int m = 0; m < ns; m++) out[(size_t)(5 + m) * N + nn] = di[(size_t)m * cC.H + q];
+}
+
+// final sums of NQ per-block partials on the device (one block of 256 threads, fixed order:
+// thread t adds blocks t, t + 256, ... in turn, then a tree), so that a reduction needs no host
+// round trip
+template <int NQ>
+__global__ void __launch_bounds__(256) k_sum_partials(const double* partial, int nb, double* out) {
+  double v[NQ];
+#pragma unroll
+  for (int m = 0; m < NQ; m++) v[m] = 0.0;
+  for (int b = threadIdx.x; b < nb; b += blockDim.x)
+#pragma unroll
+    for (int m = 0; m < NQ; m++) v[m] = v[m] + partial[(size_t)NQ * b + m];
+  block_sums<NQ>(v, out);
+}
+
 }  // namespace ocfd

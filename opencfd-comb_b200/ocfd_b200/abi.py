@@ -127,6 +127,10 @@ GPU_SIGNATURES = {
     "ocfd_gpu_init_state": (I, [PD, PD, D]),
     "ocfd_gpu_run": (I, [D, D, I, I, I]),
     "ocfd_gpu_chem_setup": (I, [C.POINTER(Thermo), C.POINTER(Kinetics), I, I]),
+    "ocfd_gpu_diag_begin": (I, []),
+    "ocfd_gpu_diag_end": (I, [PD, PD]),
+    "ocfd_gpu_snapshot": (I, [I, D]),
+    "ocfd_gpu_snapshot_wait": (I, [PI, PD, C.POINTER(PD)]),
     "ocfd_gpu_filtering": (I, [I, I, PD, PI]),
     "ocfd_gpu_keep_viscosity": (I, [I]),
     "ocfd_gpu_ana_box": (I, [D, PD]),

@@ -233,9 +233,9 @@ def _write_planes(fh, a):
     """write_3d (OCFD_IO_mpi.f90:232): one record of nx*ny doubles per k plane; a is (nz, ny, nx)
     in C order, whose planes are the Fortran (nx, ny) column-major planes."""
     a = np.ascontiguousarray(a, dtype=np.float64)
+    n = struct.pack("<i", a[0].nbytes)
     for k in range(a.shape[0]):
-        b = a[k].tobytes()
-        fh.write(struct.pack("<i", len(b))); fh.write(b); fh.write(struct.pack("<i", len(b)))
+        fh.write(n); fh.write(memoryview(a[k]).cast("B")); fh.write(n)  # no copy of the plane
 
 
 def write_3d_records(path, arrays):
@@ -263,3 +263,19 @@ def read_average(path, nx, ny, nz, nfields):
         for k in range(nz):
             out[m, k] = np.frombuffer(recs[1 + m * nz + k], dtype=np.float64).reshape(ny, nx)
     return k_average, t_average, out
+
+
+def write_flow_data(path, istep, tt, fields):
+    """save_flow_data (OCFD_IO.f90:39-64): header record (int32 Istep, real64 tt), then d, u, v, w,
+    T and every di as write_3d1 planes; fields is (5 + Ns, nz, ny, nx) in C order."""
+    with open(path, "wb") as fh:
+        hdr = struct.pack("<id", istep, tt)
+        fh.write(struct.pack("<i", len(hdr))); fh.write(hdr); fh.write(struct.pack("<i", len(hdr)))
+        for a in fields:
+            _write_planes(fh, a)
+
+
+def read_flow_data(path, nx, ny, nz, ns):
+    """read_flow_data (OCFD_IO.f90:5-36): (Istep, tt, (5 + ns, nz, ny, nx) array)."""
+    k, t, a = read_average(path, nx, ny, nz, 5 + ns)
+    return k, t, a

@@ -114,6 +114,59 @@ class Solver:
         _chk(lib().ocfd_gpu_stats(C.byref(a), C.byref(b)))
         return a.value, b.value
 
+    # ---- save / show without a host sync (save_flow_data, show_flow_msg) ----
+    def diag_begin(self):
+        _chk(lib().ocfd_gpu_diag_begin())
+
+    def diag_end(self):
+        e, k = C.c_double(), C.c_double()
+        _chk(lib().ocfd_gpu_diag_end(C.byref(e), C.byref(k)))
+        return e.value, k.value
+
+    def snapshot(self, istep, tt):
+        _chk(lib().ocfd_gpu_snapshot(istep, tt))
+
+    def snapshot_wait(self):
+        """(Istep, tt, view of the pinned (5 + Ns, nz, ny, nx) buffer); the view is valid until
+        the second-next snapshot and while the solver is open."""
+        nx, ny, nz = self.case.shape
+        nf = 5 + self.case.params.n_spec
+        ist, t, ptr = C.c_int(), C.c_double(), C.POINTER(C.c_double)()
+        _chk(lib().ocfd_gpu_snapshot_wait(C.byref(ist), C.byref(t), C.byref(ptr)))
+        return ist.value, t.value, np.ctypeslib.as_array(ptr, shape=(nf, nz, ny, nx))
+
+    def save_flow_data_async(self, path, istep, tt):
+        """save_flow_data (OCFD_IO.f90:39-64) overlapped with the following steps: the device
+        packs the fields and copies them to pinned memory on a copy stream; the previous save is
+        collected here (its copy long finished) and written to disk by a background thread that
+        touches only that pinned buffer. flush_saves() completes everything."""
+        import threading
+        from . import files
+        if not hasattr(self, "_saves"):
+            self._saves, self._writers = [], []
+        if len(self._saves) == 1:
+            self._collect()
+        while len(self._writers) > 1:  # the slot about to be reused must be written out
+            self._writers.pop(0).join()
+        self.snapshot(istep, tt)
+        self._saves.append(path)
+        self._files = files
+        self._threading = threading
+
+    def _collect(self):
+        path = self._saves.pop(0)
+        ist, t, a = self.snapshot_wait()
+        w = self._threading.Thread(target=self._files.write_flow_data, args=(path, ist, t, a))
+        w.start()
+        self._writers.append(w)
+
+    def flush_saves(self):
+        while getattr(self, "_saves", []):
+            self._collect()
+        for w in getattr(self, "_writers", []):
+            w.join()
+        self._writers = []
+
     # ---- filtering and analysis (code/others/OCFD_filtering.f90, OCFD_ANA.f90) ----
     def filtering(self, istep, table, nfiltering):
         """filtering after step istep (OCFD_NS_Solver.f90:48); table from post.filter_table.
@@ -198,6 +251,7 @@ class Solver:
         return lib().ocfd_gpu_launch_count()
 
     def close(self):
+        self.flush_saves()
         lib().ocfd_gpu_finalize()
 
 
