@@ -99,10 +99,15 @@ struct Tile {
 template <int DIR, int NC_, int TS = 0>
 struct FluxTile {
   static constexpr int C = Tile<DIR, TS>::C, NL = Tile<DIR, TS>::NL, P = C + 8, NC = NC_;
+  // pencil pitch in shared memory: odd along x, so that the lanes of a warp that read the same
+  // point of different pencils fall in different banks
+  static constexpr int PS = DIR == 0 ? P + 1 : P;
   static constexpr int NCS = 2 * NC;        // (component, sign) pairs: plus components, then minus
   static constexpr int NI = (C + 1) * NL;   // interfaces of a tile
+  // UD7L runs: R consecutive interfaces of one pencil per item (R divides the C + 1 interfaces)
+  static constexpr int R = (C + 1) % 3 == 0 ? 3 : ((C + 1) % 5 == 0 ? 5 : (C + 1) % 11 == 0 ? 11 : 1);
   static_assert((P * NL) % FLUX_THREADS == 0, "split phase must fill whole rounds");
-  static constexpr size_t smem = sizeof(double) * (size_t)(NCS * P * NL + NCS * NI) + sizeof(int) * (2 * NI + 4);
+  static constexpr size_t smem = sizeof(double) * (size_t)(NCS * PS * NL + NCS * NI) + sizeof(int) * (2 * NI + 4);
 };
 
 struct FluxArgs {
@@ -146,17 +151,17 @@ __device__ __forceinline__ double ud7l_signed(const double* v, bool plus) {
 template <int DIR, int SCHEME, int SPLIT, bool SEP, bool SCALAR, int G = 1, int TS = 0>
 __global__ void __launch_bounds__(FLUX_THREADS, Tile<DIR, TS>::MINB) k_flux(FluxArgs a) {
   using T = FluxTile<DIR, SCALAR ? G : 5, TS>;
-  constexpr int C = T::C, NL = T::NL, P = T::P, NC = T::NC, NCS = T::NCS, NI = T::NI;
+  constexpr int C = T::C, NL = T::NL, P = T::P, PS = T::PS, NC = T::NC, NCS = T::NCS, NI = T::NI;
   constexpr bool HYB = SCHEME == OCFD_SCHEME_HYBRID;
   constexpr int VS = DIR == 0 ? 1 : NL;  // stride of consecutive sweep points in shared memory
   extern __shared__ double smem[];
-  double* sf = smem;               // [NCS][P x NL] split fluxes
-  double* sh = sf + NCS * P * NL;  // [NCS][NI] interface fluxes
+  double* sf = smem;                // [NCS][PS x NL] split fluxes
+  double* sh = sf + NCS * PS * NL;  // [NCS][NI] interface fluxes
   int* squeue = reinterpret_cast<int*>(sh + NCS * NI);  // listed interfaces: scm << 16 | interface
   int* sfast = squeue + NI;                             // 1 = UD7L fast path
   int* sqn = sfast + NI;                                // list length
   // point p of pencil l, interface t of pencil l
-  auto sidx = [&](int cs, int p, int l) { return DIR == 0 ? (cs * NL + l) * P + p : (cs * P + p) * NL + l; };
+  auto sidx = [&](int cs, int p, int l) { return DIR == 0 ? (cs * NL + l) * PS + p : (cs * P + p) * NL + l; };
   auto iidx = [&](int t, int l) { return DIR == 0 ? l * (C + 1) + t : t * NL + l; };
 
   const int n = DIR == 0 ? cC.nx : (DIR == 1 ? cC.ny : cC.nz);
@@ -290,14 +295,59 @@ __global__ void __launch_bounds__(FLUX_THREADS, Tile<DIR, TS>::MINB) k_flux(Flux
     dst = cs * NI + it;
     return true;
   };
-  // two independent items per iteration, so that their dependent FP64 chains overlap
-  for (int idx = threadIdx.x; idx < nfast; idx += 2 * FLUX_THREADS) {
-    double ha = 0.0, hb = 0.0;
-    int da = 0, db = 0;
-    const bool oa = item_flux(idx, ha, da);
-    const bool ob = idx + FLUX_THREADS < nfast && item_flux(idx + FLUX_THREADS, hb, db);
-    if (oa) sh[da] = ha;
-    if (ob) sh[db] = hb;
+  if constexpr (HYB && T::R > 1) {
+    // fast interfaces: UD7L in runs of R consecutive interfaces of one pencil and (component,
+    // sign). The R + 7 split fluxes of a run are loaded once at fixed offsets and the R sums are
+    // independent FP64 chains; each sum keeps ud7l_signed's term order (the minus flux reads the
+    // stencil mirrored). Plus items come first, so only one warp mixes the two signs.
+    constexpr int R = T::R, NR = (C + 1) / R, NH = NC * NL * NR;
+    const double* U = cC.UD7L;
+    for (int it = threadIdx.x; it < 2 * NH; it += FLUX_THREADS) {
+      const bool plus = it < NH;
+      const int jt = plus ? it : it - NH;
+      int c, l, r;
+      if (DIR == 0) {  // lanes across pencils (odd pitch: no bank conflicts)
+        const int cl = jt % (NC * NL);
+        r = jt / (NC * NL); c = cl / NL; l = cl - c * NL;
+      } else {         // lanes along the contiguous i-lines
+        l = jt % NL;
+        const int rc = jt / NL;
+        r = rc % NR; c = rc / NR;
+      }
+      const int cs = plus ? c : NC + c, t0 = r * R;
+      const double* x = sf + sidx(cs, t0, l);
+      double w[R + 7];
+#pragma unroll
+      for (int m = 0; m < R + 7; m++) w[m] = x[m * VS];
+      double h[R];
+      if (plus) {
+#pragma unroll
+        for (int q = 0; q < R; q++)
+          h[q] = U[0] * w[q] + U[1] * w[q + 1] + U[2] * w[q + 2] + U[3] * w[q + 3] + U[4] * w[q + 4] +
+                 U[5] * w[q + 5] + U[6] * w[q + 6] + U[7] * w[q + 7];
+      } else {
+#pragma unroll
+        for (int q = 0; q < R; q++)
+          h[q] = U[0] * w[q + 7] + U[1] * w[q + 6] + U[2] * w[q + 5] + U[3] * w[q + 4] + U[4] * w[q + 3] +
+                 U[5] * w[q + 2] + U[6] * w[q + 1] + U[7] * w[q];
+      }
+      const bool line_ok = l0 + l <= nl_max;
+#pragma unroll
+      for (int q = 0; q < R; q++) {
+        const int ii = iidx(t0 + q, l);
+        if (line_ok && t0 + q <= ncell && sfast[ii]) sh[cs * NI + ii] = h[q];
+      }
+    }
+  } else {
+    // two independent items per iteration, so that their dependent FP64 chains overlap
+    for (int idx = threadIdx.x; idx < nfast; idx += 2 * FLUX_THREADS) {
+      double ha = 0.0, hb = 0.0;
+      int da = 0, db = 0;
+      const bool oa = item_flux(idx, ha, da);
+      const bool ob = idx + FLUX_THREADS < nfast && item_flux(idx + FLUX_THREADS, hb, db);
+      if (oa) sh[da] = ha;
+      if (ob) sh[db] = hb;
+    }
   }
   if (HYB) {  // listed interfaces: general reconstruction (closures, WENO7 / WENO5)
     for (int r = threadIdx.x; r < NCS * nq; r += FLUX_THREADS) {
