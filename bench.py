@@ -513,7 +513,8 @@ def main_ours(a):
         choice, tms = g.autotune(reps=5)
         tiles = {"mode": "auto", "choice": choice,
                  "candidate_ms": {"flux_x": tms[0:3], "flux_y": tms[3:6], "flux_z": tms[6:9],
-                                  "visc_ev_kc8_16_32_64": tms[9:13], "visc_div_kc8_16_32_64": tms[13:17]}}
+                                  "visc_ev_kc8_16_32_64": tms[9:13],
+                                  "visc_div_kc8_16_32_64_percell": tms[13:18]}}
     chk(L.ocfd_gpu_run(dt, tt, a.warmup, reac, nsub))
     tt += a.warmup * dt
 

@@ -259,10 +259,10 @@ int ocfd_gpu_ana_average(int upload, double* fields, int* k_average, double* t_a
  * ocfd_gpu_autotune times each candidate on the current state (after ocfd_gpu_init_state) over reps
  * launches, applies the fastest and remembers it for this configuration (grid, schemes, species)
  * in the process; reps = 0 applies a remembered choice without timing when there is one. choice
- * (may be NULL) receives the choice; ms (may be NULL, 17 doubles) the mean ms per launch of each
- * candidate: flux x, y, z shapes 0..2, then k_visc_ev and k_visc_div at 8, 16, 32, 64 planes
- * (-1 where not timed). The launches write only scratch arrays, so the solution is unchanged.
- * Default choice {0, 0, 0, 16, 16}. */
+ * (may be NULL) receives the choice; ms (may be NULL, 18 doubles) the mean ms per launch of each
+ * candidate: flux x, y, z shapes 0..2, k_visc_ev at 8, 16, 32, 64 planes, k_visc_div at 8, 16,
+ * 32, 64 planes and in its per-cell form (k planes 0) (-1 where not timed). The launches write
+ * only scratch arrays, so the solution is unchanged. Default choice {0, 0, 0, 16, 16}. */
 int ocfd_gpu_autotune(int reps, int* choice, double* ms);
 int ocfd_gpu_set_tiles(const int* choice);
 int ocfd_gpu_get_tiles(int* choice);

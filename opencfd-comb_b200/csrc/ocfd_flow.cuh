@@ -753,6 +753,32 @@ __global__ void __launch_bounds__(VE_THREADS, 2) k_visc_div(DivArgs a) {
   }
 }
 
+// per-cell form of k_visc_div (the autotuner's k chunk 0): one thread per cell, every stencil
+// value read through the read-only cache; the same expressions as the marching form
+template <bool SEP, int HZ>
+__global__ void __launch_bounds__(256) k_visc_div_pc(DivArgs a) {
+  constexpr int CD = HZ == 3 ? 6 : 8;
+  int i, j, k;
+  if (!cell_of((long long)blockIdx.x * blockDim.x + threadIdx.x, i, j, k)) return;
+  const int q = hidx(i, j, k), nn = nidx(i, j, k);
+  const int sy = hstride(1), sz = hstride(2);
+  const long long N = cC.N;
+  double duc[4];
+#pragma unroll
+  for (int m = 0; m < 4; m++) duc[m] = a.du[(size_t)(m + 1) * N + nn];
+  const double ajac = metric_jac<SEP>(a.g, i, j, k, q);
+#pragma unroll
+  for (int m = 0; m < 4; m++) {
+    const double* e1 = a.ev[m] + q;
+    const double* e2 = a.ev[4 + m] + q;
+    const double* e3 = a.ev[8 + m] + q;
+    double uk = cdiff_g<CD>([&](int o) { return __ldg(e1 + o); }, 0, i, cC.nx);
+    double ui = cdiff_g<CD>([&](int o) { return __ldg(e2 + o * sy); }, 1, j, cC.ny);
+    double us = cdiff_g<CD>([&](int o) { return __ldg(e3 + o * sz); }, 2, k, cC.nz);
+    a.du[(size_t)(m + 1) * N + nn] = duc[m] + (uk + ui + us) * ajac;
+  }
+}
+
 // ---------------------------------------------------------------- species: viscous part
 // du_scaler_viscous (OCFD_scaler_viscous.f90:4-79) for every species of a stage at once. The
 // reference loops over species, each pass using du(:,:,:,1) and Ev1 as scratch; no species reads
@@ -1059,21 +1085,29 @@ struct PrimArgs {
   int krk;  // 1..3 RK stage; 0 = no update (start-up conversion only)
   double dt;
 };
-template <int NS>
+// KRK (1..3, or 0 for the start-up conversion) is a template parameter, so that every stage's
+// loads are straight-line code issued together
+template <int NS, int KRK>
 __global__ void __launch_bounds__(256) k_rk_prims(PrimArgs a) {
   int i, j, k;
   if (!cell_of((long long)blockIdx.x * blockDim.x + threadIdx.x, i, j, k)) return;
   const int q = hidx(i, j, k), nn = nidx(i, j, k);
   const long long N = cC.N;
-  const double ra[3] = {0.0, 3.0 / 4.0, 1.0 / 3.0}, rb[3] = {1.0, 1.0 / 4.0, 2.0 / 3.0};
-  double f[5];
+  double f[5], fo[5], g[5], e[5];
 #pragma unroll
   for (int m = 0; m < 5; m++) {
-    size_t o = (size_t)m * N + nn;
-    if (a.krk == 1) f[m] = a.fn[o] + a.dt * a.du[o];
-    else if (a.krk > 1) f[m] = ra[a.krk - 1] * a.fn[o] + rb[a.krk - 1] * (a.f[o] + a.dt * a.du[o]);
-    else f[m] = a.f[o];
-    a.f[o] = f[m];
+    const size_t o = (size_t)m * N + nn;
+    if (KRK >= 1) fo[m] = __ldg(a.fn + o);
+    if (KRK >= 1) g[m] = __ldg(a.du + o);
+    if (KRK != 1) e[m] = a.f[o];
+  }
+#pragma unroll
+  for (int m = 0; m < 5; m++) {
+    if (KRK == 1) f[m] = fo[m] + a.dt * g[m];
+    else if (KRK == 2) f[m] = (3.0 / 4.0) * fo[m] + (1.0 / 4.0) * (e[m] + a.dt * g[m]);
+    else if (KRK == 3) f[m] = (1.0 / 3.0) * fo[m] + (2.0 / 3.0) * (e[m] + a.dt * g[m]);
+    else f[m] = e[m];
+    if (KRK != 0) a.f[(size_t)m * N + nn] = f[m];
   }
   double dd = f[0];
   double uu = f[1] / f[0], vv = f[2] / f[0], ww = f[3] / f[0];

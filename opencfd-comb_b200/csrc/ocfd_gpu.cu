@@ -318,7 +318,13 @@ void prims_t(int krk, double dt) {
   a.dt = dt;
   {
     KTimer t(KC_RK_PRIMS);
-    k_rk_prims<NS><<<nblk(L->hc.N, 256), 256, 0, L->st>>>(a);
+    const unsigned nb = nblk(L->hc.N, 256);
+    switch (krk) {
+      case 1: k_rk_prims<NS, 1><<<nb, 256, 0, L->st>>>(a); break;
+      case 2: k_rk_prims<NS, 2><<<nb, 256, 0, L->st>>>(a); break;
+      case 3: k_rk_prims<NS, 3><<<nb, 256, 0, L->st>>>(a); break;
+      default: k_rk_prims<NS, 0><<<nb, 256, 0, L->st>>>(a); break;
+    }
     LAUNCH_CHECK();
   }
   {
@@ -369,6 +375,10 @@ void visc_div_go(const DivArgs& da) {
     attr = true;
   }
   const ocfd_params& P = L->P;
+  if (da.kc == 0) {  // per-cell form
+    k_visc_div_pc<SEP, HZ><<<nblk(L->hc.N, 256), 256, 0, L->st>>>(da);
+    return;
+  }
   dim3 grid(nblk(P.nx, VE_TX), nblk(P.ny, VE_TY), nblk(P.nz, da.kc));
   k_visc_div<SEP, HZ><<<grid, VE_THREADS, sm, L->st>>>(da);
 }
@@ -537,7 +547,7 @@ void chem_t(double dt2, int nsub) {
 // Tile choices {flux x, y, z shape; k_visc_ev, k_visc_div k planes per block}. Every choice
 // gives bit-identical results (a tile decides which block computes a point, not how), so the
 // tuner is free to pick by time alone. Choices are remembered per configuration in the process.
-constexpr int TUNE_N = 5, TUNE_TIMES = 3 * FLUX_TILE_SHAPES + 8;
+constexpr int TUNE_N = 5, TUNE_TIMES = 3 * FLUX_TILE_SHAPES + 9;
 std::map<std::string, std::array<int, TUNE_N>> g_tune_cache;
 
 std::string tune_key() {
@@ -597,7 +607,7 @@ void tune_t(int reps, int* best, double* ms) {
       L->flux_ts[d] = best[d];
     }
     best[3] = best[4] = VE_KC;
-    for (int m = 0; m < 4; m++) ms[3 * FLUX_TILE_SHAPES + m] = ms[3 * FLUX_TILE_SHAPES + 4 + m] = -1.0;
+    for (int m = 3 * FLUX_TILE_SHAPES; m < TUNE_TIMES; m++) ms[m] = -1.0;
     if (P.if_viscous == 1) {
       double t_ev = 1e300, t_div = 1e300;
       for (int m = 0; m < 4; m++) {
@@ -607,9 +617,9 @@ void tune_t(int reps, int* best, double* ms) {
         ms[3 * FLUX_TILE_SHAPES + m] = t;
         if (t < t_ev) { t_ev = t; best[3] = va.kc; }
       }
-      for (int m = 0; m < 4; m++) {
+      for (int m = 0; m < 5; m++) {  // the four k chunks, then the per-cell form (0)
         DivArgs da = div_args();
-        da.kc = VE_KC_CHOICES[m];
+        da.kc = m < 4 ? VE_KC_CHOICES[m] : 0;
         const double t = timed([&] { visc_div_launch(da); });
         ms[3 * FLUX_TILE_SHAPES + 4 + m] = t;
         if (t < t_div) { t_div = t; best[4] = da.kc; }
@@ -2049,7 +2059,10 @@ int ocfd_gpu_set_tiles(const int* choice) {
       g_err = "the characteristic flux has one tile shape (0)";
       return OCFD_ERR_PARAM;
     }
-    if (choice[3] < 1 || choice[4] < 1) { g_err = "k planes per block must be >= 1"; return OCFD_ERR_PARAM; }
+    if (choice[3] < 1 || choice[4] < 0) {
+      g_err = "k planes per block must be >= 1 (k_visc_div: >= 0, 0 = per-cell form)";
+      return OCFD_ERR_PARAM;
+    }
     apply_tiles(choice);
     return 0;
   });

@@ -214,7 +214,7 @@ class Solver:
         """Times the candidate tile shapes on the current state and applies the fastest; returns
         (choice, ms per launch of each candidate)."""
         ch = (C.c_int * 5)()
-        ms = (C.c_double * 17)()
+        ms = (C.c_double * 18)()
         _chk(lib().ocfd_gpu_autotune(reps, ch, ms))
         return list(ch), list(ms)
 

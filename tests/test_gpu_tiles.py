@@ -13,6 +13,7 @@ CHOICES = [
     [1, 1, 1, 8, 32],
     [2, 2, 2, 64, 8],
     [1, 2, 0, 3, 5],  # k chunks that do not divide nz
+    [0, 1, 2, 16, 0],  # per-cell k_visc_div
 ]
 
 
@@ -56,7 +57,7 @@ def test_autotune_choice_and_solution():
     ref, _ = _run(c)
     st, (choice, ms) = _run(c, tune=True)
     assert choice[0] in (0, 1, 2) and choice[1] in (0, 1, 2) and choice[2] in (0, 1, 2)
-    assert choice[3] in (8, 16, 32, 64) and choice[4] in (8, 16, 32, 64)
+    assert choice[3] in (8, 16, 32, 64) and choice[4] in (0, 8, 16, 32, 64)
     assert all(t > 0 for t in ms), ms  # viscous case: every candidate timed
     for d in range(3):
         assert ms[3 * d + choice[d]] == min(ms[3 * d:3 * d + 3])
@@ -80,7 +81,7 @@ def test_bad_tile_choice_is_rejected():
     c = _case("isotropic")
     g = solver.Solver(c)
     g.init_state()
-    for bad in ([3, 0, 0, 16, 16], [0, -1, 0, 16, 16], [0, 0, 0, 0, 16]):
+    for bad in ([3, 0, 0, 16, 16], [0, -1, 0, 16, 16], [0, 0, 0, 0, 16], [0, 0, 0, 16, -1]):
         with pytest.raises(solver.OcfdError):
             g.set_tiles(bad)
     g.close()
