@@ -26,6 +26,10 @@ int sg_cells_chem(int ns, double* f, double* Et, double* T, double* p, double* d
                   cudaStream_t st);
 int sg_cells_setup(int ns, long long N, double tol);
 long long sg_cells_rejected(long long* reasons);
+// set-up kernels (defined below) that the tile autotuner also launches
+__global__ void k_fill(double* p, long long n, double v);
+__global__ void k_jacobian(const double* X, const double* Y, const double* Z, double* const* m);
+__global__ void k_metric_ratio(double* const* m, long long H);
 }  // namespace ocfd
 #include "ocfd_launch.h"
 
@@ -86,6 +90,10 @@ struct Lib {
   // sweep direction, k planes per block of k_visc_ev and k_visc_div
   int flux_ts[3] = {0, 0, 0};
   int kc_ev = VE_KC, kc_div = VE_KC;
+  // metric form per kernel family on a tensor-product grid: false = computed from the 1-D
+  // derivatives (separable), true = read from the 19 stored arrays (allocated on first use)
+  bool met_flux = false, met_ev = false, met_div = false;
+  double* met_store = nullptr;
   // analysis (ocfd_gpu_keep_viscosity, ocfd_gpu_ana_*): the single-species stage viscosity kept
   // for ana_box, reduction partials, time-average accumulators
   bool keep_amu = false;
@@ -205,15 +213,16 @@ void launch_flux(int dir, const FluxArgs& a, int group = 0, int ngroups = 1) {
   const ocfd_params& P = L->P;
   const bool ch = P.if_scheme_character == 1;
   const int ts = (group == 0 && !ch) ? L->flux_ts[dir] : 0;
+  const bool sep = L->sep && !L->met_flux;
   if (ts != 0) {
     using Fn = void (*)(int, int, bool, const FluxArgs&, int, int, int, cudaStream_t);
     static const Fn tab[3][2] = {{launch_flux_x_t1, launch_flux_x_t2},
                                  {launch_flux_y_t1, launch_flux_y_t2},
                                  {launch_flux_z_t1, launch_flux_z_t2}};
-    tab[dir][ts - 1](P.scheme_invis, P.flux_splitting, L->sep, a, P.nx, P.ny, P.nz, L->st);
-  } else if (dir == 0) launch_flux_x(P.scheme_invis, P.flux_splitting, L->sep, group, ngroups, ch, a, P.nx, P.ny, P.nz, L->st);
-  else if (dir == 1) launch_flux_y(P.scheme_invis, P.flux_splitting, L->sep, group, ngroups, ch, a, P.nx, P.ny, P.nz, L->st);
-  else launch_flux_z(P.scheme_invis, P.flux_splitting, L->sep, group, ngroups, ch, a, P.nx, P.ny, P.nz, L->st);
+    tab[dir][ts - 1](P.scheme_invis, P.flux_splitting, sep, a, P.nx, P.ny, P.nz, L->st);
+  } else if (dir == 0) launch_flux_x(P.scheme_invis, P.flux_splitting, sep, group, ngroups, ch, a, P.nx, P.ny, P.nz, L->st);
+  else if (dir == 1) launch_flux_y(P.scheme_invis, P.flux_splitting, sep, group, ngroups, ch, a, P.nx, P.ny, P.nz, L->st);
+  else launch_flux_z(P.scheme_invis, P.flux_splitting, sep, group, ngroups, ch, a, P.nx, P.ny, P.nz, L->st);
   LAUNCH_CHECK();
 }
 
@@ -416,13 +425,13 @@ DivArgs div_args() {
 template <int NS>
 void visc_ev_launch(const ViscArgs& va) {
   const bool cd8 = L->P.scheme_vis == OCFD_SCHEME_CD8;
-  if (L->sep) cd8 ? visc_ev_go<NS, true, 4>(va) : visc_ev_go<NS, true, 3>(va);
+  if (L->sep && !L->met_ev) cd8 ? visc_ev_go<NS, true, 4>(va) : visc_ev_go<NS, true, 3>(va);
   else cd8 ? visc_ev_go<NS, false, 4>(va) : visc_ev_go<NS, false, 3>(va);
   LAUNCH_CHECK();
 }
 void visc_div_launch(const DivArgs& da) {
   const bool cd8 = L->P.scheme_vis == OCFD_SCHEME_CD8;
-  if (L->sep) cd8 ? visc_div_go<true, 4>(da) : visc_div_go<true, 3>(da);
+  if (L->sep && !L->met_div) cd8 ? visc_div_go<true, 4>(da) : visc_div_go<true, 3>(da);
   else cd8 ? visc_div_go<false, 4>(da) : visc_div_go<false, 3>(da);
   LAUNCH_CHECK();
 }
@@ -544,10 +553,12 @@ void chem_t(double dt2, int nsub) {
 }
 
 // ---------------------------------------------------------------- stencil tile autotuner
-// Tile choices {flux x, y, z shape; k_visc_ev, k_visc_div k planes per block}. Every choice
-// gives bit-identical results (a tile decides which block computes a point, not how), so the
-// tuner is free to pick by time alone. Choices are remembered per configuration in the process.
-constexpr int TUNE_N = 5, TUNE_TIMES = 3 * FLUX_TILE_SHAPES + 9;
+// Tile choices {flux x, y, z shape; k_visc_ev, k_visc_div k planes per block; metric form of the
+// flux sweeps, k_visc_ev, k_visc_div}. Every choice gives bit-identical results (a tile decides
+// which block computes a point, not how; the stored metric arrays hold the values the separable
+// form computes), so the tuner is free to pick by time alone. Choices are remembered per
+// configuration in the process.
+constexpr int TUNE_N = 8, TUNE_TIMES = 3 * FLUX_TILE_SHAPES + 9 + 5;
 std::map<std::string, std::array<int, TUNE_N>> g_tune_cache;
 
 std::string tune_key() {
@@ -558,10 +569,40 @@ std::string tune_key() {
   return b;
 }
 
+void set_geo_device_ptrs();
+// the 19 metric arrays of a tensor-product grid, as the general path computes them
+// (comput_Jacobian3d, the periodic exchange, Akx1..Asz1), beside the separable form
+void ensure_stored_metrics() {
+  if (!L->sep || L->met_store) return;
+  const long long H = L->hc.H, N = L->hc.N;
+  CK(cudaMalloc(&L->met_store, sizeof(double) * 19 * H));
+  for (int m = 0; m < 19; m++) L->met[m] = L->met_store + (size_t)m * H;
+  for (int m = 0; m < 19; m++) {
+    k_fill<<<nblk(H, 256), 256, 0, L->st>>>(L->met[m], H, 1.0);
+    LAUNCH_CHECK();
+  }
+  double** mp = nullptr;
+  CK(cudaMalloc(&mp, sizeof(double*) * 19));
+  CK(cudaMemcpyAsync(mp, L->met, sizeof(double*) * 19, cudaMemcpyHostToDevice, L->st));
+  k_jacobian<<<nblk(N, 256), 256, 0, L->st>>>(L->X, L->Y, L->Z, mp);
+  LAUNCH_CHECK();
+  std::vector<double*> ml(L->met, L->met + 10);
+  exchange_v(ml, 7);
+  k_metric_ratio<<<nblk(H, 256), 256, 0, L->st>>>(mp, H);
+  LAUNCH_CHECK();
+  CK(cudaStreamSynchronize(L->st));
+  CK(cudaFree(mp));
+  set_geo_device_ptrs();
+}
+
 void apply_tiles(const int* c) {
   for (int d = 0; d < 3; d++) L->flux_ts[d] = c[d];
   L->kc_ev = c[3];
   L->kc_div = c[4];
+  if (L->sep && (c[5] | c[6] | c[7])) ensure_stored_metrics();
+  L->met_flux = c[5] != 0;
+  L->met_ev = c[6] != 0;
+  L->met_div = c[7] != 0;
   if (L->gexec) {  // the captured step holds the old launches
     CK(cudaGraphExecDestroy(L->gexec));
     L->gexec = nullptr;
@@ -607,6 +648,7 @@ void tune_t(int reps, int* best, double* ms) {
       L->flux_ts[d] = best[d];
     }
     best[3] = best[4] = VE_KC;
+    best[5] = best[6] = best[7] = L->sep ? 0 : 1;
     for (int m = 3 * FLUX_TILE_SHAPES; m < TUNE_TIMES; m++) ms[m] = -1.0;
     if (P.if_viscous == 1) {
       double t_ev = 1e300, t_div = 1e300;
@@ -623,6 +665,42 @@ void tune_t(int reps, int* best, double* ms) {
         const double t = timed([&] { visc_div_launch(da); });
         ms[3 * FLUX_TILE_SHAPES + 4 + m] = t;
         if (t < t_div) { t_div = t; best[4] = da.kc; }
+      }
+    }
+    if (L->sep) {  // the stored metric arrays, each family at its best tile
+      ensure_stored_metrics();
+      const FluxArgs fm = flow_flux_args();  // geometry with the stored arrays
+      const int M0 = 3 * FLUX_TILE_SHAPES + 9;
+      L->met_flux = true;
+      for (int d = 0; d < 3; d++) {
+        L->flux_ts[d] = best[d];
+        const double t = timed([&] { launch_flux(d, fm); });
+        ms[M0 + d] = t;
+        if (t < ms[d * FLUX_TILE_SHAPES + best[d]]) best[5] = 1;  // one form for the three sweeps
+      }
+      if (best[5] == 1) {  // keep the stored form only if the three sweeps together are faster
+        double a = 0.0, b = 0.0;
+        for (int d = 0; d < 3; d++) { a += ms[M0 + d]; b += ms[d * FLUX_TILE_SHAPES + best[d]]; }
+        best[5] = a < b ? 1 : 0;
+      }
+      L->met_flux = false;
+      if (P.if_viscous == 1) {
+        L->met_ev = true;
+        ViscArgs va = visc_args<NS>();
+        va.kc = best[3];
+        ms[M0 + 3] = timed([&] { visc_ev_launch<NS>(va); });
+        L->met_ev = false;
+        int mi = 0;
+        for (int m = 0; m < 4; m++) if (VE_KC_CHOICES[m] == best[3]) mi = m;
+        best[6] = ms[M0 + 3] < ms[3 * FLUX_TILE_SHAPES + mi] ? 1 : 0;
+        L->met_div = true;
+        DivArgs da = div_args();
+        da.kc = best[4];
+        ms[M0 + 4] = timed([&] { visc_div_launch(da); });
+        L->met_div = false;
+        int mj = 4;
+        for (int m = 0; m < 4; m++) if (VE_KC_CHOICES[m] == best[4]) mj = m;
+        best[7] = ms[M0 + 4] < ms[3 * FLUX_TILE_SHAPES + 4 + mj] ? 1 : 0;
       }
     }
   } catch (...) {
@@ -827,6 +905,7 @@ void release() {
   for (auto& e : L->ev_pool) { cudaEventDestroy(e.first); cudaEventDestroy(e.second); }
   if (L->arena) cudaFree(L->arena);
   if (L->amu_keep) cudaFree(L->amu_keep);
+  if (L->met_store) cudaFree(L->met_store);
   if (L->cst) cudaStreamSynchronize(L->cst);
   for (int m = 0; m < 2; m++) {
     if (L->snap_dev[m]) cudaFree(L->snap_dev[m]);
@@ -1199,7 +1278,7 @@ int ocfd_gpu_init(const ocfd_params* p, const ocfd_thermo* th, const ocfd_kineti
     }
     CK(cudaMemcpyToSymbol(cC, &c, sizeof(DevConst)));
 
-    L->sep = separable(p, coords);
+    L->sep = metrics == nullptr && separable(p, coords);  // given metrics are used as given
     for (int m = 0; m < 6; m++)
       if (p->ghost_cell[m] != 0) L->sep = false;  // ghost slabs carry their own metrics
     const long long H = c.H, N = c.N;
@@ -2063,6 +2142,8 @@ int ocfd_gpu_set_tiles(const int* choice) {
       g_err = "k planes per block must be >= 1 (k_visc_div: >= 0, 0 = per-cell form)";
       return OCFD_ERR_PARAM;
     }
+    for (int m = 5; m < 8; m++)
+      if (choice[m] != 0 && choice[m] != 1) { g_err = "metric form must be 0 (computed) or 1 (stored)"; return OCFD_ERR_PARAM; }
     apply_tiles(choice);
     return 0;
   });
@@ -2073,6 +2154,9 @@ int ocfd_gpu_get_tiles(int* choice) {
   for (int d = 0; d < 3; d++) choice[d] = L->flux_ts[d];
   choice[3] = L->kc_ev;
   choice[4] = L->kc_div;
+  choice[5] = L->sep ? (int)L->met_flux : 1;
+  choice[6] = L->sep ? (int)L->met_ev : 1;
+  choice[7] = L->sep ? (int)L->met_div : 1;
   return 0;
 }
 

@@ -213,17 +213,19 @@ class Solver:
     def autotune(self, reps=5):
         """Times the candidate tile shapes on the current state and applies the fastest; returns
         (choice, ms per launch of each candidate)."""
-        ch = (C.c_int * 5)()
-        ms = (C.c_double * 18)()
+        ch = (C.c_int * 8)()
+        ms = (C.c_double * 23)()
         _chk(lib().ocfd_gpu_autotune(reps, ch, ms))
         return list(ch), list(ms)
 
     def set_tiles(self, choice):
-        ch = (C.c_int * 5)(*choice)
+        """choice: 8 ints (see ocfd_gpu_autotune); a 5-int choice keeps the computed metric form."""
+        choice = list(choice) + [0] * (8 - len(choice))
+        ch = (C.c_int * 8)(*choice)
         _chk(lib().ocfd_gpu_set_tiles(ch))
 
     def tiles(self):
-        ch = (C.c_int * 5)()
+        ch = (C.c_int * 8)()
         _chk(lib().ocfd_gpu_get_tiles(ch))
         return list(ch)
 

@@ -151,6 +151,29 @@ def test_separable_metrics_match_oracle(oracle, gpu):
     assert np.array_equal(interior(mo), interior(mg))
 
 
+def test_given_metrics_on_a_tensor_grid(gpu):
+    """Metrics handed to ocfd_gpu_init (Iflag_Gridtype = 31) on a tensor-product grid take the
+    stored-array path and give the separable path's results bit for bit."""
+    c = cases.flatplate(nx=40, ny=24, nz=12, scheme="HYBRID", lx=0.01, ly=0.004, y1=2e-5)
+    out = []
+    for given in (False, True):
+        g = gpu.Solver(c)
+        m = g.metrics()
+        if given:
+            g.close()
+            g = gpu.Solver(c, metrics=m)
+            assert gpu.lib().ocfd_gpu_is_separable() == 0
+        g.init_state()
+        for s in range(2):
+            g.tt = s * c.dt
+            g.step(c.dt, 0, 1)
+        out.append(g.download_state())
+        g.close()
+    (f0, d0, p0), (f1, d1, p1) = out
+    assert np.array_equal(f0, f1)
+    assert np.array_equal(interior(p0), interior(p1)) and np.array_equal(interior(d0), interior(d1))
+
+
 def test_two_species_realgas_bitwise(oracle, gpu):
     """N_SPEC = 2 (O2/N2): species transport, Newton T(E), Fickian diffusion with enthalpy flux."""
     c = cases.isotropic(n=12, species=["O2", "N2"], Y=[0.233, 0.767])
