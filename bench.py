@@ -54,8 +54,9 @@ def parse():
                     help="jet workload: compare FP64 chemistry with the gated surrogate (trains it first)")
     ap.add_argument("--character", action="store_true",
                     help="characteristic-space inviscid flux (IF_Scheme_Character = 1) instead of component-wise")
-    ap.add_argument("--tiles", default="auto", choices=["auto", "default"],
-                    help="stencil tiles: timed by the autotuner before the warm-up (auto) or the defaults")
+    ap.add_argument("--tiles", default="auto",
+                    help="stencil tiles: 'auto' (timed by the autotuner before the warm-up), 'default', or an "
+                         "explicit choice of 8 comma-separated ints (see ocfd_gpu_autotune)")
     ap.add_argument("--nz", type=int, default=None,
                     help="cells along z (flat plate: 128 = full; jet: 256 = full), for small profiling runs")
     return ap.parse_args()
@@ -507,7 +508,10 @@ def main_ours(a):
     chk = solver._chk
     reac, nsub = int(getattr(c, "if_reaction", 0) or 0), int(getattr(c, "nsub", 1) or 1)
     tiles = {"mode": a.tiles, "choice": g.tiles()}
-    if a.tiles == "auto":
+    if a.tiles not in ("auto", "default"):
+        g.set_tiles([int(x) for x in a.tiles.split(",")])
+        tiles = {"mode": "given", "choice": g.tiles()}
+    elif a.tiles == "auto":
         chk(L.ocfd_gpu_run(dt, tt, 1, reac, nsub))  # one step so that the tuner sees a running state
         tt += dt
         choice, tms = g.autotune(reps=5)
