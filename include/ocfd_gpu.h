@@ -175,8 +175,10 @@ int ocfd_gpu_chem_advance(double dt2, int nsub);
  * if_reaction), flow(dt/2). Captured as a CUDA graph after the first call with a given dt. */
 int ocfd_gpu_step(double dt, double tt, int if_reaction, int nsub);
 
-/* nsteps consecutive ocfd_gpu_step calls (solver time tt0, tt0+dt, ...) replayed back to back on
- * the device with one status check at the end; the reference's time loop without I/O steps. */
+/* nsteps consecutive ocfd_gpu_step calls (solver time tt0, tt0+dt, ..., accumulated as the
+ * reference's tt = tt + dt) replayed back to back on the device with one status check at the end;
+ * the reference's time loop without I/O steps. Chunks of 16 steps are one graph launch each (the
+ * captured step as a child graph, the step's wall-disturbance time taken on the device). */
 int ocfd_gpu_run(double dt, double tt0, int nsteps, int if_reaction, int nsub);
 
 /* Downloads the state; any pointer may be NULL to skip that part. */

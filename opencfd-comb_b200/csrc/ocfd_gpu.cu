@@ -30,6 +30,13 @@ long long sg_cells_rejected(long long* reasons);
 __global__ void k_fill(double* p, long long n, double v);
 __global__ void k_jacobian(const double* X, const double* Y, const double* Z, double* const* m);
 __global__ void k_metric_ratio(double* const* m, long long H);
+// the wall-disturbance time of the next step of a multi-step run: ht = seq[counter++] (one thread;
+// the steps of a run are ordered on one stream, so the counter needs no atomics)
+__global__ void k_next_ht(const double* seq, int* counter, double* ht) {
+  const int c = *counter;
+  *ht = seq[c];
+  *counter = c + 1;
+}
 }  // namespace ocfd
 #include "ocfd_launch.h"
 
@@ -82,8 +89,11 @@ struct Lib {
   Geo geo{};
   int inlet_kind = 0, upper_kind = 0, outlet = 0;
   std::vector<double> tm, fait;
-  // graph of one Strang step
-  cudaGraphExec_t gexec = nullptr;
+  // graph of one Strang step (the captured graph is kept as the child of the chunk graph, which
+  // replays RUN_CHUNK steps with one launch)
+  cudaGraphExec_t gexec = nullptr, gchunk = nullptr;
+  cudaGraph_t gstep = nullptr;
+  int* ht_counter = nullptr;
   double g_dt = 0;
   int g_ifr = -1, g_nsub = -1, g_par = -1, g_launches = 0;
   // stencil tile choices (ocfd_gpu_set_tiles / ocfd_gpu_autotune): flow-flux tile shape per
@@ -570,6 +580,12 @@ std::string tune_key() {
 }
 
 void set_geo_device_ptrs();
+// forgets the captured step and the chunk graph built on it (re-captured at the next step)
+void drop_graphs() {
+  if (L->gchunk) { CK(cudaGraphExecDestroy(L->gchunk)); L->gchunk = nullptr; }
+  if (L->gexec) { CK(cudaGraphExecDestroy(L->gexec)); L->gexec = nullptr; }
+  if (L->gstep) { CK(cudaGraphDestroy(L->gstep)); L->gstep = nullptr; }
+}
 // the 19 metric arrays of a tensor-product grid, as the general path computes them
 // (comput_Jacobian3d, the periodic exchange, Akx1..Asz1), beside the separable form
 void ensure_stored_metrics() {
@@ -603,10 +619,7 @@ void apply_tiles(const int* c) {
   L->met_flux = c[5] != 0;
   L->met_ev = c[6] != 0;
   L->met_div = c[7] != 0;
-  if (L->gexec) {  // the captured step holds the old launches
-    CK(cudaGraphExecDestroy(L->gexec));
-    L->gexec = nullptr;
-  }
+  drop_graphs();  // the captured step holds the old launches
 }
 
 // times every candidate of each family on the current state (one warm-up launch, then reps
@@ -902,6 +915,9 @@ void fill_trans(DevConst& c, const ocfd_transport* tr, int ns) {
 void release() {
   if (!L) return;
   if (L->gexec) cudaGraphExecDestroy(L->gexec);
+  if (L->gchunk) cudaGraphExecDestroy(L->gchunk);
+  if (L->gstep) cudaGraphDestroy(L->gstep);
+  if (L->ht_counter) cudaFree(L->ht_counter);
   for (auto& e : L->ev_pool) { cudaEventDestroy(e.first); cudaEventDestroy(e.second); }
   if (L->arena) cudaFree(L->arena);
   if (L->amu_keep) cudaFree(L->amu_keep);
@@ -1546,7 +1562,7 @@ void ensure_graph(double dt, int if_reaction, int nsub) {
   if (L->gexec && L->g_dt == dt && L->g_ifr == if_reaction && L->g_nsub == nsub && L->g_par == L->cur &&
       L->g_mode == L->chem_mode)
     return;
-  if (L->gexec) { CK(cudaGraphExecDestroy(L->gexec)); L->gexec = nullptr; }
+  drop_graphs();
   int cur0 = L->cur;
   long long l0 = L->launches;
   cudaGraph_t graph;
@@ -1563,12 +1579,35 @@ void ensure_graph(double dt, int if_reaction, int nsub) {
     throw;
   }
   CK(cudaStreamEndCapture(L->st, &graph));
+  L->gstep = graph;
   CK(cudaGraphInstantiate(&L->gexec, graph, 0));
-  CK(cudaGraphDestroy(graph));
   L->g_dt = dt; L->g_ifr = if_reaction; L->g_nsub = nsub; L->g_par = cur0; L->g_mode = L->chem_mode;
   L->g_launches = (int)(L->launches - l0);
   L->launches = l0;
   L->cur = cur0;  // six stages: the Et buffer parity returns to its start value
+}
+// RUN_CHUNK steps as one graph: [k_next_ht -> step] x RUN_CHUNK, each step a child node holding a
+// copy of the captured step, so that a multi-step run needs no host launch per step
+constexpr int RUN_CHUNK = 16;
+void ensure_chunk() {
+  if (L->gchunk) return;
+  cudaGraph_t cg;
+  CK(cudaGraphCreate(&cg, 0));
+  cudaGraphNode_t prev = nullptr;
+  for (int s = 0; s < RUN_CHUNK; s++) {
+    cudaKernelNodeParams kp{};
+    void* args[3] = {&L->ht_seq, &L->ht_counter, &L->ht_dev};
+    kp.func = (void*)k_next_ht;
+    kp.gridDim = dim3(1);
+    kp.blockDim = dim3(1);
+    kp.kernelParams = args;
+    cudaGraphNode_t kn, cn;
+    CK(cudaGraphAddKernelNode(&kn, cg, prev ? &prev : nullptr, prev ? 1 : 0, &kp));
+    CK(cudaGraphAddChildGraphNode(&cn, cg, &kn, 1, L->gstep));
+    prev = cn;
+  }
+  CK(cudaGraphInstantiate(&L->gchunk, cg, 0));
+  CK(cudaGraphDestroy(cg));
 }
 }  // namespace
 
@@ -1601,21 +1640,39 @@ int ocfd_gpu_run(double dt, double tt0, int nsteps, int if_reaction, int nsub) {
     if (if_reaction && !L->have_kin) { g_err = "no reaction mechanism given to ocfd_gpu_init"; return OCFD_ERR_PARAM; }
     if (nsteps <= 0) return 0;
     if (nsub < 1) nsub = 1;
-    if (nsteps > L->ht_cap) {
+    if (nsteps > L->ht_cap) {  // the chunk graph holds the old sequence pointer
+      CK(cudaStreamSynchronize(L->st));
+      if (L->gchunk) { CK(cudaGraphExecDestroy(L->gchunk)); L->gchunk = nullptr; }
       if (L->ht_seq) cudaFree(L->ht_seq);
       if (L->ht_seq_host) cudaFreeHost(L->ht_seq_host);
-      CK(cudaMalloc(&L->ht_seq, sizeof(double) * nsteps));
-      CK(cudaMallocHost(&L->ht_seq_host, sizeof(double) * nsteps));
-      L->ht_cap = nsteps;
+      const int cap = std::max(nsteps, 4096);
+      CK(cudaMalloc(&L->ht_seq, sizeof(double) * cap));
+      CK(cudaMallocHost(&L->ht_seq_host, sizeof(double) * cap));
+      L->ht_cap = cap;
     }
+    if (!L->ht_counter) CK(cudaMalloc(&L->ht_counter, sizeof(int)));
     CK(cudaStreamSynchronize(L->st));
-    for (int s = 0; s < nsteps; s++) L->ht_seq_host[s] = wall_ht(tt0 + s * dt);
-    CK(cudaMemcpyAsync(L->ht_seq, L->ht_seq_host, sizeof(double) * nsteps, cudaMemcpyHostToDevice, L->st));
-    ensure_graph(dt, if_reaction, nsub);
+    double tt = tt0;  // tt = tt + dt after every step (OCFD_NS_Solver.f90:46)
     for (int s = 0; s < nsteps; s++) {
-      CK(cudaMemcpyAsync(L->ht_dev, L->ht_seq + s, sizeof(double), cudaMemcpyDeviceToDevice, L->st));
+      L->ht_seq_host[s] = wall_ht(tt);
+      tt = tt + dt;
+    }
+    CK(cudaMemcpyAsync(L->ht_seq, L->ht_seq_host, sizeof(double) * nsteps, cudaMemcpyHostToDevice, L->st));
+    CK(cudaMemsetAsync(L->ht_counter, 0, sizeof(int), L->st));
+    ensure_graph(dt, if_reaction, nsub);
+    int s = 0;
+    if (nsteps >= RUN_CHUNK) {
+      ensure_chunk();
+      for (; s + RUN_CHUNK <= nsteps; s += RUN_CHUNK) {
+        CK(cudaGraphLaunch(L->gchunk, L->st));
+        L->launches += (long long)RUN_CHUNK * (L->g_launches + 1);
+      }
+    }
+    for (; s < nsteps; s++) {
+      k_next_ht<<<1, 1, 0, L->st>>>(L->ht_seq, L->ht_counter, L->ht_dev);
+      LAUNCH_CHECK();
       CK(cudaGraphLaunch(L->gexec, L->st));
-      L->launches += L->g_launches;
+      L->launches += L->g_launches + 1;
     }
     return check_status();
   });
@@ -2010,7 +2067,7 @@ int ocfd_gpu_keep_viscosity(int on) {
     }
     if (L->keep_amu != want) {
       L->keep_amu = want;
-      if (L->gexec) { CK(cudaGraphExecDestroy(L->gexec)); L->gexec = nullptr; }
+      drop_graphs();
     }
     return 0;
   });

@@ -82,6 +82,14 @@ class Solver:
         self.istep += 1
         self.tt += dt
 
+    def run(self, dt, nsteps, if_reaction=0, nsub=1):
+        """nsteps steps back to back (NS_solver's loop without I/O steps): chunks of 16 steps are
+        one graph launch each, the wall-disturbance time of every step is picked on the device."""
+        _chk(lib().ocfd_gpu_run(dt, self.tt, nsteps, if_reaction, nsub))
+        self.istep += nsteps
+        for _ in range(nsteps):
+            self.tt += dt
+
     def show_flow_msg(self):
         """Mean total energy and kinetic energy (OCFD_Time_Adv.f90:210-223)."""
         e, k = C.c_double(), C.c_double()

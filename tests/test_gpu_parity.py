@@ -151,6 +151,33 @@ def test_separable_metrics_match_oracle(oracle, gpu):
     assert np.array_equal(interior(mo), interior(mg))
 
 
+@pytest.mark.parametrize("kind", ["flatplate", "jet"])
+def test_multistep_run_equals_single_steps(gpu, kind):
+    """ocfd_gpu_run (chunks of 16 steps per graph launch plus single steps, the wall-disturbance
+    time taken on the device) gives the same state as one ocfd_gpu_step per step."""
+    if kind == "flatplate":
+        c = cases.flatplate(nx=40, ny=24, nz=12, scheme="HYBRID", lx=0.01, ly=0.004, y1=2e-5)
+        n, reac, nsub = 37, 0, 1
+    else:
+        c = cases.jet(nx=24, ny=16, nz=16)
+        n, reac, nsub = 18, 1, c.nsub
+    out = []
+    for multi in (False, True):
+        g = gpu.Solver(c)
+        g.init_state()
+        if multi:
+            g.run(c.dt, n, reac, nsub)
+        else:
+            for s in range(n):
+                g.step(c.dt, reac, nsub)
+        assert abs(g.tt - n * c.dt) < 1e-12 * n * c.dt
+        out.append(g.download_state())
+        g.close()
+    (f0, d0, p0), (f1, d1, p1) = out
+    assert np.array_equal(f0, f1)
+    assert np.array_equal(interior(p0), interior(p1)) and np.array_equal(interior(d0), interior(d1))
+
+
 def test_given_metrics_on_a_tensor_grid(gpu):
     """Metrics handed to ocfd_gpu_init (Iflag_Gridtype = 31) on a tensor-product grid take the
     stored-array path and give the separable path's results bit for bit."""
