@@ -519,9 +519,11 @@ def main_ours(a):
                  "candidate_ms": {"flux_x": tms[0:3], "flux_y": tms[3:6], "flux_z": tms[6:9],
                                   "visc_ev_kc8_16_32_64": tms[9:13],
                                   "visc_div_kc8_16_32_64_percell": tms[13:18],
-                                  "stored_metrics_flux_xyz_ev_div": tms[18:23]},
+                                  "stored_metrics_flux_xyz_ev_div": tms[18:23],
+                                  "flow_rhs_visc_after_beside": tms[23:25]},
                  "choice_keys": ["flux_x_shape", "flux_y_shape", "flux_z_shape", "visc_ev_kc", "visc_div_kc",
-                                 "flux_stored_metrics", "visc_ev_stored_metrics", "visc_div_stored_metrics"]}
+                                 "flux_stored_metrics", "visc_ev_stored_metrics", "visc_div_stored_metrics",
+                                 "visc_ev_second_stream"]}
     chk(L.ocfd_gpu_run(dt, tt, a.warmup, reac, nsub))
     tt += a.warmup * dt
 

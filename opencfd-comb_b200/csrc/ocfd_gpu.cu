@@ -11,6 +11,7 @@
 #include <cstring>
 #include <map>
 #include <stdexcept>
+#include <utility>
 #include <string>
 #include <vector>
 
@@ -92,6 +93,10 @@ struct Lib {
   // graph of one Strang step (the captured graph is kept as the child of the chunk graph, which
   // replays RUN_CHUNK steps with one launch)
   cudaGraphExec_t gexec = nullptr, gchunk = nullptr;
+  // second stream of a stage: k_visc_ev and its halo exchange run beside the flux sweeps
+  cudaStream_t st2 = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+  bool fork_visc = true;
   cudaGraph_t gstep = nullptr;
   int* ht_counter = nullptr;
   double g_dt = 0;
@@ -446,6 +451,49 @@ void visc_div_launch(const DivArgs& da) {
   LAUNCH_CHECK();
 }
 
+// the flow part of a stage's right-hand side: the three flux sweeps into du, the viscous fluxes
+// Ev with their halo exchange, and their divergence added to du
+template <int NS>
+void flow_rhs_t(const FluxArgs& fa) {
+  const bool visc = L->P.if_viscous == 1;
+  auto visc_ev_part = [&]() {
+    {
+      KTimer t(KC_VISC_EV);
+      visc_ev_launch<NS>(visc_args<NS>());
+    }
+    exchange({L->ev[0], L->ev[1], L->ev[2], L->ev[3]}, 1);
+    exchange({L->ev[4], L->ev[5], L->ev[6], L->ev[7]}, 2);
+    exchange({L->ev[8], L->ev[9], L->ev[10], L->ev[11]}, 4);
+  };
+  // k_visc_ev reads only the primitives (and, for N_SPEC > 1, the transport and enthalpy fluxes
+  // computed above) and writes only Ev, while the flux sweeps write du: the two run side by side
+  // on two streams (two branches of the step's graph), joined before k_visc_div. The per-kernel
+  // timing mode keeps them in order.
+  const bool fork = visc && L->fork_visc && !L->prof && L->st2;
+  if (fork) {
+    CK(cudaEventRecord(L->ev_fork, L->st));
+    CK(cudaStreamWaitEvent(L->st2, L->ev_fork, 0));
+    std::swap(L->st, L->st2);  // the launch helpers use L->st
+    try {
+      visc_ev_part();
+    } catch (...) {
+      std::swap(L->st, L->st2);
+      throw;
+    }
+    CK(cudaEventRecord(L->ev_join, L->st));
+    std::swap(L->st, L->st2);
+  }
+  for (int dd = 0; dd < 3; dd++) launch_flux(dd, fa);
+  if (visc) {
+    if (fork) CK(cudaStreamWaitEvent(L->st, L->ev_join, 0));
+    else visc_ev_part();
+    {
+      KTimer t(KC_VISC_DIV);
+      visc_div_launch(div_args());
+    }
+  }
+}
+
 template <int NS>
 void stage_t(int krk, double dt1) {
   const long long N = L->hc.N, H = L->hc.H;
@@ -505,20 +553,7 @@ void stage_t(int krk, double dt1) {
   }
   fa.fs = nullptr;
   fa.out = L->du;
-  for (int dd = 0; dd < 3; dd++) launch_flux(dd, fa);
-  if (L->P.if_viscous == 1) {
-    {
-      KTimer t(KC_VISC_EV);
-      visc_ev_launch<NS>(visc_args<NS>());
-    }
-    exchange({L->ev[0], L->ev[1], L->ev[2], L->ev[3]}, 1);
-    exchange({L->ev[4], L->ev[5], L->ev[6], L->ev[7]}, 2);
-    exchange({L->ev[8], L->ev[9], L->ev[10], L->ev[11]}, 4);
-    {
-      KTimer t(KC_VISC_DIV);
-      visc_div_launch(div_args());
-    }
-  }
+  flow_rhs_t<NS>(fa);
   // N_SPEC = 1: di = d over the whole array (OCFD_Time_Adv.f90:45-52). Nothing between the stage
   // start and here reads di, and the inline transport of k_visc_ev must see the previous stage's
   // di (comput_Amu_Amk_AMD runs before the copy in the reference), so the copy happens here.
@@ -564,11 +599,12 @@ void chem_t(double dt2, int nsub) {
 
 // ---------------------------------------------------------------- stencil tile autotuner
 // Tile choices {flux x, y, z shape; k_visc_ev, k_visc_div k planes per block; metric form of the
-// flux sweeps, k_visc_ev, k_visc_div}. Every choice gives bit-identical results (a tile decides
+// flux sweeps, k_visc_ev, k_visc_div; k_visc_ev beside the flux sweeps on a second stream or after
+// them}. Every choice gives bit-identical results (a tile decides
 // which block computes a point, not how; the stored metric arrays hold the values the separable
 // form computes), so the tuner is free to pick by time alone. Choices are remembered per
 // configuration in the process.
-constexpr int TUNE_N = 8, TUNE_TIMES = 3 * FLUX_TILE_SHAPES + 9 + 5;
+constexpr int TUNE_N = 9, TUNE_TIMES = 3 * FLUX_TILE_SHAPES + 9 + 5 + 2;
 std::map<std::string, std::array<int, TUNE_N>> g_tune_cache;
 
 std::string tune_key() {
@@ -619,6 +655,7 @@ void apply_tiles(const int* c) {
   L->met_flux = c[5] != 0;
   L->met_ev = c[6] != 0;
   L->met_div = c[7] != 0;
+  L->fork_visc = c[8] != 0;
   drop_graphs();  // the captured step holds the old launches
 }
 
@@ -662,6 +699,7 @@ void tune_t(int reps, int* best, double* ms) {
     }
     best[3] = best[4] = VE_KC;
     best[5] = best[6] = best[7] = L->sep ? 0 : 1;
+    best[8] = 1;
     for (int m = 3 * FLUX_TILE_SHAPES; m < TUNE_TIMES; m++) ms[m] = -1.0;
     if (P.if_viscous == 1) {
       double t_ev = 1e300, t_div = 1e300;
@@ -715,6 +753,22 @@ void tune_t(int reps, int* best, double* ms) {
         for (int m = 0; m < 4; m++) if (VE_KC_CHOICES[m] == best[4]) mj = m;
         best[7] = ms[M0 + 4] < ms[3 * FLUX_TILE_SHAPES + 4 + mj] ? 1 : 0;
       }
+    }
+    if (P.if_viscous == 1) {  // k_visc_ev beside the flux sweeps or after them: the whole flow
+                              // right-hand side of a stage with the chosen tiles, both ways
+      const int M1 = 3 * FLUX_TILE_SHAPES + 9 + 5;
+      for (int d = 0; d < 3; d++) L->flux_ts[d] = best[d];
+      L->kc_ev = best[3];
+      L->kc_div = best[4];
+      L->met_flux = best[5] && L->sep;
+      L->met_ev = best[6] && L->sep;
+      L->met_div = best[7] && L->sep;
+      const FluxArgs fr = flow_flux_args();
+      L->fork_visc = false;
+      ms[M1] = timed([&] { flow_rhs_t<NS>(fr); });
+      L->fork_visc = true;
+      ms[M1 + 1] = timed([&] { flow_rhs_t<NS>(fr); });
+      best[8] = ms[M1 + 1] < ms[M1] ? 1 : 0;
     }
   } catch (...) {
     cudaEventDestroy(e0);
@@ -943,6 +997,9 @@ void release() {
   if (L->ht_seq_host) cudaFreeHost(L->ht_seq_host);
   for (auto& e : L->uev)
     if (e) cudaEventDestroy(e);
+  if (L->ev_fork) cudaEventDestroy(L->ev_fork);
+  if (L->ev_join) cudaEventDestroy(L->ev_join);
+  if (L->st2) cudaStreamDestroy(L->st2);
   if (L->st) cudaStreamDestroy(L->st);
   delete L;
   L = nullptr;
@@ -1248,6 +1305,9 @@ int ocfd_gpu_init(const ocfd_params* p, const ocfd_thermo* th, const ocfd_kineti
     L->P = *p;
     L->NS = p->n_spec;
     CK(cudaStreamCreateWithFlags(&L->st, cudaStreamNonBlocking));
+    CK(cudaStreamCreateWithFlags(&L->st2, cudaStreamNonBlocking));
+    CK(cudaEventCreateWithFlags(&L->ev_fork, cudaEventDisableTiming));
+    CK(cudaEventCreateWithFlags(&L->ev_join, cudaEventDisableTiming));
     DevConst& c = L->hc;
     c.nx = p->nx; c.ny = p->ny; c.nz = p->nz; c.ns = p->n_spec;
     c.HX = p->nx + 2 * OCFD_L; c.HY = p->ny + 2 * OCFD_L; c.HZ = p->nz + 2 * OCFD_L;
@@ -2199,8 +2259,11 @@ int ocfd_gpu_set_tiles(const int* choice) {
       g_err = "k planes per block must be >= 1 (k_visc_div: >= 0, 0 = per-cell form)";
       return OCFD_ERR_PARAM;
     }
-    for (int m = 5; m < 8; m++)
-      if (choice[m] != 0 && choice[m] != 1) { g_err = "metric form must be 0 (computed) or 1 (stored)"; return OCFD_ERR_PARAM; }
+    for (int m = 5; m < 9; m++)
+      if (choice[m] != 0 && choice[m] != 1) {
+        g_err = "metric forms and the second-stream switch must be 0 or 1";
+        return OCFD_ERR_PARAM;
+      }
     apply_tiles(choice);
     return 0;
   });
@@ -2214,6 +2277,7 @@ int ocfd_gpu_get_tiles(int* choice) {
   choice[5] = L->sep ? (int)L->met_flux : 1;
   choice[6] = L->sep ? (int)L->met_ev : 1;
   choice[7] = L->sep ? (int)L->met_div : 1;
+  choice[8] = (int)L->fork_visc;
   return 0;
 }
 

@@ -221,19 +221,20 @@ class Solver:
     def autotune(self, reps=5):
         """Times the candidate tile shapes on the current state and applies the fastest; returns
         (choice, ms per launch of each candidate)."""
-        ch = (C.c_int * 8)()
-        ms = (C.c_double * 23)()
+        ch = (C.c_int * 9)()
+        ms = (C.c_double * 25)()
         _chk(lib().ocfd_gpu_autotune(reps, ch, ms))
         return list(ch), list(ms)
 
     def set_tiles(self, choice):
-        """choice: 8 ints (see ocfd_gpu_autotune); a 5-int choice keeps the computed metric form."""
-        choice = list(choice) + [0] * (8 - len(choice))
-        ch = (C.c_int * 8)(*choice)
+        """choice: 9 ints (see ocfd_gpu_autotune); a shorter choice keeps the computed metric
+        form and the second stream of the defaults."""
+        choice = list(choice) + [0, 0, 0, 1][len(choice) - 5:] if len(choice) < 9 else list(choice)
+        ch = (C.c_int * 9)(*choice)
         _chk(lib().ocfd_gpu_set_tiles(ch))
 
     def tiles(self):
-        ch = (C.c_int * 8)()
+        ch = (C.c_int * 9)()
         _chk(lib().ocfd_gpu_get_tiles(ch))
         return list(ch)
 

@@ -9,11 +9,11 @@ from ocfd_b200 import abi, cases, solver
 pytestmark = pytest.mark.gpu
 
 CHOICES = [
-    [0, 0, 0, 16, 16, 0, 0, 0],
-    [1, 1, 1, 8, 32, 0, 0, 0],
-    [2, 2, 2, 64, 8, 1, 0, 1],
-    [1, 2, 0, 3, 5, 0, 1, 0],  # k chunks that do not divide nz
-    [0, 1, 2, 16, 0, 1, 1, 1],  # per-cell k_visc_div, stored metric arrays everywhere
+    [0, 0, 0, 16, 16, 0, 0, 0, 0],  # everything on one stream
+    [1, 1, 1, 8, 32, 0, 0, 0, 1],
+    [2, 2, 2, 64, 8, 1, 0, 1, 1],
+    [1, 2, 0, 3, 5, 0, 1, 0, 0],  # k chunks that do not divide nz
+    [0, 1, 2, 16, 0, 1, 1, 1, 1],  # per-cell k_visc_div, stored metric arrays everywhere
 ]
 
 
@@ -31,7 +31,7 @@ def _run(c, choice=None, tune=False, steps=2):
     tuned = None
     if choice is not None:
         g.set_tiles(choice)
-        expect = list(choice) if solver.lib().ocfd_gpu_is_separable() else choice[:5] + [1, 1, 1]
+        expect = list(choice) if solver.lib().ocfd_gpu_is_separable() else choice[:5] + [1, 1, 1] + choice[8:]
         assert g.tiles() == expect
     if tune:
         tuned = g.autotune(reps=2)
@@ -59,7 +59,7 @@ def test_autotune_choice_and_solution():
     st, (choice, ms) = _run(c, tune=True)
     assert choice[0] in (0, 1, 2) and choice[1] in (0, 1, 2) and choice[2] in (0, 1, 2)
     assert choice[3] in (8, 16, 32, 64) and choice[4] in (0, 8, 16, 32, 64)
-    assert all(x in (0, 1) for x in choice[5:])
+    assert all(x in (0, 1) for x in choice[5:]) and len(choice) == 9
     assert all(t > 0 for t in ms), ms  # viscous separable case: every candidate timed
     for d in range(3):
         assert ms[3 * d + choice[d]] == min(ms[3 * d:3 * d + 3])
@@ -72,7 +72,7 @@ def test_autotune_remembers_the_configuration():
     g = solver.Solver(c)
     g.init_state()
     first, _ = g.autotune(reps=2)
-    g.set_tiles([0, 0, 0, 16, 16, 0, 0, 0])
+    g.set_tiles([0, 0, 0, 16, 16, 0, 0, 0, 1])
     again, ms = g.autotune(reps=0)  # cached: applied without timing
     assert again == first and all(t == -1.0 for t in ms)
     assert g.tiles() == first
@@ -83,7 +83,7 @@ def test_bad_tile_choice_is_rejected():
     c = _case("isotropic")
     g = solver.Solver(c)
     g.init_state()
-    for bad in ([3, 0, 0, 16, 16], [0, -1, 0, 16, 16], [0, 0, 0, 0, 16], [0, 0, 0, 16, -1], [0, 0, 0, 16, 16, 2]):
+    for bad in ([3, 0, 0, 16, 16], [0, -1, 0, 16, 16], [0, 0, 0, 0, 16], [0, 0, 0, 16, -1], [0, 0, 0, 16, 16, 2], [0, 0, 0, 16, 16, 0, 0, 0, 3]):
         with pytest.raises(solver.OcfdError):
             g.set_tiles(bad)
     g.close()
