@@ -57,9 +57,20 @@ def parse():
     ap.add_argument("--tiles", default="auto",
                     help="stencil tiles: 'auto' (timed by the autotuner before the warm-up), 'default', or an "
                          "explicit choice of 8 comma-separated ints (see ocfd_gpu_autotune)")
+    ap.add_argument("--profile-region", action="store_true",
+                    help="bracket the timed region with cudaProfilerStart/Stop, for ncu --profile-from-start off")
     ap.add_argument("--nz", type=int, default=None,
                     help="cells along z (flat plate: 128 = full; jet: 256 = full), for small profiling runs")
     return ap.parse_args()
+
+
+def profiler(on, enabled):
+    """cudaProfilerStart / Stop around a timed region when --profile-region is given."""
+    if not enabled:
+        return
+    import torch
+    rt = torch.cuda.cudart()
+    (rt.cudaProfilerStart if on else rt.cudaProfilerStop)()
 
 
 def make_case(workload, nz=None):
@@ -364,7 +375,9 @@ def main_surrogate(a):
     k = max(1, min(a.steps, 5))
     with Clocks(0) as clk:
         ms_plain = timed(plain, k)
+        profiler(True, a.profile_region)
         ms_gated = timed(gated, k)
+        profiler(False, a.profile_region)
         ms_net = timed(network, k)
     acc = sg.evaluate(n=n, seed=4242, tol_T=a.sg_tol)
     peaks_file = os.path.join(ROOT, "MEASURED_PEAKS.json")
@@ -531,9 +544,11 @@ def main_ours(a):
     barrier()
     l0 = L.ocfd_gpu_launch_count()
     with Clocks(0) as clk:
+        profiler(True, a.profile_region)
         chk(L.ocfd_gpu_event_record(0))
         chk(L.ocfd_gpu_run(dt, tt, a.steps, reac, nsub))
         chk(L.ocfd_gpu_event_record(1))
+        profiler(False, a.profile_region)
         ms = C.c_double()
         chk(L.ocfd_gpu_event_elapsed(0, 1, C.byref(ms)))
     tt += a.steps * dt

@@ -352,6 +352,12 @@ long long ocfd_gpu_surrogate_blob(float* host, long long nfloats, int set);
 int ocfd_gpu_surrogate_grad(int B, const float* x, const float* t, float* grads, double* loss);
 int ocfd_gpu_chem_temperature(int n, const double* d_di, const double* d_e, double* d_T);
 
+/* Inference form of the network: 1 (default) = one fused tcgen05 kernel for the four layers (the
+ * hidden activations stay in shared memory / TMEM), 0 = one GEMM per layer through global memory;
+ * both issue the same MMAs and epilogue arithmetic. on < 0 only queries. Returns the previous
+ * setting. */
+int ocfd_gpu_surrogate_fused(int on);
+
 /* Chemistry of the flow solver's Strang step (ocfd_gpu_step, ocfd_gpu_run, ocfd_gpu_chem_advance):
  * mode 0 the FP64 integrator of Chemical_time_advance (default), mode 1 the gated surrogate, whose
  * rejected cells (|T_energy - T_pred| > tol_T, negative composition, outside the training range)

@@ -215,6 +215,199 @@ int launch_gemm(const GemmArgs& g, cudaStream_t st) {
   return g.N > 128 ? launch_bn<256>(g, st) : launch_bn<128>(g, st);
 }
 
+// ---------------------------------------------------------------- fused inference pass
+// One CTA (8 warps) carries a 128-row tile through the four layers. Per layer the MMAs accumulate
+// into a 128 x 256 FP32 TMEM accumulator; the epilogue (bias, GELU, BF16) writes the activations
+// back to shared memory in the K-major layout, where they are the next layer's A operand, so only
+// the 16 inputs and 16 outputs of a row touch global memory. The 256 x 256 weights stream through
+// two 32-wide K-chunk buffers (chunk c + 1 is staged while the MMAs of chunk c run); all CTAs read
+// the same 272 KB of weights, which stay in L2. Each layer issues the same K = 16 MMAs in the same
+// order as the layer-by-layer GEMMs and the epilogues evaluate the same expressions.
+namespace fused {
+constexpr int MT = 128, THR = 256, KC = 32, NK = 256 / KC;
+constexpr int ACT_BYTES = MT * 256 * 2, X_BYTES = MT * 16 * 2, WB_BYTES = 256 * KC * 2;
+constexpr int BYTES = ACT_BYTES + X_BYTES + 2 * WB_BYTES + 64;
+static_assert(2 * BYTES <= 226 * 1024, "two blocks per SM");
+}  // namespace fused
+
+// stage rows r0 .. r0 + R - 1, columns k0 .. k0 + KN - 1 of a row-major BF16 matrix (row stride ld)
+// into the K-major layout of an R-row tile; rows at or beyond nrows are zero. Eight consecutive
+// lanes fill one 128-byte core-matrix column (no bank conflict); a thread's 16-byte loads are all
+// issued before its stores.
+template <int R, int KN>
+__device__ __forceinline__ void stage_rows(uint8_t* dst, const __nv_bfloat16* src, long long ld, int r0, int nrows,
+                                           int k0) {
+  constexpr int CK = KN / 8, ITEMS = R * CK, PER = (ITEMS + fused::THR - 1) / fused::THR;
+  uint4 v[PER];
+#pragma unroll
+  for (int it = 0; it < PER; it++) {
+    const int c = threadIdx.x + it * fused::THR;
+    if (c < ITEMS) {
+      const int w = c % (8 * CK), r = (c / (8 * CK)) * 8 + (w & 7), kc = w >> 3;
+      v[it] = r0 + r < nrows ? __ldg(reinterpret_cast<const uint4*>(src + (long long)(r0 + r) * ld + k0 + kc * 8))
+                             : make_uint4(0u, 0u, 0u, 0u);
+    }
+  }
+#pragma unroll
+  for (int it = 0; it < PER; it++) {
+    const int c = threadIdx.x + it * fused::THR;
+    if (c < ITEMS) {
+      const int w = c % (8 * CK), r = (c / (8 * CK)) * 8 + (w & 7), kc = w >> 3;
+      *reinterpret_cast<uint4*>(dst + tc::kmajor_off(r, kc * 8, R)) = v[it];
+    }
+  }
+}
+
+__global__ void __launch_bounds__(fused::THR, 2) k_mlp_fused(MlpArgs a) {
+  using namespace fused;
+  extern __shared__ __align__(1024) uint8_t sm[];
+  uint8_t* act = sm;                      // 128 x 256 activations, K-major
+  uint8_t* xin = sm + ACT_BYTES;          // 128 x 16 inputs
+  uint8_t* wb0 = xin + X_BYTES;           // weight chunk buffers (256 x 32, or W0 / W3 whole)
+  uint8_t* wb1 = wb0 + WB_BYTES;
+  uint64_t* bar = reinterpret_cast<uint64_t*>(wb1 + WB_BYTES);  // one mbarrier per buffer
+  uint32_t* tslot = reinterpret_cast<uint32_t*>(bar + 2);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int m0 = blockIdx.x * MT;
+
+  if (warp == 0) tc::tmem_alloc(tslot, 256);
+  if (tid == 0) {
+    tc::mbar_init(&bar[0], 1);
+    tc::mbar_init(&bar[1], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  tc::fence_before();
+  __syncthreads();
+  tc::fence_after();
+  const uint32_t tmem = *tslot;
+  int nd[2] = {0, 0};  // completions of each mbarrier waited for so far
+  // thread 0 waits for the next completion of barrier b; the block learns the outcome
+  auto wait_bar = [&](int b) -> bool {
+    bool o = true;
+    if (tid == 0) o = tc::mbar_wait(&bar[b], (uint32_t)(nd[b] & 1), WAIT_LIMIT);
+    nd[b]++;
+    const bool all = __syncthreads_and(o ? 1 : 0) != 0;
+    tc::fence_after();
+    return all;
+  };
+  // hidden-layer epilogue: warp w reads TMEM lanes 32 (w % 4) .. + 31 (its rows) and the 128
+  // columns of half w / 4, then writes bias + GELU as BF16 into act
+  auto hidden_epilogue = [&](const float* bias) {
+    const int rl = 32 * (warp & 3) + lane, c_lo = (warp >> 2) * 128;
+#pragma unroll 1
+    for (int c0 = c_lo; c0 < c_lo + 128; c0 += 32) {
+      float v[32];
+      tc::tmem_ld32(tmem + ((uint32_t)(32 * (warp & 3)) << 16) + (uint32_t)c0, v);
+#pragma unroll
+      for (int q = 0; q < 4; q++) {
+        __align__(16) __nv_bfloat16 pk[8];
+#pragma unroll
+        for (int j = 0; j < 8; j++) pk[j] = __float2bfloat16(gelu(v[q * 8 + j] + bias[c0 + q * 8 + j]));
+        *reinterpret_cast<uint4*>(act + tc::kmajor_off(rl, c0 + q * 8, MT)) = *reinterpret_cast<const uint4*>(pk);
+      }
+    }
+    tc::fence_proxy_async();  // generic shared-memory writes -> operands of the next MMAs
+    tc::fence_before();
+    __syncthreads();
+  };
+  constexpr uint32_t id256 = tc::idesc_bf16(MT, 256), id16 = tc::idesc_bf16(MT, 16);
+  bool ok = true;
+
+  // layer 0: 16 -> 256, one K = 16 MMA
+  stage_rows<MT, 16>(xin, a.x, 16, m0, a.M, 0);
+  stage_rows<256, 16>(wb0, a.w[0], 16, 0, 256, 0);
+  tc::fence_proxy_async();
+  __syncthreads();
+  if (tid == 0) {
+    tc::fence_after();
+    tc::mma_bf16(tmem, tc::smem_desc(tc::smem_u32(xin), MT * 16, 128), tc::smem_desc(tc::smem_u32(wb0), 256 * 16, 128),
+                 id256, 0u);
+    tc::mma_commit(tc::smem_u32(&bar[0]));
+  }
+  ok = wait_bar(0);
+  if (ok) hidden_epilogue(a.b[0]);
+
+  // layers 1, 2: 256 -> 256 in K-chunks of 32 through the two buffers
+  for (int l = 1; l <= 2 && ok; l++) {
+    for (int kc = 0; kc < NK && ok; kc++) {
+      const int buf = kc & 1;
+      uint8_t* wb = buf ? wb1 : wb0;
+      if (kc >= 2) {  // the MMAs of chunk kc - 2 have read this buffer
+        ok = wait_bar(buf);
+        if (!ok) break;
+      }
+      stage_rows<256, KC>(wb, a.w[l], 256, 0, 256, kc * KC);
+      tc::fence_proxy_async();
+      __syncthreads();
+      if (tid == 0) {
+        tc::fence_after();
+#pragma unroll
+        for (int s = 0; s < KC / 16; s++) {
+          const uint64_t ad = tc::smem_desc(tc::smem_u32(act) + (uint32_t)((kc * KC / 8 + 2 * s) * (MT * 16)), MT * 16, 128);
+          const uint64_t bd = tc::smem_desc(tc::smem_u32(wb) + (uint32_t)(2 * s * (256 * 16)), 256 * 16, 128);
+          tc::mma_bf16(tmem, ad, bd, id256, (kc > 0 || s > 0) ? 1u : 0u);
+        }
+        tc::mma_commit(tc::smem_u32(&bar[buf]));
+      }
+    }
+    if (ok) ok = wait_bar(0);  // chunks NK - 2 and NK - 1: every MMA of the layer is done
+    if (ok) ok = wait_bar(1);
+    if (ok) hidden_epilogue(a.b[l]);
+  }
+
+  // layer 3: 256 -> 16, W3 staged whole, sixteen K = 16 MMAs of N = 16
+  if (ok) {
+    stage_rows<16, 256>(wb0, a.w[3], 256, 0, 16, 0);
+    tc::fence_proxy_async();
+    __syncthreads();
+    if (tid == 0) {
+      tc::fence_after();
+#pragma unroll
+      for (int s = 0; s < 16; s++) {
+        const uint64_t ad = tc::smem_desc(tc::smem_u32(act) + (uint32_t)(2 * s * (MT * 16)), MT * 16, 128);
+        const uint64_t bd = tc::smem_desc(tc::smem_u32(wb0) + (uint32_t)(2 * s * (16 * 16)), 16 * 16, 128);
+        tc::mma_bf16(tmem, ad, bd, id16, s > 0 ? 1u : 0u);
+      }
+      tc::mma_commit(tc::smem_u32(&bar[0]));
+    }
+    ok = wait_bar(0);
+  }
+  if (ok) {
+    if (warp < 4) {
+      const int row = m0 + 32 * warp + lane;
+      float v[32];
+      tc::tmem_ld32(tmem + ((uint32_t)(32 * warp) << 16), v);
+      if (row < a.M) {
+        float4* o = reinterpret_cast<float4*>(a.out + (long long)row * 16);
+#pragma unroll
+        for (int q = 0; q < 4; q++)
+          o[q] = make_float4(v[4 * q] + a.b[3][4 * q], v[4 * q + 1] + a.b[3][4 * q + 1], v[4 * q + 2] + a.b[3][4 * q + 2],
+                             v[4 * q + 3] + a.b[3][4 * q + 3]);
+      }
+    }
+  } else if (tid == 0) {
+    atomicExch(a.err, 1);
+    // let MMAs still in flight finish (bounded) before the TMEM is released
+    tc::mbar_wait(&bar[0], (uint32_t)(nd[0] & 1), WAIT_LIMIT);
+    tc::mbar_wait(&bar[1], (uint32_t)(nd[1] & 1), WAIT_LIMIT);
+  }
+  tc::fence_before();
+  __syncthreads();
+  if (warp == 0) tc::tmem_dealloc(tmem, 256);
+}
+
+int launch_mlp_fused(const MlpArgs& a, cudaStream_t st) {
+  if (a.M <= 0) return 0;
+  static bool attr = false;
+  if (!attr) {
+    if (cudaFuncSetAttribute(k_mlp_fused, cudaFuncAttributeMaxDynamicSharedMemorySize, fused::BYTES) != cudaSuccess)
+      return -2;
+    attr = true;
+  }
+  k_mlp_fused<<<(a.M + fused::MT - 1) / fused::MT, fused::THR, fused::BYTES, st>>>(a);
+  return cudaGetLastError() == cudaSuccess ? 0 : -2;
+}
+
 }  // namespace mlp
 }  // namespace ocfd
 

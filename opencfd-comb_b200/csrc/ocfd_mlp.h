@@ -27,5 +27,18 @@ struct GemmArgs {
 // launches k_gemm_bf16 on stream st; 0 or -2 (CUDA error)
 int launch_gemm(const GemmArgs& g, cudaStream_t st);
 
+// the whole inference pass of the surrogate's network 16 -> 256 -> 256 -> 256 -> 16 (GELU after
+// the three hidden layers) in one kernel: W0 (256 x 16), W1, W2 (256 x 256), W3 (16 x 256) BF16
+// row-major (row = output neuron), biases FP32, x (M x 16) BF16, out (M x 16) FP32
+struct MlpArgs {
+  const __nv_bfloat16* x;
+  const __nv_bfloat16* w[4];
+  const float* b[4];
+  float* out;
+  int M;
+  int* err;  // set to 1 when an mbarrier wait runs out
+};
+int launch_mlp_fused(const MlpArgs& a, cudaStream_t st);
+
 }  // namespace mlp
 }  // namespace ocfd

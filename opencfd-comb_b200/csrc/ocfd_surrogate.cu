@@ -286,10 +286,27 @@ struct Gemm {
   }
 };
 
+bool g_fused = true;  // inference through the fused four-layer kernel (ocfd_gpu_surrogate_fused)
+
 // forward pass of rows rows of x (BF16, PAD wide): hidden activations into h[0..2] (BF16, HID wide,
-// and their pre-activations into pre[0..2] when given), outputs into out (FP32, PAD wide)
+// and their pre-activations into pre[0..2] when given), outputs into out (FP32, PAD wide). Without
+// pre-activations (inference) the four layers run as one fused kernel; the hidden activations then
+// stay on chip and h is not written.
 void forward(Gemm& gemm, int rows, const __nv_bfloat16* x, __nv_bfloat16* const* h, float* const* pre, float* out,
              cudaStream_t st) {
+  if (!pre && g_fused) {
+    mlp::MlpArgs m{};
+    m.x = x;
+    for (int l = 0; l < NLAYER; l++) {
+      m.w[l] = S.wb[l];
+      m.b[l] = S.b[l];
+    }
+    m.out = out;
+    m.M = rows;
+    m.err = S.d_err;
+    if (gemm.rc == 0) gemm.rc = mlp::launch_mlp_fused(m, st);
+    return;
+  }
   const __nv_bfloat16* in = x;
   long long ld = PAD;
   for (int l = 0; l < 3; l++) {
@@ -718,6 +735,12 @@ int run_surrogate(int n, int mode, double* di, double* e, const double* dt, cons
 }  // namespace
 
 extern "C" {
+int ocfd_gpu_surrogate_fused(int on) {
+  const int was = g_fused ? 1 : 0;
+  if (on >= 0) g_fused = on != 0;
+  return was;
+}
+
 int ocfd_gpu_surrogate_init(unsigned seed) {
   const int ns = current_nspec();
   if (ns < 2) return -5;

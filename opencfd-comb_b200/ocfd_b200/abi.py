@@ -131,6 +131,7 @@ GPU_SIGNATURES = {
     "ocfd_gpu_diag_end": (I, [PD, PD]),
     "ocfd_gpu_snapshot": (I, [I, D]),
     "ocfd_gpu_snapshot_wait": (I, [PI, PD, C.POINTER(PD)]),
+    "ocfd_gpu_surrogate_fused": (I, [I]),
     "ocfd_gpu_filtering": (I, [I, I, PD, PI]),
     "ocfd_gpu_keep_viscosity": (I, [I]),
     "ocfd_gpu_ana_box": (I, [D, PD]),

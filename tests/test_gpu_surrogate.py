@@ -74,6 +74,28 @@ def test_gated_surrogate_against_fp64(trained):
     assert r["ungated_T_err_max_K"] < 0.5 * r["no_reaction_T_err_max_K"], r
 
 
+def test_fused_network_equals_layer_gemms(trained):
+    """The fused four-layer kernel and the per-layer GEMMs issue the same MMAs and epilogue
+    arithmetic: identical network outputs, so identical gated results."""
+    sg, _ = trained
+    t = sg.torch
+    n = 3 * 128 + 37  # ragged last tile
+    di, E, dt, nsub = sg.reactors(n, seed=77)
+    outs = []
+    for fused in (0, 1):
+        was = sg.L.ocfd_gpu_surrogate_fused(fused)
+        d_di, d_e, d_dt = [t.from_numpy(np.ascontiguousarray(a)).to("cuda") for a in (di, E, dt)]
+        o_di, o_e = t.empty_like(d_di), t.empty_like(d_e)
+        Tp, Te = t.empty_like(d_e), t.empty_like(d_e)
+        t.cuda.synchronize()
+        assert sg.L.ocfd_gpu_surrogate_predict(n, d_di.data_ptr(), d_e.data_ptr(), d_dt.data_ptr(), o_di.data_ptr(),
+                                               o_e.data_ptr(), Tp.data_ptr(), Te.data_ptr()) == 0
+        outs.append([x.cpu().numpy() for x in (o_di, o_e, Tp, Te)])
+        sg.L.ocfd_gpu_surrogate_fused(was)
+    for a, b in zip(*outs):
+        assert np.array_equal(a, b)
+
+
 def test_blob_roundtrip(trained):
     sg, _ = trained
     b = sg.blob()
