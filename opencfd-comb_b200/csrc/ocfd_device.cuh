@@ -45,6 +45,8 @@ struct DevConst {
   // Wilke pair constants of comput_vis_coeff, sqrt(Mi(j)/Mi(k)) and sqrt(8*(1+Mi(k)/Mi(j))):
   // cell-independent, evaluated on the host with the same correctly rounded operations
   double wk_a[OCFD_MAX_SPEC][OCFD_MAX_SPEC], wk_b[OCFD_MAX_SPEC][OCFD_MAX_SPEC];
+  // the same pair constants for the multi-species transport kernel: sqrt(wk_a) and 1 / wk_b
+  double wk_c[OCFD_MAX_SPEC][OCFD_MAX_SPEC], wk_binv[OCFD_MAX_SPEC][OCFD_MAX_SPEC];
   // kinetics
   int nreac, rereac, timeadv;
   int af_type[OCFD_MAX_REAC], tr_reac[OCFD_MAX_REAC];

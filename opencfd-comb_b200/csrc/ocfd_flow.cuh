@@ -868,12 +868,16 @@ static __global__ void k_scal_rk(int krk, double dt, const double* dus, const do
 // One thread per (cell, species): a block is 32 consecutive cells (threadIdx.x) x NS species
 // (threadIdx.y). The per-species exponentials, the Wilke rows and the NS (NS-1) / 2 distinct
 // binary-diffusion pairs are spread over a cell's NS threads; every sum is taken from shared
-// memory in the reference's order, so the results equal the one-thread-per-cell evaluation.
+// memory in the reference's order. The divisions and square roots of the pair terms are
+// restated as products (square roots of the viscosities per species, reciprocal pair constants
+// from the host, 1 / D2 as exp(-poly) * 1e4): the same quantities up to last-place rounding,
+// which the transcendental functions of this path already make inexact against the oracle.
 template <int NS>
 __global__ void __launch_bounds__(32 * NS) k_transport(const double* d, const double* T, const double* p,
                                                        const double* di, double* amu, double* amk, double* amd) {
   constexpr int NP = NS * (NS - 1) / 2;
   __shared__ double sX[NS][32], sD0[NS][32], sMu[NS][32], sK[NS][32], sW[NS][32], sD2[NP > 0 ? NP : 1][32];
+  __shared__ double sSq[NS][32], sRs[NS][32];  // sqrt(mu_k), 1 / sqrt(mu_k)
   const int ks = threadIdx.y, lane = threadIdx.x;
   int i, j, k;
   const bool ok = cell_of((long long)blockIdx.x * 32 + lane, i, j, k);
@@ -896,8 +900,13 @@ __global__ void __launch_bounds__(32 * NS) k_transport(const double* d, const do
 #pragma unroll
   for (int m = 0; m < NS; m++) Xi[m] = sW[m][lane];
   const double L = log(Tq);
-  if (cC.flag_vis != 0)
-    sMu[ks][lane] = exp(cC.mu_an[ks][0] + cC.mu_an[ks][1] * L + cC.mu_an[ks][2] * q2(L) + cC.mu_an[ks][3] * q3(L)) * 0.1;
+  if (cC.flag_vis != 0) {
+    const double muk = exp(cC.mu_an[ks][0] + cC.mu_an[ks][1] * L + cC.mu_an[ks][2] * q2(L) + cC.mu_an[ks][3] * q3(L)) * 0.1;
+    sMu[ks][lane] = muk;
+    const double sq = sqrt(muk);
+    sSq[ks][lane] = sq;
+    sRs[ks][lane] = 1.0 / sq;
+  }
   if (cC.flag_cond != 0)
     sK[ks][lane] = exp(cC.k_an[ks][0] + cC.k_an[ks][1] * L + cC.k_an[ks][2] * q2(L) + cC.k_an[ks][3] * q3(L)) * 1.0e-5;
   if (cC.flag_diff != 0) {
@@ -905,8 +914,9 @@ __global__ void __launch_bounds__(32 * NS) k_transport(const double* d, const do
       int a = 0, r = pi;
       while (r >= NS - 1 - a) { r -= NS - 1 - a; a++; }
       const int b = a + 1 + r;
+      // 1 / D2 of the pair: exp(-poly) * 1e4 (the reciprocal of exp(poly) * 1e-4 up to rounding)
       sD2[pi][lane] =
-          exp(cC.d_an[a][b][0] + cC.d_an[a][b][1] * L + cC.d_an[a][b][2] * q2(L) + cC.d_an[a][b][3] * q3(L)) * 1.0e-4;
+          exp(-(cC.d_an[a][b][0] + cC.d_an[a][b][1] * L + cC.d_an[a][b][2] * q2(L) + cC.d_an[a][b][3] * q3(L))) * 1.0e4;
     }
   }
   __syncthreads();
@@ -916,12 +926,15 @@ __global__ void __launch_bounds__(32 * NS) k_transport(const double* d, const do
     const double TA = 288.15, TC = 110.4;
     mu = cC.amu0 * sqrt(q3(Tq / TA)) * (TA + TC) / (TC + Tq);
   } else {
-    const double muk = sMu[ks][lane];
+    // Wilke's phi_kj = (1 + sqrt(mu_k / mu_j) (M_j / M_k)^(1/4))^2 / sqrt(8 (1 + M_k / M_j)), with
+    // the square roots of the viscosities taken once per species and the pair constants'
+    // reciprocals precomputed (the same quantities up to rounding; TRANSPORT_modules.f90:259-300)
+    const double muk = sMu[ks][lane], sqk = sSq[ks][lane];
     double pk0 = 0.0;
 #pragma unroll
     for (int jj = 0; jj < NS; jj++) {
-      double s1 = 1.0 + sqrt(muk / sMu[jj][lane] * cC.wk_a[ks][jj]);
-      double pkj = q2(s1) / cC.wk_b[ks][jj];
+      double s1 = 1.0 + sqk * sRs[jj][lane] * cC.wk_c[ks][jj];
+      double pkj = q2(s1) * cC.wk_binv[ks][jj];
       pk0 = pk0 + Xi[jj] * pkj;
     }
     sW[ks][lane] = Xi[ks] * muk / pk0;
@@ -968,7 +981,7 @@ __global__ void __launch_bounds__(32 * NS) k_transport(const double* d, const do
       if (jj == ks) continue;
       const int a = ks < jj ? ks : jj, b = ks < jj ? jj : ks;
       const int pi = a * NS - a * (a + 1) / 2 + (b - a - 1);
-      ds = ds + Xi[jj] / sD2[pi][lane];
+      ds = ds + Xi[jj] * sD2[pi][lane];  // sD2 holds 1 / D2
     }
     ad = (1.0 - Xi[ks]) / (ds + 1.0e-20) * 1.013e5 / p[q];
   }

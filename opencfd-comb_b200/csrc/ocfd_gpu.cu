@@ -963,6 +963,8 @@ void fill_trans(DevConst& c, const ocfd_transport* tr, int ns) {
     for (int j = 0; j < ns; j++) {
       c.wk_a[k][j] = std::sqrt(c.Mi[j] / c.Mi[k]);
       c.wk_b[k][j] = std::sqrt(8.0 * (1.0 + c.Mi[k] / c.Mi[j]));
+      c.wk_c[k][j] = std::sqrt(c.wk_a[k][j]);
+      c.wk_binv[k][j] = 1.0 / c.wk_b[k][j];
     }
 }
 
