@@ -219,16 +219,50 @@ int launch_gemm(const GemmArgs& g, cudaStream_t st) {
 // One CTA (8 warps) carries a 128-row tile through the four layers. Per layer the MMAs accumulate
 // into a 128 x 256 FP32 TMEM accumulator; the epilogue (bias, GELU, BF16) writes the activations
 // back to shared memory in the K-major layout, where they are the next layer's A operand, so only
-// the 16 inputs and 16 outputs of a row touch global memory. The 256 x 256 weights stream through
-// two 32-wide K-chunk buffers (chunk c + 1 is staged while the MMAs of chunk c run); all CTAs read
-// the same 272 KB of weights, which stay in L2. Each layer issues the same K = 16 MMAs in the same
-// order as the layer-by-layer GEMMs and the epilogues evaluate the same expressions.
+// the 16 inputs and 16 outputs of a row touch global memory. The weights are packed beforehand
+// (k_pack_mlp) into the exact shared-memory image of each 16-wide K chunk, so one thread brings a
+// chunk in with a single bulk copy whose completion lands on a transaction mbarrier: four chunk
+// buffers keep three chunks in flight while an MMA runs, and the next layer's first chunks are
+// fetched during the current epilogue. All CTAs read the same 272 KB of packed weights, which stay
+// in L2. Each layer issues the same K = 16 MMAs in the same order as the layer-by-layer GEMMs and
+// the epilogues evaluate the same expressions.
 namespace fused {
-constexpr int MT = 128, THR = 256, KC = 32, NK = 256 / KC;
-constexpr int ACT_BYTES = MT * 256 * 2, X_BYTES = MT * 16 * 2, WB_BYTES = 256 * KC * 2;
-constexpr int BYTES = ACT_BYTES + X_BYTES + 2 * WB_BYTES + 64;
+constexpr int MT = 128, THR = 256, KCH = 16, NKC = 256 / KCH, NBUF = 4, CHUNK = 256 * KCH * 2;
+constexpr int ACT_BYTES = MT * 256 * 2, X_BYTES = MT * 16 * 2;
+constexpr int BYTES = ACT_BYTES + X_BYTES + NBUF * CHUNK + 128;
 static_assert(2 * BYTES <= 226 * 1024, "two blocks per SM");
+static_assert(MLP_PACK_BYTES == (2 + 2 * NKC) * CHUNK, "packed weight layout");
+// byte offsets of the packed images: W0 (256 x 16), the 16 chunks of W1 and of W2 (256 x 16
+// each), W3 (16 x 256); every image is CHUNK bytes
+__host__ __device__ constexpr int pack_w0() { return 0; }
+__host__ __device__ constexpr int pack_chunk(int l, int c) { return CHUNK * (1 + (l - 1) * NKC + c); }
+__host__ __device__ constexpr int pack_w3() { return CHUNK * (1 + 2 * NKC); }
 }  // namespace fused
+
+// the weights in shared-memory image form: one thread per weight element
+__global__ void k_pack_mlp(MlpArgs a) {
+  using namespace fused;
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  uint32_t off;
+  __nv_bfloat16 v;
+  if (e < 256 * 16) {  // W0
+    const int r = e / 16, k = e % 16;
+    v = a.w[0][e];
+    off = pack_w0() + tc::kmajor_off(r, k, 256);
+  } else if (e < 256 * 16 + 2 * 256 * 256) {  // W1, W2
+    const int f0 = e - 256 * 16, l = 1 + f0 / (256 * 256), f = f0 % (256 * 256);
+    const int r = f / 256, k = f % 256;
+    v = a.w[l][f];
+    off = pack_chunk(l, k / KCH) + tc::kmajor_off(r, k % KCH, 256);
+  } else if (e < 256 * 16 + 2 * 256 * 256 + 16 * 256) {  // W3
+    const int f = e - 256 * 16 - 2 * 256 * 256, r = f / 256, k = f % 256;
+    v = a.w[3][f];
+    off = pack_w3() + tc::kmajor_off(r, k, 16);
+  } else {
+    return;
+  }
+  *reinterpret_cast<__nv_bfloat16*>(a.pack + off) = v;
+}
 
 // stage rows r0 .. r0 + R - 1, columns k0 .. k0 + KN - 1 of a row-major BF16 matrix (row stride ld)
 // into the K-major layout of an R-row tile; rows at or beyond nrows are zero. Eight consecutive
@@ -261,32 +295,40 @@ __device__ __forceinline__ void stage_rows(uint8_t* dst, const __nv_bfloat16* sr
 __global__ void __launch_bounds__(fused::THR, 2) k_mlp_fused(MlpArgs a) {
   using namespace fused;
   extern __shared__ __align__(1024) uint8_t sm[];
-  uint8_t* act = sm;                      // 128 x 256 activations, K-major
-  uint8_t* xin = sm + ACT_BYTES;          // 128 x 16 inputs
-  uint8_t* wb0 = xin + X_BYTES;           // weight chunk buffers (256 x 32, or W0 / W3 whole)
-  uint8_t* wb1 = wb0 + WB_BYTES;
-  uint64_t* bar = reinterpret_cast<uint64_t*>(wb1 + WB_BYTES);  // one mbarrier per buffer
-  uint32_t* tslot = reinterpret_cast<uint32_t*>(bar + 2);
+  uint8_t* act = sm;               // 128 x 256 activations, K-major
+  uint8_t* xin = sm + ACT_BYTES;   // 128 x 16 inputs
+  uint8_t* wbase = xin + X_BYTES;  // NBUF weight chunk buffers of CHUNK bytes
+  uint64_t* tb = reinterpret_cast<uint64_t*>(wbase + NBUF * CHUNK);  // chunk landed (bulk copy)
+  uint64_t* mb = tb + NBUF;                                          // MMAs reading the chunk done
+  uint32_t* tslot = reinterpret_cast<uint32_t*>(mb + NBUF);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int m0 = blockIdx.x * MT;
 
   if (warp == 0) tc::tmem_alloc(tslot, 256);
   if (tid == 0) {
-    tc::mbar_init(&bar[0], 1);
-    tc::mbar_init(&bar[1], 1);
+    for (int b = 0; b < NBUF; b++) {
+      tc::mbar_init(&tb[b], 1);
+      tc::mbar_init(&mb[b], 1);
+    }
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   tc::fence_before();
   __syncthreads();
   tc::fence_after();
   const uint32_t tmem = *tslot;
-  int nd[2] = {0, 0};  // completions of each mbarrier waited for so far
-  // thread 0 waits for the next completion of barrier b; the block learns the outcome
-  auto wait_bar = [&](int b) -> bool {
-    bool o = true;
-    if (tid == 0) o = tc::mbar_wait(&bar[b], (uint32_t)(nd[b] & 1), WAIT_LIMIT);
-    nd[b]++;
-    const bool all = __syncthreads_and(o ? 1 : 0) != 0;
+  // thread 0 drives the pipeline: completions of each barrier waited for so far
+  int ntb[NBUF] = {0, 0, 0, 0}, nmb[NBUF] = {0, 0, 0, 0};
+  bool ok = true;
+  auto buf = [&](int c) { return wbase + (c % NBUF) * CHUNK; };
+  auto fetch = [&](int c, int off) {  // chunk image at pack + off into buffer c % NBUF
+    tc::mbar_arrive_expect_tx(&tb[c % NBUF], CHUNK);
+    tc::bulk_g2s(buf(c), a.pack + off, CHUNK, &tb[c % NBUF]);
+  };
+  auto wait_t = [&](int b) { return tc::mbar_wait(&tb[b], (uint32_t)(ntb[b]++ & 1), WAIT_LIMIT); };
+  auto wait_m = [&](int b) { return tc::mbar_wait(&mb[b], (uint32_t)(nmb[b]++ & 1), WAIT_LIMIT); };
+  // the block learns thread 0's outcome
+  auto agree = [&]() {
+    const bool all = __syncthreads_and(ok ? 1 : 0) != 0;
     tc::fence_after();
     return all;
   };
@@ -311,68 +353,77 @@ __global__ void __launch_bounds__(fused::THR, 2) k_mlp_fused(MlpArgs a) {
     __syncthreads();
   };
   constexpr uint32_t id256 = tc::idesc_bf16(MT, 256), id16 = tc::idesc_bf16(MT, 16);
-  bool ok = true;
 
-  // layer 0: 16 -> 256, one K = 16 MMA
+  // layer 0: 16 -> 256, one K = 16 MMA; W0 arrives by bulk copy while the inputs are staged
+  if (tid == 0) fetch(0, pack_w0());
   stage_rows<MT, 16>(xin, a.x, 16, m0, a.M, 0);
-  stage_rows<256, 16>(wb0, a.w[0], 16, 0, 256, 0);
   tc::fence_proxy_async();
   __syncthreads();
   if (tid == 0) {
-    tc::fence_after();
-    tc::mma_bf16(tmem, tc::smem_desc(tc::smem_u32(xin), MT * 16, 128), tc::smem_desc(tc::smem_u32(wb0), 256 * 16, 128),
-                 id256, 0u);
-    tc::mma_commit(tc::smem_u32(&bar[0]));
+    ok = wait_t(0);
+    if (ok) {
+      tc::fence_after();
+      tc::mma_bf16(tmem, tc::smem_desc(tc::smem_u32(xin), MT * 16, 128), tc::smem_desc(tc::smem_u32(buf(0)), 256 * 16, 128),
+                   id256, 0u);
+      tc::mma_commit(tc::smem_u32(&mb[0]));
+      ok = wait_m(0);
+    }
+    if (ok)  // layer 1's first chunks travel during the epilogue
+      for (int c = 0; c < NBUF - 1; c++) fetch(c, pack_chunk(1, c));
   }
-  ok = wait_bar(0);
-  if (ok) hidden_epilogue(a.b[0]);
+  bool all = agree();
+  if (all) hidden_epilogue(a.b[0]);
 
-  // layers 1, 2: 256 -> 256 in K-chunks of 32 through the two buffers
-  for (int l = 1; l <= 2 && ok; l++) {
-    for (int kc = 0; kc < NK && ok; kc++) {
-      const int buf = kc & 1;
-      uint8_t* wb = buf ? wb1 : wb0;
-      if (kc >= 2) {  // the MMAs of chunk kc - 2 have read this buffer
-        ok = wait_bar(buf);
+  // layers 1, 2: 256 -> 256, sixteen K = 16 chunks through the NBUF buffers
+  for (int l = 1; l <= 2 && all; l++) {
+    if (tid == 0) {
+      for (int c = 0; c < NKC && ok; c++) {
+        const int b = c % NBUF;
+        ok = wait_t(b);  // chunk c landed
         if (!ok) break;
+        tc::fence_after();
+        const uint64_t ad = tc::smem_desc(tc::smem_u32(act) + (uint32_t)(2 * c * (MT * 16)), MT * 16, 128);
+        const uint64_t bd = tc::smem_desc(tc::smem_u32(buf(c)), 256 * 16, 128);
+        tc::mma_bf16(tmem, ad, bd, id256, c > 0 ? 1u : 0u);
+        tc::mma_commit(tc::smem_u32(&mb[b]));
+        const int nx = c + NBUF - 1;  // refill the buffer of chunk c - 1 once its MMA is done
+        if (nx < NKC) {
+          if (c >= 1) ok = wait_m((c - 1) % NBUF);
+          if (ok) fetch(nx, pack_chunk(l, nx));
+        }
       }
-      stage_rows<256, KC>(wb, a.w[l], 256, 0, 256, kc * KC);
-      tc::fence_proxy_async();
-      __syncthreads();
-      if (tid == 0) {
+      // the MMAs whose completion the loop did not wait for, in issue order
+      for (int c = NKC - NBUF; c < NKC && ok; c++) ok = wait_m(c % NBUF);
+      if (ok) {  // the next layer's first chunks (or W3) travel during the epilogue
+        if (l == 1)
+          for (int c = 0; c < NBUF - 1; c++) fetch(c, pack_chunk(2, c));
+        else
+          fetch(0, pack_w3());
+      }
+    }
+    all = agree();
+    if (all) hidden_epilogue(a.b[l]);
+  }
+
+  // layer 3: 256 -> 16, sixteen K = 16 MMAs of N = 16 on the whole W3 image
+  if (all) {
+    if (tid == 0) {
+      ok = wait_t(0);
+      if (ok) {
         tc::fence_after();
 #pragma unroll
-        for (int s = 0; s < KC / 16; s++) {
-          const uint64_t ad = tc::smem_desc(tc::smem_u32(act) + (uint32_t)((kc * KC / 8 + 2 * s) * (MT * 16)), MT * 16, 128);
-          const uint64_t bd = tc::smem_desc(tc::smem_u32(wb) + (uint32_t)(2 * s * (256 * 16)), 256 * 16, 128);
-          tc::mma_bf16(tmem, ad, bd, id256, (kc > 0 || s > 0) ? 1u : 0u);
+        for (int s = 0; s < 16; s++) {
+          const uint64_t ad = tc::smem_desc(tc::smem_u32(act) + (uint32_t)(2 * s * (MT * 16)), MT * 16, 128);
+          const uint64_t bd = tc::smem_desc(tc::smem_u32(buf(0)) + (uint32_t)(2 * s * (16 * 16)), 16 * 16, 128);
+          tc::mma_bf16(tmem, ad, bd, id16, s > 0 ? 1u : 0u);
         }
-        tc::mma_commit(tc::smem_u32(&bar[buf]));
+        tc::mma_commit(tc::smem_u32(&mb[0]));
+        ok = wait_m(0);
       }
     }
-    if (ok) ok = wait_bar(0);  // chunks NK - 2 and NK - 1: every MMA of the layer is done
-    if (ok) ok = wait_bar(1);
-    if (ok) hidden_epilogue(a.b[l]);
+    all = agree();
   }
-
-  // layer 3: 256 -> 16, W3 staged whole, sixteen K = 16 MMAs of N = 16
-  if (ok) {
-    stage_rows<16, 256>(wb0, a.w[3], 256, 0, 16, 0);
-    tc::fence_proxy_async();
-    __syncthreads();
-    if (tid == 0) {
-      tc::fence_after();
-#pragma unroll
-      for (int s = 0; s < 16; s++) {
-        const uint64_t ad = tc::smem_desc(tc::smem_u32(act) + (uint32_t)(2 * s * (MT * 16)), MT * 16, 128);
-        const uint64_t bd = tc::smem_desc(tc::smem_u32(wb0) + (uint32_t)(2 * s * (16 * 16)), 16 * 16, 128);
-        tc::mma_bf16(tmem, ad, bd, id16, s > 0 ? 1u : 0u);
-      }
-      tc::mma_commit(tc::smem_u32(&bar[0]));
-    }
-    ok = wait_bar(0);
-  }
-  if (ok) {
+  if (all) {
     if (warp < 4) {
       const int row = m0 + 32 * warp + lane;
       float v[32];
@@ -387,9 +438,11 @@ __global__ void __launch_bounds__(fused::THR, 2) k_mlp_fused(MlpArgs a) {
     }
   } else if (tid == 0) {
     atomicExch(a.err, 1);
-    // let MMAs still in flight finish (bounded) before the TMEM is released
-    tc::mbar_wait(&bar[0], (uint32_t)(nd[0] & 1), WAIT_LIMIT);
-    tc::mbar_wait(&bar[1], (uint32_t)(nd[1] & 1), WAIT_LIMIT);
+    // let copies and MMAs still in flight finish (bounded) before the TMEM and shared memory go
+    for (int b = 0; b < NBUF; b++) {
+      tc::mbar_wait(&tb[b], (uint32_t)(ntb[b] & 1), WAIT_LIMIT);
+      tc::mbar_wait(&mb[b], (uint32_t)(nmb[b] & 1), WAIT_LIMIT);
+    }
   }
   tc::fence_before();
   __syncthreads();
@@ -398,12 +451,15 @@ __global__ void __launch_bounds__(fused::THR, 2) k_mlp_fused(MlpArgs a) {
 
 int launch_mlp_fused(const MlpArgs& a, cudaStream_t st) {
   if (a.M <= 0) return 0;
+  if (!a.pack || (reinterpret_cast<uintptr_t>(a.pack) & 15) != 0) return -1;
   static bool attr = false;
   if (!attr) {
     if (cudaFuncSetAttribute(k_mlp_fused, cudaFuncAttributeMaxDynamicSharedMemorySize, fused::BYTES) != cudaSuccess)
       return -2;
     attr = true;
   }
+  constexpr int NW = 256 * 16 + 2 * 256 * 256 + 16 * 256;
+  k_pack_mlp<<<(NW + 255) / 256, 256, 0, st>>>(a);
   k_mlp_fused<<<(a.M + fused::MT - 1) / fused::MT, fused::THR, fused::BYTES, st>>>(a);
   return cudaGetLastError() == cudaSuccess ? 0 : -2;
 }

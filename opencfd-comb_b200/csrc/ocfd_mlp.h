@@ -36,8 +36,11 @@ struct MlpArgs {
   const float* b[4];
   float* out;
   int M;
-  int* err;  // set to 1 when an mbarrier wait runs out
+  int* err;            // set to 1 when an mbarrier wait runs out
+  unsigned char* pack; // MLP_PACK_BYTES of device scratch for the weights in shared-memory image form
 };
+constexpr int MLP_PACK_BYTES = (2 + 2 * 16) * 8192;  // W0, 16 + 16 chunks of W1 / W2, W3
+// packs the weights (launch on the same stream before the kernel), then runs the kernel
 int launch_mlp_fused(const MlpArgs& a, cudaStream_t st);
 
 }  // namespace mlp

@@ -50,6 +50,7 @@ struct State {
   Norm* d_norm = nullptr;
   double* d_proj = nullptr;  // ns x ns element projection
   int* d_err = nullptr;
+  unsigned char* d_wpack = nullptr;  // weights packed for the fused inference kernel
   long long adam_t = 0;
 };
 State S;
@@ -304,6 +305,7 @@ void forward(Gemm& gemm, int rows, const __nv_bfloat16* x, __nv_bfloat16* const*
     m.out = out;
     m.M = rows;
     m.err = S.d_err;
+    m.pack = S.d_wpack;
     if (gemm.rc == 0) gemm.rc = mlp::launch_mlp_fused(m, st);
     return;
   }
@@ -332,7 +334,7 @@ int ensure_params(int ns, unsigned seed) {
         return -2;
     }
     if (cudaMalloc(&S.d_norm, sizeof(Norm)) || cudaMalloc(&S.d_proj, sizeof(double) * PAD * PAD) ||
-        cudaMalloc(&S.d_err, sizeof(int)))
+        cudaMalloc(&S.d_err, sizeof(int)) || cudaMalloc(&S.d_wpack, mlp::MLP_PACK_BYTES))
       return -2;
   }
   // He initialisation over the used fan-in; padded rows / columns start (and stay) at zero
