@@ -794,8 +794,14 @@ static __global__ void k_ci(const double* di, const double* d, double* ci, long 
 // (threadIdx.y), so every species' loads are coalesced and the NS stencil evaluations of a cell
 // run in parallel. The enthalpy-flux sums Qp go through shared memory and are added by the
 // species-0 thread in species order.
+// resident blocks per SM given to the register allocator of the (cell, species) kernels: 3 (at
+// most 75 registers at 9 species) instead of the 90-94 the compiler picks alone, which allowed
+// only two 288-thread blocks; measured on the 9-species jet: species work 424 -> 294 ms per step
+#ifndef OCFD_SPECIES_MINB
+#define OCFD_SPECIES_MINB 3
+#endif
 template <int NS, bool SEP>
-__global__ void __launch_bounds__(32 * NS) k_scal_ev(const double* ci, const double* d, const double* T,
+__global__ void __launch_bounds__(32 * NS, OCFD_SPECIES_MINB) k_scal_ev(const double* ci, const double* d, const double* T,
                                                      const double* amd, double* qpx, double* qpy, double* qpz,
                                                      double* e1, double* e2, double* e3, Geo g) {
   __shared__ double sq[3][NS][32];
@@ -893,7 +899,7 @@ static __global__ void k_scal_rk(int krk, double dt, const double* dus, const do
 // from the host, 1 / D2 as exp(-poly) * 1e4): the same quantities up to last-place rounding,
 // which the transcendental functions of this path already make inexact against the oracle.
 template <int NS>
-__global__ void __launch_bounds__(32 * NS) k_transport(const double* d, const double* T, const double* p,
+__global__ void __launch_bounds__(32 * NS, OCFD_SPECIES_MINB) k_transport(const double* d, const double* T, const double* p,
                                                        const double* di, double* amu, double* amk, double* amd) {
   constexpr int NP = NS * (NS - 1) / 2;
   __shared__ double sX[NS][32], sD0[NS][32], sMu[NS][32], sK[NS][32], sW[NS][32], sD2[NP > 0 ? NP : 1][32];
