@@ -759,10 +759,16 @@ __global__ void __launch_bounds__(VE_THREADS, 2) k_visc_div(DivArgs a) {
   }
 }
 
+// resident-block target of the per-cell k_visc_div: it waits on its stencil loads, so a fifth
+// block per SM (48 registers, about 20 bytes spilled to L1) measured 4 % faster than four (55
+// registers); six (40 registers, 50 bytes spilled) gained nothing
+#ifndef OCFD_VDIV_MINB
+#define OCFD_VDIV_MINB 5
+#endif
 // per-cell form of k_visc_div (the autotuner's k chunk 0): one thread per cell, every stencil
 // value read through the read-only cache; the same expressions as the marching form
 template <bool SEP, int HZ>
-__global__ void __launch_bounds__(256) k_visc_div_pc(DivArgs a) {
+__global__ void __launch_bounds__(256, OCFD_VDIV_MINB) k_visc_div_pc(DivArgs a) {
   constexpr int CD = HZ == 3 ? 6 : 8;
   int i, j, k;
   if (!cell_of((long long)blockIdx.x * blockDim.x + threadIdx.x, i, j, k)) return;
