@@ -916,8 +916,10 @@ static __global__ void k_scal_rk(int krk, double dt, const double* dus, const do
 // restated as products (square roots of the viscosities per species, reciprocal pair constants
 // from the host, 1 / D2 as exp(-poly) * 1e4): the same quantities up to last-place rounding,
 // which the transcendental functions of this path already make inexact against the oracle.
+// k_transport runs one block more than k_scal_ev: at 4 blocks of 9 species it needs 56 registers
+// and spills only 32 bytes (k_scal_ev would spill 120-280), measured 504 -> 495.5 ms per jet step
 #ifndef OCFD_TRANSPORT_MINB
-#define OCFD_TRANSPORT_MINB OCFD_SPECIES_MINB
+#define OCFD_TRANSPORT_MINB 4
 #endif
 template <int NS>
 __global__ void __launch_bounds__(32 * NS, OCFD_TRANSPORT_MINB) k_transport(const double* d, const double* T, const double* p,
