@@ -808,7 +808,8 @@ static __global__ void k_ci(const double* di, const double* d, double* ci, long 
 // species-0 thread in species order.
 // resident blocks per SM given to the register allocator of the (cell, species) kernels: 3 (at
 // most 75 registers at 9 species) instead of the 90-94 the compiler picks alone, which allowed
-// only two 288-thread blocks; measured on the 9-species jet: species work 424 -> 294 ms per step
+// only two 288-thread blocks; measured on the 9-species jet: species work 424 -> 294 ms per step.
+// k_scal_ev at 4 (56 registers, 120-280 bytes spilled) made the jet step 2 % slower
 #ifndef OCFD_SPECIES_MINB
 #define OCFD_SPECIES_MINB 3
 #endif
