@@ -1,21 +1,28 @@
 """Throughput of the OpenCFD-Comb hot path on B200: Mcell-steps/s of whole reference time steps
-(two RK3 flow half-steps, chemistry between them when the workload reacts).
+(two RK3 flow half-steps with the finite-rate chemistry between them).
 
-  python bench.py [--gpus N] [--steps K] [--warmup W] [--workload flatplate|isotropic]
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--workload jet|flatplate|isotropic|reactors|surrogate]
   python bench.py --impl reference ...      (the reference algorithm on the host cores)
 
-Workload (default): the Mach 2.25 flat-plate boundary layer, 1024x160x128 cells, HYBRID
-UD7L/WENO7/WENO5 with the pressure sensor, CD6 viscous terms, Steger-Warming splitting,
-boundary-layer boundary conditions with the Rai blowing/suction strip, seeded synthetic state.
+Workload (default): the 3-D reacting H2 jet into hot air coflow, 384x256x256 cells, 9 species and
+19 reactions, WENO5 Steger-Warming inviscid flux, CD6 viscous terms, Wilke transport, FP64
+implicit-Euler chemistry, BC_JET inflow with seeded 2 % velocity noise. The same process runs
+the jet twice from the same start: once with the plain FP64 chemistry integrator and once with
+the gated BF16 chemistry surrogate (trained first, on the GPU, on cells of an FP64 run). `value` is
+the plain FP64 form; the `surrogate` object holds the surrogate form's throughput, its speed-up
+over the plain form, its fallback fraction and its temperature and species errors against the
+plain FP64 run after the configured 200 steps. The flat plate (1024x160x128, HYBRID) is
+`--workload flatplate`.
+
 Multi-GPU runs are independent replicas (one per rank, weak scaling): the single-rank solver has
 no exchange step, so no collective is invented; ranks meet only for the timing barrier and the
 max-over-ranks reduction.
 
 The device-resident number (value) times K graph-replayed steps with CUDA events on the library
-stream; the state (several GB) is far larger than the 126 MB L2, so no flush is needed. e2e times
-the same steps through the C ABI with the state uploaded from pinned host memory and the
-conserved variables downloaded every step. The roofline object names the kernel class with the
-largest share of a step, timed live with per-launch CUDA events.
+stream; the state (tens of GB) is far larger than the 126 MB L2, so no flush is needed. e2e times
+steps through the C ABI with the state uploaded from pinned host memory and the conserved
+variables and species densities downloaded every step. The roofline object names the kernel
+class with the largest share of a step, timed live with per-launch CUDA events.
 """
 import argparse
 import json
@@ -40,18 +47,21 @@ def parse():
     ap.add_argument("--steps", type=int, default=40)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="flatplate", choices=["flatplate", "isotropic", "jet", "reactors", "surrogate"],
-                    help="flatplate = the headline configuration; isotropic, jet and reactors are the other "
-                         "configurations of the metric (64^3 decaying turbulence, the 384x256x256 reacting H2 jet, "
-                         "2^20 batched 0-D reactors)")
+    ap.add_argument("--workload", default="jet", choices=["jet", "flatplate", "isotropic", "reactors", "surrogate"],
+                    help="jet = the metric's configuration (384x256x256 reacting H2 jet, plain FP64 and gated "
+                         "surrogate chemistry); flatplate, isotropic, reactors and surrogate are the other "
+                         "configurations (1024x160x128 M2.25 flat plate, 64^3 decaying turbulence, 2^20 batched "
+                         "0-D reactors, the surrogate on 2^20 held-out reactors)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--sg-train", type=int, default=1 << 21, help="surrogate workload: training reactors")
     ap.add_argument("--sg-epochs", type=int, default=20, help="surrogate workload: training epochs")
     ap.add_argument("--sg-tol", type=float, default=5.0, help="surrogate workload: gate tolerance on T (K)")
-    ap.add_argument("--surrogate", action="store_true",
-                    help="jet workload: compare FP64 chemistry with the gated surrogate (trains it first)")
+    ap.add_argument("--no-surrogate", action="store_true",
+                    help="jet workload: plain FP64 chemistry only (no surrogate training or second run)")
+    ap.add_argument("--total-steps", type=int, default=200,
+                    help="jet workload: steps of each run (plain and surrogate) after which the errors are taken")
     ap.add_argument("--character", action="store_true",
                     help="characteristic-space inviscid flux (IF_Scheme_Character = 1) instead of component-wise")
     ap.add_argument("--tiles", default="auto",
@@ -163,7 +173,8 @@ ALG_FLOPS_PER_CELL = {"flux_x": 356, "flux_y": 394, "flux_z": 402, "visc_ev": 30
 
 def main_reference(a):
     """The reference's algorithm on the host cores: the C++ restatement of the Fortran (no
-    Fortran compiler exists on this image, so the reference binary itself cannot be built)."""
+    Fortran compiler exists on this image, so the reference binary itself cannot be built). Each
+    timed step is one full time step of a bounded sample of the workload, on all host threads."""
     if int(os.environ.get("RANK", "0")) != 0:
         return 0
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
@@ -171,9 +182,8 @@ def main_reference(a):
     cores = pyoracle.lib().ocfd_cpu_set_threads(os.cpu_count() or 1)
     if a.workload in ("reactors", "surrogate"):  # the reference has only the FP64 integrator
         return reactors_reference(a, pyoracle, cores)
-    # size the per-step sample so that warmup + steps take about two minutes
-    rate = 0.0
     if a.workload == "flatplate":
+        # size the slab so that warmup + steps take about two minutes
         probe, _ = make_case(a.workload, nz=8)
         o = pyoracle.OracleSolver(probe)
         o.init_state()
@@ -181,16 +191,20 @@ def main_reference(a):
         o.step(probe.dt, 0.0)
         rate = probe.ncell / (time.perf_counter() - t0)
         o.close()
-    if a.workload == "flatplate":
         nz = int(max(8, min(128, 120.0 * rate / (1024 * 160 * (a.steps + a.warmup)))))
         c, name = make_case(a.workload, nz=nz)
-        sample = "per step: one full time step of a 1024x160x%d slab of the workload (z periodic)" % nz
+        full_name = make_case(a.workload)[1]
+        sample = "per step: one full time step of a 1024x160x%d slab of the 1024x160x128 workload (z periodic)" % nz
     elif a.workload == "jet":
         from ocfd_b200 import cases
-        c, name = cases.jet(nx=96, ny=64, nz=64), make_case("jet", nz=8)[1].replace("96x64x8", "384x256x256")
-        sample = "per step: one reacting time step of the jet on a 96x64x64 grid (same physics)"
+        c = cases.jet(nx=96, ny=64, nz=64)
+        name = "jet-96x64x64-H2air-9sp-19reac-WENO5-CD6-SW-Wilke-implicitChem"
+        full_name = "jet-384x256x256-H2air-9sp-19reac-WENO5-CD6-SW-Wilke-implicitChem"
+        sample = ("per step: one reacting time step (plain FP64 chemistry) of the jet on a 96x64x64 grid (same "
+                  "physics and inflow as the 384x256x256 workload)")
     else:
         c, name = make_case(a.workload)
+        full_name = name
         sample = "per step: one full time step of the 64^3 workload"
     reac, nsub = int(getattr(c, "if_reaction", 0) or 0), int(getattr(c, "nsub", 1) or 1)
     o = pyoracle.OracleSolver(c)
@@ -206,8 +220,8 @@ def main_reference(a):
     out = {"metric": METRIC, "value": val, "unit": UNIT, "n_gpus": a.gpus, "steps": a.steps, "warmup": a.warmup,
            "ms_per_step": el * 1e3 / a.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
            "dtype": "f64", "data": "synthetic (seeded)", "impl": "reference",
-           "config": {"workload": make_case(a.workload, nz=8)[1].replace("x8-", "x128-") if a.workload == "flatplate" else name,
-                      "sample_cells": c.ncell},
+           "config": {"workload": name, "sample_of": full_name, "sample_cells": c.ncell,
+                      "chemistry": "plain FP64 implicit Euler" if reac else "off"},
            "cpu_baseline": {"value": val, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample},
            "e2e": {"value": val, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(out))
@@ -407,107 +421,366 @@ def main_surrogate(a):
     return 0
 
 
-def main_jet_surrogate(a):
-    """C5 with the gated surrogate: the surrogate is trained on 2^21 batch reactors plus cells of a
-    jet snapshot, then the jet runs K steps with FP64 chemistry and K steps with the surrogate from
-    the same start; the line reports both throughputs and the surrogate run's temperature and
-    species errors against the FP64 run."""
+# algorithmic bytes per cell and RK stage of each kernel class on the reacting jet (N_SPEC = 9,
+# FP64; every input read once, every output written once; the grid is a tensor product, so the
+# metrics are 1-D arrays and count as 0). A class of several launches per stage counts them all:
+#  flux_x / flux_y / flux_z : read d,u,v,w,p,Et (6); write du (5), y / z also read du (5)
+#  visc_ev : read u,v,w,T,Amu,Amk,Qp(3) (9); write Ev1..Ev3 (12)                      = 21 doubles
+#  visc_div: read Ev (12); read + write du(2..5) (8)                                   = 20
+#  rk_prims: read f,fn,du (15), di (9); write f (5), d,u,v,w,T,p,Et (7), di (9)        = 45
+#  transport (k_transport): read d,T,p,di(9) (12); write Amu, Amk, AmD(9) (11)         = 23
+#  species_flux (x, y, z scalar sweeps): read di(9),u,v,w; write Dus(9); y, z read Dus = 81
+#  species_visc: k_ci read di(9),d, write ci(9) (19); k_scal_ev read ci(9),d,T,AmD(9),
+#    write Ev(27),Qp(3) (50); k_scal_div read Ev(27), read + write Dus(9) (45)         = 114
+#  species_rk (k_scal_rk): read Dus(9), din(9), di(9); write di(9)                      = 36
+#  chem (once per step, k_chem_cells): read + write di(9), Et, f5; read T, p            = 22
+JET_ALG_BYTES = {"flux_x": 88, "flux_y": 128, "flux_z": 128, "visc_ev": 168, "visc_div": 160, "rk_prims": 360,
+                 "transport": 184, "species_flux": 648, "species_visc": 912, "species_rk": 288}
+JET_CHEM_BYTES = 176
+JET_STAGES_PER_STEP = 6
+
+
+class Ranks:
+    """One process per GPU under torchrun (replicas): NCCL only for the timing barrier and the
+    max-over-ranks reduction."""
+
+    def __init__(self):
+        self.world = int(os.environ.get("WORLD_SIZE", "1"))
+        self.rank = int(os.environ.get("RANK", "0"))
+        local = int(os.environ.get("LOCAL_RANK", "0"))
+        if self.world > 1:
+            vis = os.environ.get("CUDA_VISIBLE_DEVICES")
+            devs = vis.split(",") if vis else [str(i) for i in range(64)]
+            os.environ["CUDA_VISIBLE_DEVICES"] = devs[local]
+        import torch
+        self.torch = torch
+        self.dist = None
+        if self.world > 1:
+            import datetime
+            import torch.distributed as dist
+            torch.cuda.set_device(0)
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+            self.dist = dist
+
+    def barrier(self):
+        if self.dist is not None:
+            self.dist.barrier()
+        self.torch.cuda.synchronize()
+
+    def max(self, x):
+        if self.dist is None:
+            return x
+        t = self.torch.tensor([x], dtype=self.torch.float64, device="cuda")
+        self.dist.all_reduce(t, op=self.dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def close(self):
+        if self.dist is not None:
+            self.dist.barrier()
+            self.dist.destroy_process_group()
+
+
+def merge_clocks(*cs):
+    sm = [x for c in cs for x in ([c["sm_mhz"]] if c.get("sm_mhz") else [])]
+    mx = [c["sm_max_mhz"] for c in cs if c.get("sm_max_mhz")]
+    return {"sm_mhz": min(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+            "reasons": sorted({r for c in cs for r in c.get("reasons", [])}),
+            "samples": sum(c.get("samples", 0) for c in cs)}
+
+
+def timed_run(L, dt, tt, k, reac, nsub):
+    """K graph-replayed steps between two CUDA events on the library stream; (ms, launches, clocks)."""
+    import ctypes as C
+    from ocfd_b200 import solver
+    chk = solver._chk
+    l0 = L.ocfd_gpu_launch_count()
+    with Clocks(0) as clk:
+        chk(L.ocfd_gpu_event_record(0))
+        chk(L.ocfd_gpu_run(dt, tt, k, reac, nsub))
+        chk(L.ocfd_gpu_event_record(1))
+        ms = C.c_double()
+        chk(L.ocfd_gpu_event_elapsed(0, 1, C.byref(ms)))
+    return ms.value, L.ocfd_gpu_launch_count() - l0, clk.summary()
+
+
+def e2e_steps(L, c, dt, tt, nsteps, reac, nsub, ranks):
+    """nsteps steps through the C ABI with host buffers: every step uploads the state (f, di and
+    the primitives) from pinned host memory, runs the step and downloads f and di."""
+    import ctypes as C
+    import numpy as np
+    from ocfd_b200 import abi, solver
+    chk = solver._chk
+    nx, ny, nz = c.shape
+    hs = c.halo_shape()
+    H = hs[0] * hs[1] * hs[2]
+    N = c.ncell
+    ns = c.params.n_spec
+    nbytes_f, nbytes_di, nbytes_pr = 8 * 5 * N, 8 * ns * H, 8 * 7 * H
+    bufs = []
+
+    def pinned(nb, shape):
+        p = C.c_void_p()
+        chk(L.ocfd_gpu_pinned_alloc(nb, C.byref(p)))
+        bufs.append(p)
+        return np.ctypeslib.as_array(C.cast(p, C.POINTER(C.c_double)), shape=shape)
+
+    hf = pinned(nbytes_f, (5, nz, ny, nx))
+    hdi = pinned(nbytes_di, (ns,) + hs)
+    hpr = pinned(nbytes_pr, (7,) + hs)
+    chk(L.ocfd_gpu_download_state(abi.dptr(hf), abi.dptr(hdi), abi.dptr(hpr)))
+    ranks.barrier()
+    chk(L.ocfd_gpu_event_record(2))
+    for s in range(nsteps):
+        chk(L.ocfd_gpu_upload_state(abi.dptr(hf), abi.dptr(hdi), abi.dptr(hpr)))
+        chk(L.ocfd_gpu_run(dt, tt, 1, reac, nsub))
+        tt += dt
+        chk(L.ocfd_gpu_download_state(abi.dptr(hf), abi.dptr(hdi), None))
+    chk(L.ocfd_gpu_event_record(3))
+    ms = C.c_double()
+    chk(L.ocfd_gpu_event_elapsed(2, 3, C.byref(ms)))
+    e2e_ms = ranks.max(ms.value)
+    for p in bufs:
+        L.ocfd_gpu_pinned_free(p)
+    return {"value": ranks.world * N * nsteps / (e2e_ms * 1e-3) / 1e6, "unit": UNIT,
+            "h2d_bytes_per_step": nbytes_f + nbytes_di + nbytes_pr, "d2h_bytes_per_step": nbytes_f + nbytes_di,
+            "steps": nsteps}, tt
+
+
+def cpu_sample(workload):
+    """The oracle (C++ restatement of the reference's Fortran) on all host threads: one time step
+    of a bounded sample of the workload after one warm-up step."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle
+    cores = pyoracle.lib().ocfd_cpu_set_threads(os.cpu_count() or 1)
+    if workload == "flatplate":
+        cs, _ = make_case("flatplate", nz=16)
+        sample = "one time step of a 1024x160x16 slab of the workload (z periodic), after one warm-up step"
+    elif workload == "jet":
+        from ocfd_b200 import cases
+        cs = cases.jet(nx=96, ny=64, nz=64)
+        sample = ("one reacting time step (plain FP64 chemistry) of the jet on a 96x64x64 grid (same physics and "
+                  "inflow), after one warm-up step")
+    else:
+        cs, _ = make_case("isotropic")
+        sample = "one time step of the 64^3 workload after one warm-up step"
+    o = pyoracle.OracleSolver(cs)
+    o.init_state()
+    creac, cnsub = int(getattr(cs, "if_reaction", 0) or 0), int(getattr(cs, "nsub", 1) or 1)
+    o.step(cs.dt, 0.0, creac, cnsub)
+    t0 = time.perf_counter()
+    o.step(cs.dt, cs.dt, creac, cnsub)
+    el = time.perf_counter() - t0
+    o.close()
+    return {"value": cs.ncell / el / 1e6, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample}
+
+
+def jet_roofline(prof, nsteps, ncell):
+    """Per-class device time of nsteps plain-launch steps (per-launch CUDA events) against the
+    classes' algorithmic bytes; the roofline object is the class with the largest share."""
+    hbm, hbm_kind = peaks()
+    step_ms = sum(v[0] for v in prof.values()) / nsteps
+    classes = {}
+    for k, (ms, n) in prof.items():
+        if n == 0:
+            continue
+        ms_step = ms / nsteps
+        row = {"ms_per_step": round(ms_step, 4), "launches_per_step": n / nsteps,
+               "share_of_step": round(ms_step / step_ms, 4) if step_ms > 0 else None}
+        alg = None
+        if k in JET_ALG_BYTES:
+            alg = JET_ALG_BYTES[k] * JET_STAGES_PER_STEP * ncell
+        elif k == "chem":
+            alg = JET_CHEM_BYTES * ncell
+        if alg is not None:
+            gbs = alg / (ms_step * 1e-3) / 1e9
+            row.update({"alg_bytes_per_step": alg, "achieved_gbs": round(gbs, 1), "frac": round(gbs / hbm, 4)})
+        classes[k] = row
+    dom = max((k for k in classes if "achieved_gbs" in classes[k]), key=lambda k: classes[k]["ms_per_step"])
+    d = classes[dom]
+    launches = d["launches_per_step"]
+    traffic = None
+    tfile = os.path.join(ROOT, "profiles", "traffic_per_cell_jet.json")
+    if os.path.exists(tfile):
+        with open(tfile) as fh:
+            tr = json.load(fh)
+        if dom in tr:
+            traffic = tr[dom] * ncell
+    return {"bound": "hbm", "kernel": dom, "achieved": d["achieved_gbs"], "peak": hbm, "unit": "GB/s",
+            "frac": d["frac"], "traffic": traffic, "peak_kind": hbm_kind,
+            "alg_bytes_per_launch": d["alg_bytes_per_step"] / launches,
+            "avg_launch_ms": d["ms_per_step"] / launches, "share_of_step": d["share_of_step"],
+            "note": "a class of several kernels (species_flux, species_visc) counts one stage's launches "
+                    "together: achieved = their algorithmic bytes / their summed device time",
+            "classes": classes}
+
+
+def main_jet(a):
+    """C5: the reacting jet with plain FP64 chemistry (value, e2e, roofline) and with the gated
+    surrogate (trained first on cells of an FP64 run), both for the same number of steps from the
+    same start, the surrogate's errors taken against the plain run at the end."""
+    ranks = Ranks()
     import numpy as np
     import ctypes as C
     from ocfd_b200 import cases, solver, surrogate
-    nz = a.nz or 256
-    case = cases.jet(nx=384, ny=256, nz=nz)
-    name = "jet-%dx%dx%d-H2air-9sp-19reac-WENO5-CD6-Wilke" % case.shape
-    sg = surrogate.Surrogate()
-    t0 = time.perf_counter()
-    # the jet's chemical change per step is orders of magnitude below the batch reactors', so the
-    # network is trained on jet states alone (two snapshots of the run) to resolve it
-    parts = [sg.flow_samples(case, 8, 1 << 20, seed=1), sg.flow_samples(case, 16, 1 << 20, seed=2)]
-    hist = sg.train_on(parts, epochs=a.sg_epochs)
-    train_s = time.perf_counter() - t0
     L = solver.lib()
     chk = solver._chk
-    res = {}
-    for mode in (0, 1):
+    nz = a.nz or 256
+    case = cases.jet(nx=384, ny=256, nz=nz)
+    name = "jet-%dx%dx%d-H2air-9sp-19reac-WENO5-CD6-SW-Wilke-implicitChem" % case.shape
+    dt, nsub, N = case.dt, case.nsub, case.ncell
+    n_e2e = 0 if a.no_e2e else max(1, min(a.e2e_steps, 5))
+    n_prof = 2
+    total = max(a.total_steps, 1 + a.warmup + a.steps + n_prof + n_e2e)
+
+    # ---- surrogate training set: cells of an FP64 run after 8 and 16 steps ----
+    sg, train = None, None
+    if not a.no_surrogate:
+        sg = surrogate.Surrogate()
+        t0 = time.perf_counter()
         g = solver.Solver(case)
         g.init_state()
-        if mode == 1:
-            chk(L.ocfd_gpu_chem_mode(1, a.sg_tol))
-        dt, tt = case.dt, 0.0
-        chk(L.ocfd_gpu_run(dt, tt, a.warmup, 1, case.nsub))
-        tt += a.warmup * dt
-        with Clocks(0) as clk:
-            chk(L.ocfd_gpu_event_record(0))
-            chk(L.ocfd_gpu_run(dt, tt, a.steps, 1, case.nsub))
-            chk(L.ocfd_gpu_event_record(1))
-            ms = C.c_double()
-            chk(L.ocfd_gpu_event_elapsed(0, 1, C.byref(ms)))
-        reasons = (C.c_longlong * 5)()
-        rejected = L.ocfd_gpu_chem_surrogate_rejected(reasons) if mode == 1 else 0
-        f, di, prims = g.download_state()
+        parts = []
+        for s0, s1, seed in ((0, 8, 1), (8, 16, 2)):
+            chk(L.ocfd_gpu_run(dt, s0 * dt, s1 - s0, 1, nsub))
+            _, di, prims = g.download_state()
+            parts.append(sg.samples_from_state(case, di, prims, 1 << 20, seed))
         g.close()
-        Li = 4
-        T = prims[4][Li:-Li, Li:-Li, Li:-Li]
-        dd = di[:, Li:-Li, Li:-Li, Li:-Li]
-        Y = dd / dd.sum(axis=0, keepdims=True)
-        res[mode] = dict(ms=ms.value / a.steps, T=T, Y=Y, rejected=rejected, reasons=list(reasons), clocks=clk.summary())
-    T0, T1 = res[0]["T"], res[1]["T"]
-    ncell = case.ncell
-    out = {"metric": METRIC, "value": ncell / (res[1]["ms"] * 1e-3) / 1e6, "unit": UNIT, "n_gpus": 1,
-           "steps": a.steps, "warmup": a.warmup, "ms_per_step": res[1]["ms"], "higher_is_better": True,
-           "scaling": "weak", "vs_baseline": None, "dtype": "f64 flow + bf16 gated surrogate chemistry",
-           "data": "synthetic (seeded)",
-           "config": {"workload": name + "-surrogateChem", "cells_per_gpu": ncell, "dt": case.dt,
-                      "train": "2 x 2^20 cells of jet snapshots after 8 and 16 steps, %d epochs, %.0f s" %
-                               (a.sg_epochs, train_s),
-                      "loss_first_last": [float(hist[0]), float(hist[-1])], "tol_T_K": a.sg_tol},
-           "plain_fp64": {"value": ncell / (res[0]["ms"] * 1e-3) / 1e6, "ms_per_step": res[0]["ms"]},
-           "speedup_vs_plain": res[0]["ms"] / res[1]["ms"],
-           "accuracy_vs_plain_after_steps": {
-               "steps": a.warmup + a.steps,
-               "peak_T_rel_err": float(abs(T1.max() - T0.max()) / T0.max()),
-               "T_err_max_K": float(np.abs(T1 - T0).max()),
-               "Y_err_max": float(np.abs(res[1]["Y"] - res[0]["Y"]).max())},
-           "rejected_cells_last_call": int(res[1]["rejected"]),
-           "rejection_reasons": dict(zip(["negative_Y", "T_check", "T_range", "logp_range", "logdt_range"],
-                                         res[1]["reasons"])),
-           "clocks": res[1]["clocks"], "cpu_baseline": None, "e2e": None, "gpu_launches": None}
-    print(json.dumps(out))
+        hist = sg.train_on(parts, epochs=a.sg_epochs)
+        train = {"cells": sum(len(p[1]) for p in parts), "epochs": a.sg_epochs,
+                 "source": "2 x 2^20 cells of the plain FP64 jet run after 8 and 16 steps (seeded choice)",
+                 "seconds": round(time.perf_counter() - t0, 1),
+                 "loss_first_last": [float(hist[0]), float(hist[-1])]}
+
+    # ---- plain FP64 chemistry: tune, warm up, K timed steps, roofline, e2e, up to `total` ----
+    g = solver.Solver(case)
+    state_gb = L.ocfd_gpu_device_bytes() / 1e9
+    g.init_state()
+    tt, done = 0.0, 0
+    chk(L.ocfd_gpu_run(dt, tt, 1, 1, nsub))  # one step so that the tuner sees a running state
+    tt += dt
+    done += 1
+    tiles = {"mode": a.tiles, "choice": g.tiles()}
+    if a.tiles == "auto":
+        choice, tms = g.autotune(reps=5)
+        tiles = {"mode": "auto", "choice": choice}
+    elif a.tiles != "default":
+        g.set_tiles([int(x) for x in a.tiles.split(",")])
+        tiles = {"mode": "given", "choice": g.tiles()}
+    chk(L.ocfd_gpu_run(dt, tt, a.warmup, 1, nsub))
+    tt += a.warmup * dt
+    done += a.warmup
+    ranks.barrier()
+    ms, launches, clk_plain = timed_run(L, dt, tt, a.steps, 1, nsub)
+    ranks.barrier()
+    tt += a.steps * dt
+    done += a.steps
+    el_ms = ranks.max(ms)
+    value = ranks.world * N * a.steps / (el_ms * 1e-3) / 1e6
+    solver.Solver.profile(True)
+    for s in range(n_prof):
+        g.tt = tt
+        g.step(dt, 1, nsub)
+        tt += dt
+    prof = solver.Solver.profile_read()
+    solver.Solver.profile(False)
+    done += n_prof
+    roof = jet_roofline(prof, n_prof, N)
+    e2e = None
+    if n_e2e:
+        e2e, tt = e2e_steps(L, case, dt, tt, n_e2e, 1, nsub, ranks)
+        done += n_e2e
+    if total > done:
+        chk(L.ocfd_gpu_run(dt, tt, total - done, 1, nsub))
+        tt += (total - done) * dt
+    _, di0, pr0 = g.download_state()
+    g.close()
+    Li = 4
+    T0 = pr0[4][Li:-Li, Li:-Li, Li:-Li].copy()
+    d0 = di0[:, Li:-Li, Li:-Li, Li:-Li]
+    Y0 = d0 / d0.sum(axis=0, keepdims=True)
+    del di0, pr0, d0
+    chem_share = roof["classes"].get("chem", {}).get("share_of_step")
+
+    # ---- gated surrogate chemistry: same start, same steps ----
+    sgo = None
+    clk_sg = {}
+    if sg is not None:
+        g = solver.Solver(case)
+        g.init_state()
+        chk(L.ocfd_gpu_chem_mode(1, a.sg_tol))
+        tt = 0.0
+        chk(L.ocfd_gpu_run(dt, tt, 1, 1, nsub))
+        tt += dt
+        if tiles["mode"] == "auto":
+            g.autotune(reps=0)  # the plain run's choice, remembered for this configuration
+        else:
+            g.set_tiles(tiles["choice"])
+        chk(L.ocfd_gpu_run(dt, tt, a.warmup, 1, nsub))
+        tt += a.warmup * dt
+        ranks.barrier()
+        ms_sg, _, clk_sg = timed_run(L, dt, tt, a.steps, 1, nsub)
+        ranks.barrier()
+        tt += a.steps * dt
+        reasons = (C.c_longlong * 5)()
+        rejected = L.ocfd_gpu_chem_surrogate_rejected(reasons)
+        rest = total - (1 + a.warmup + a.steps)
+        if rest > 0:
+            chk(L.ocfd_gpu_run(dt, tt, rest, 1, nsub))
+        _, di1, pr1 = g.download_state()
+        g.close()
+        T1 = pr1[4][Li:-Li, Li:-Li, Li:-Li]
+        d1 = di1[:, Li:-Li, Li:-Li, Li:-Li]
+        Y1 = d1 / d1.sum(axis=0, keepdims=True)
+        ms_sg = ranks.max(ms_sg)
+        peak = float(abs(T1.max() - T0.max()) / T0.max())
+        yerr = float(np.abs(Y1 - Y0).max())
+        sgo = {"value": ranks.world * N * a.steps / (ms_sg * 1e-3) / 1e6, "unit": UNIT,
+               "ms_per_step": ms_sg / a.steps, "speedup_vs_plain": el_ms / ms_sg,
+               "accuracy_vs_plain_fp64": {
+                   "steps": total, "peak_T_rel_err": peak,
+                   "T_err_max_K": float(np.abs(T1 - T0).max()),
+                   "T_err_rel_max": float((np.abs(T1 - T0) / T0).max()),
+                   "Y_err_max": yerr,
+                   "target": "peak T error <= 1 %, species mass fraction error <= 1e-3",
+                   "meets_target": bool(peak <= 0.01 and yerr <= 1e-3)},
+               "fallback_fraction_last_step": rejected / N,
+               "rejection_reasons_last_step": dict(zip(["negative_Y", "T_check", "T_range", "logp_range",
+                                                         "logdt_range"], list(reasons))),
+               "tol_T_K": a.sg_tol, "train": train,
+               "chemistry_share_of_plain_step": chem_share,
+               "amdahl_bound_on_speedup": (1.0 / (1.0 - chem_share)) if chem_share else None,
+               "clocks": clk_sg}
+
+    cpu = None
+    if ranks.rank == 0 and ranks.world == 1 and not a.no_cpu:
+        cpu = cpu_sample("jet")
+    if ranks.rank == 0:
+        out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ranks.world, "steps": a.steps,
+               "warmup": a.warmup, "ms_per_step": el_ms / a.steps, "higher_is_better": True, "scaling": "weak",
+               "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
+               "value_form": "plain FP64 chemistry (implicit Euler + Gauss, the reference's integrator)",
+               "config": {"workload": name, "cells_per_gpu": N, "dt": dt, "steps_per_run": total,
+                          "chemistry": "plain FP64 implicit Euler, %d sub-step per step; surrogate run: gated BF16 "
+                                       "MLP with FP64 fallback" % nsub,
+                          "parallelism": "replicas x%d (no data-path collective)" % ranks.world,
+                          "tiles": tiles,
+                          "l2": "device state %.1f GB per GPU >> 126 MB L2; no flush between steps" % state_gb},
+               "surrogate": sgo,
+               "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches),
+               "clocks": merge_clocks(clk_plain, clk_sg) if clk_sg else clk_plain}
+        print(json.dumps(out))
+    ranks.close()
     return 0
 
 
 def main_ours(a):
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    if world > 1:
-        vis = os.environ.get("CUDA_VISIBLE_DEVICES")
-        devs = vis.split(",") if vis else [str(i) for i in range(64)]
-        os.environ["CUDA_VISIBLE_DEVICES"] = devs[local]
+    ranks = Ranks()
+    world, rank = ranks.world, ranks.rank
     import numpy as np
-    import torch
-    dist = None
-    if world > 1:
-        import datetime
-        import torch.distributed as dist
-        torch.cuda.set_device(0)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
-
     from ocfd_b200 import abi, solver
     L = solver.lib()
     import ctypes as C
-
-    def barrier():
-        if dist is not None:
-            dist.barrier()
-        torch.cuda.synchronize()
-
-    def max_over_ranks(x):
-        if dist is None:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+    barrier, max_over_ranks = ranks.barrier, ranks.max
 
     c, name = make_case(a.workload, nz=a.nz)
     if a.character:
@@ -565,102 +838,50 @@ def main_ours(a):
         tt += dt
     prof = solver.Solver.profile_read()
     solver.Solver.profile(False)
-    step_ms = sum(v[0] for v in prof.values()) / 2.0
-    dom = max((k for k in prof if k in ALG_BYTES_PER_CELL), key=lambda k: prof[k][0])
-    dom_ms = prof[dom][0] / max(prof[dom][1], 1)
-    hbm, hbm_kind = peaks()
-    alg = ALG_BYTES_PER_CELL[dom] * c.ncell
-    achieved = alg / (dom_ms * 1e-3) / 1e9
-    traffic = None
-    tfile = os.path.join(ROOT, "profiles", "traffic_per_cell.json")
-    if os.path.exists(tfile):
-        with open(tfile) as fh:
-            tr = json.load(fh)
-        if dom in tr:
-            traffic = tr[dom] * c.ncell
-    fp64 = solver.fp64_peak_gflops()
-    # the build keeps multiplies and adds separate (no FMA), so the FP64 operation peak is half
-    # the measured FMA flop rate
-    fp64_ops_peak = fp64 / 2.0
-    fp64_roof = None
-    if a.workload == "flatplate" and dom in ALG_FLOPS_PER_CELL:
-        ops = ALG_FLOPS_PER_CELL[dom] * c.ncell
-        ach = ops / (dom_ms * 1e-3) / 1e9
-        fp64_roof = {"achieved": ach, "peak": fp64_ops_peak, "unit": "GFLOP/s", "frac": ach / fp64_ops_peak,
-                     "alg_flops_per_launch": ops, "peak_kind": "measured FP64 FMA rate / 2 (no-FMA build)"}
-    roof = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm, "unit": "GB/s",
-            "frac": achieved / hbm, "traffic": traffic, "peak_kind": hbm_kind,
-            "alg_bytes_per_launch": alg, "avg_launch_ms": dom_ms,
-            "share_of_step": prof[dom][0] / 2.0 / step_ms if step_ms > 0 else None,
-            "fp64": fp64_roof,
-            "fp64_fma_peak_gflops_measured": fp64,
-            "kernel_shares": {k: round(v[0] / 2.0 / step_ms, 4) for k, v in prof.items() if v[1] > 0}}
+    if a.workload == "jet":
+        roof = jet_roofline(prof, 2, c.ncell)
+    else:
+        step_ms = sum(v[0] for v in prof.values()) / 2.0
+        dom = max((k for k in prof if k in ALG_BYTES_PER_CELL and prof[k][1] > 0), key=lambda k: prof[k][0])
+        dom_ms = prof[dom][0] / max(prof[dom][1], 1)
+        hbm, hbm_kind = peaks()
+        alg = ALG_BYTES_PER_CELL[dom] * c.ncell
+        achieved = alg / (dom_ms * 1e-3) / 1e9
+        traffic = None
+        tfile = os.path.join(ROOT, "profiles", "traffic_per_cell.json")
+        if os.path.exists(tfile) and a.workload == "flatplate":
+            with open(tfile) as fh:
+                tr = json.load(fh)
+            if dom in tr:
+                traffic = tr[dom] * c.ncell
+        fp64 = solver.fp64_peak_gflops()
+        # the build keeps multiplies and adds separate (no FMA), so the FP64 operation peak is half
+        # the measured FMA flop rate
+        fp64_ops_peak = fp64 / 2.0
+        fp64_roof = None
+        if a.workload == "flatplate" and dom in ALG_FLOPS_PER_CELL:
+            ops = ALG_FLOPS_PER_CELL[dom] * c.ncell
+            ach = ops / (dom_ms * 1e-3) / 1e9
+            fp64_roof = {"achieved": ach, "peak": fp64_ops_peak, "unit": "GFLOP/s", "frac": ach / fp64_ops_peak,
+                         "alg_flops_per_launch": ops, "peak_kind": "measured FP64 FMA rate / 2 (no-FMA build)"}
+        roof = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                "frac": achieved / hbm, "traffic": traffic, "peak_kind": hbm_kind,
+                "alg_bytes_per_launch": alg, "avg_launch_ms": dom_ms,
+                "share_of_step": prof[dom][0] / 2.0 / step_ms if step_ms > 0 else None,
+                "fp64": fp64_roof,
+                "fp64_fma_peak_gflops_measured": fp64,
+                "kernel_shares": {k: round(v[0] / 2.0 / step_ms, 4) for k, v in prof.items() if v[1] > 0}}
 
     # ---- e2e through the C ABI with host buffers ----
     e2e = None
     if not a.no_e2e:
-        nx, ny, nz = c.shape
-        hs = c.halo_shape()
-        H = hs[0] * hs[1] * hs[2]
-        N = c.ncell
-        ns = c.params.n_spec
-        nbytes_f, nbytes_di, nbytes_pr = 8 * 5 * N, 8 * ns * H, 8 * 7 * H
-        bufs = []
-
-        def pinned(nb, shape):
-            p = C.c_void_p()
-            chk(L.ocfd_gpu_pinned_alloc(nb, C.byref(p)))
-            bufs.append(p)
-            arr = np.ctypeslib.as_array(C.cast(p, C.POINTER(C.c_double)), shape=shape)
-            return arr
-
-        hf = pinned(nbytes_f, (5, nz, ny, nx))
-        hdi = pinned(nbytes_di, (ns,) + hs)
-        hpr = pinned(nbytes_pr, (7,) + hs)
-        chk(L.ocfd_gpu_download_state(abi.dptr(hf), abi.dptr(hdi), abi.dptr(hpr)))
-        barrier()
-        chk(L.ocfd_gpu_event_record(2))
-        for s in range(a.e2e_steps):
-            chk(L.ocfd_gpu_upload_state(abi.dptr(hf), abi.dptr(hdi), abi.dptr(hpr)))
-            chk(L.ocfd_gpu_run(dt, tt, 1, reac, nsub))
-            tt += dt
-            chk(L.ocfd_gpu_download_state(abi.dptr(hf), abi.dptr(hdi), None))
-        chk(L.ocfd_gpu_event_record(3))
-        ms2 = C.c_double()
-        chk(L.ocfd_gpu_event_elapsed(2, 3, C.byref(ms2)))
-        e2e_ms = max_over_ranks(ms2.value)
-        e2e = {"value": world * N * a.e2e_steps / (e2e_ms * 1e-3) / 1e6, "unit": UNIT,
-               "h2d_bytes_per_step": nbytes_f + nbytes_di + nbytes_pr, "d2h_bytes_per_step": nbytes_f + nbytes_di,
-               "steps": a.e2e_steps}
-        for p in bufs:
-            L.ocfd_gpu_pinned_free(p)
+        e2e, tt = e2e_steps(L, c, dt, tt, a.e2e_steps, reac, nsub, ranks)
     g.close()
 
     # ---- CPU baseline (rank 0, N = 1): the oracle on a bounded sample ----
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu:
-        sys.path.insert(0, os.path.join(ROOT, "oracle"))
-        import pyoracle
-        cores = pyoracle.lib().ocfd_cpu_set_threads(os.cpu_count() or 1)
-        if a.workload == "flatplate":
-            cs, _ = make_case("flatplate", nz=16)
-            sample = "one time step of a 1024x160x16 slab of the workload (z periodic), after one warm-up step"
-        elif a.workload == "jet":
-            from ocfd_b200 import cases
-            cs = cases.jet(nx=96, ny=64, nz=64)
-            sample = "one reacting time step of the jet on a 96x64x64 grid (same physics), after one warm-up step"
-        else:
-            cs, _ = make_case("isotropic")
-            sample = "one time step of the 64^3 workload after one warm-up step"
-        o = pyoracle.OracleSolver(cs)
-        o.init_state()
-        creac, cnsub = int(getattr(cs, "if_reaction", 0) or 0), int(getattr(cs, "nsub", 1) or 1)
-        o.step(cs.dt, 0.0, creac, cnsub)
-        t0 = time.perf_counter()
-        o.step(cs.dt, cs.dt, creac, cnsub)
-        el = time.perf_counter() - t0
-        o.close()
-        cpu = {"value": cs.ncell / el / 1e6, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample}
+        cpu = cpu_sample(a.workload)
 
     if rank == 0:
         out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps,
@@ -673,9 +894,7 @@ def main_ours(a):
                "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches),
                "clocks": clk.summary()}
         print(json.dumps(out))
-    if dist is not None:
-        dist.barrier()
-        dist.destroy_process_group()
+    ranks.close()
     return 0
 
 
@@ -687,6 +906,6 @@ if __name__ == "__main__":
         sys.exit(main_reactors(a) if int(os.environ.get("RANK", "0")) == 0 else 0)
     if a.workload == "surrogate":
         sys.exit(main_surrogate(a) if int(os.environ.get("RANK", "0")) == 0 else 0)
-    if a.workload == "jet" and a.surrogate:
-        sys.exit(main_jet_surrogate(a) if int(os.environ.get("RANK", "0")) == 0 else 0)
+    if a.workload == "jet" and not a.no_surrogate:
+        sys.exit(main_jet(a))
     sys.exit(main_ours(a))

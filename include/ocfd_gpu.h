@@ -46,6 +46,8 @@ extern "C" {
 #define OCFD_ERR_STATE (-5)       /* call order violated (e.g. advance before init) */
 #define OCFD_ERR_TIMEOUT (-6)     /* a bounded device wait ran out (persistent chemistry queue) */
 #define OCFD_ERR_UNSUPPORTED (-7) /* reference feature outside the built scope */
+#define OCFD_ERR_CHEM (-8)        /* chemistry: zero pivot in the implicit step's Gauss elimination
+                                     (CHEM_reactions.f90:523-567) or a non-finite reactor result */
 
 /* scheme / option ids: code/head/MODULE_parameter.f90:13-30 */
 #define OCFD_SCHEME_WENO5 1
@@ -214,9 +216,18 @@ int ocfd_gpu_download_metrics(double* metrics);
  * work-queue kernel on the device; host buffers in and out. */
 int ocfd_gpu_chem_batch(int n, double* di, double* e, const double* dt, const int* nsub);
 
-/* Same as ocfd_gpu_chem_batch with device pointers (no host copies). */
+/* Same as ocfd_gpu_chem_batch with device pointers (no host copies).
+ * The batched calls (these two and ocfd_gpu_chem_batch_noalloc) return OCFD_ERR_CHEM when a
+ * reactor's implicit step met a zero Gauss pivot or its result is not finite: every reactor's
+ * values are still written back as computed (the reference divides by the zero pivot and goes
+ * on), the code reports it. n < 0 is OCFD_ERR_PARAM, n = 0 does nothing. */
 int ocfd_gpu_chem_batch_device(int n, double* d_di, double* d_e, const double* d_dt,
                                const int* d_nsub);
+
+/* The last batched chemistry call's counts: reactors whose Newton T(E) iteration did not converge
+ * (comput_T_rgas, CHEM_thermdyn.f90:327-382, at most 31 iterations) and reactors reported by
+ * OCFD_ERR_CHEM (zero pivot or non-finite result). Either pointer may be NULL. */
+int ocfd_gpu_chem_batch_status(long long* newton_fail, long long* bad);
 
 /* Sets up the chemistry tables alone (no grid) for ocfd_gpu_chem_batch: read_Spec + read_Reac
  * content, IF_RealGas and CHEM_TimeAdv. */

@@ -21,17 +21,17 @@ namespace ocfd {
 
 void launch_chem_cells(int ns, long long ncell, double* f, double* Et, double* T, double* p, double* di, double dt2,
                        int nsub, int* nfail, cudaStream_t st) {
-  unsigned nb = (unsigned)((ncell + 127) / 128);
-  NS_CASES(k_chem_cells<NSV><<<nb, 128, 0, st>>>(f, Et, T, p, di, dt2, nsub, nfail));
+  unsigned nb = (unsigned)((ncell + OCFD_CHEM_TPB - 1) / OCFD_CHEM_TPB);
+  NS_CASES(k_chem_cells<NSV><<<nb, OCFD_CHEM_TPB, 0, st>>>(f, Et, T, p, di, dt2, nsub, nfail));
 }
 
 void launch_chem_batch(int ns, int sms, int n, double* di, double* e, const double* dt, const int* nsub,
                        const int* perm, int* counter, int* nfail, cudaStream_t st) {
   NS_CASES({
     int per = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_chem_batch<NSV>, 128, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_chem_batch<NSV>, OCFD_CHEM_TPB, 0);
     if (per < 1) per = 1;
-    k_chem_batch<NSV><<<sms * per, 128, 0, st>>>(n, di, e, dt, nsub, perm, counter, nfail);
+    k_chem_batch<NSV><<<sms * per, OCFD_CHEM_TPB, 0, st>>>(n, di, e, dt, nsub, perm, counter, nfail);
   });
 }
 }  // namespace ocfd

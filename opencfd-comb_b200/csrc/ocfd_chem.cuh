@@ -6,82 +6,104 @@
 // Euler with a partially pivoted Gauss elimination). The mechanism lives in constant memory, so
 // the reaction loops are warp-uniform broadcasts.
 //
+// Nothing of a reactor is indexed at run time in thread-local memory: the reference's per-reaction
+// coefficient arrays (wf, wr) are consumed inside one reaction loop, the species loops are unrolled
+// (registers), and the NS x NS implicit-Euler matrix lives in the block's shared memory, one
+// column-strided slab per thread (element m of thread t at sA[m * TPB + t]: a warp's accesses
+// are consecutive words). The Gauss elimination is unrolled over the pivot column; only the pivot
+// row index is a run-time value (a shared-memory address; the right-hand side in registers is
+// swapped by predicated selects). Empty asm statements with a memory clobber between the matrix
+// columns / rows keep the compiler from hoisting every shared-memory load of the unrolled loops
+// to the top (which made it spill).
+//
 // k_chem_cells : Chemical_time_advance x nsub + comput_T_P on the flow grid (OCFD_Time_Adv.f90:169-196)
 // k_chem_batch : independent 0-D reactors as a persistent work queue. Reactors are visited in
 //                descending order of their sub-step count (counting sort on the device), so the
 //                32 reactors of a warp carry near-equal work and long reactors start first.
+//
+// Error words (nfail points at two ints): nfail[0] counts Newton T(E) iterations that did not
+// converge (comput_T_rgas, CHEM_thermdyn.f90:327-382), nfail[1] reactors whose Gauss elimination
+// met a zero pivot or whose result is not finite. The arithmetic goes on as the reference's
+// does (a zero pivot divides by zero); the host turns nfail[1] > 0 into an error code.
 #pragma once
 #include "ocfd_device.cuh"
 
-// resident 128-thread blocks per SM given to the register allocator of the chemistry kernels:
-// 3 (at most 170 registers) measured 16-18 % faster than the unconstrained 255 registers on the
-// 2^20-reactor batch and the jet's cells, 4 (128 registers) spills too much
+// threads per block of the chemistry kernels and the resident-block target given to the register
+// allocator: 64-thread blocks hold their 64 implicit-Euler matrices in 41.5 KB of shared memory
+// (9 species); four of them per SM (two warps per scheduler) leave 255 registers per thread, which
+// the 9-species cell kernel fills without spilling (five blocks cap it at 168 and spill 400 bytes)
+#ifndef OCFD_CHEM_TPB
+#define OCFD_CHEM_TPB 64
+#endif
 #ifndef OCFD_CHEM_MINB
-#define OCFD_CHEM_MINB 3
+#define OCFD_CHEM_MINB 4
 #endif
 
 namespace ocfd {
 
+// one thread's NS x NS matrix in a column-strided shared-memory slab
+template <int STRIDE>
+struct Slab {
+  double* b;
+  __device__ __forceinline__ double& operator[](int m) const { return b[m * STRIDE]; }
+};
+
+// Forward and reverse rate coefficients of reaction j (Reaction_rate_coef,
+// CHEM_reactions.f90:130-197), three-body factor included. Arrhenius A T^b exp(-E/T) is evaluated
+// as A exp(b ln T - E (1/T)) with ln T and 1/T formed once per reactor: the same quantity, one
+// exponential instead of a power and an exponential. 0.67 and 1.27 of the Troe form are
+// single-precision literals in the reference.
 template <int NS>
-__device__ __forceinline__ void rate_coef(const double* ci, double* wf, double* wr, double T) {
-  double gi[NS];
-  double Rs = 8.314 / 1.013e5 * 1.0e6;
-  if (cC.rereac == 0) {
-    double lt = log(T);
+__device__ __forceinline__ void rate_coef_j(int j, const double* ci, const double* gi, double T, double lt, double rT,
+                                            double& w, double& r) {
+  double Ctrb = 0.0;
+  const int tb = cC.tr_reac[j];
+  if (tb == 1) {
 #pragma unroll
-    for (int i = 0; i < NS; i++) gi[i] = dev_gibbs(i, T, lt);
+    for (int i = 0; i < NS; i++) Ctrb = Ctrb + ci[i] * cC.treff[j][i];
   }
-  for (int j = 0; j < cC.nreac; j++) {
-    double Ctrb = 0.0;
-    if (cC.tr_reac[j] == 1) {
+  const double wf1 = cC.af[j][0] * exp(cC.bf[j][0] * lt - cC.ef[j][0] * rT);
+  const int at = cC.af_type[j];
+  if (at == 0) {
+    w = wf1;
+  } else {
+    const double wf2 = cC.af[j][1] * exp(cC.bf[j][1] * lt - cC.ef[j][1] * rT);
+    if (at == 2) {
+      w = wf1 + wf2;
+    } else {  // Troe fall-off
+      double Prs = wf1 / wf2 * Ctrb;
+      double lfc = log10(cC.fc_troe[j]);
+      double ac = -0.4 - (double)0.67f * lfc;
+      double an = 0.75 - (double)1.27f * lfc;
+      double lpr = log10(Prs);
+      double qq = (lpr + ac) / (an - 0.14 * (lpr + ac));
+      double Fx = pow(10.0, lfc / (1.0 + q2(qq)));
+      w = wf2 * Prs / (1.0 + Prs) * Fx;
+    }
+  }
+  if (cC.rereac == 0) {
+    const double Rs = 8.314 / 1.013e5 * 1.0e6;
+    double dgi = 0.0;
 #pragma unroll
-      for (int i = 0; i < NS; i++) Ctrb = Ctrb + ci[i] * cC.treff[j][i];
-    }
-    double wf1 = cC.af[j][0] * pow(T, cC.bf[j][0]) * exp(-cC.ef[j][0] / T);
-    double w;
-    const int at = cC.af_type[j];
-    if (at == 0) {
-      w = wf1;
-    } else {
-      double wf2 = cC.af[j][1] * pow(T, cC.bf[j][1]) * exp(-cC.ef[j][1] / T);
-      if (at == 2) {
-        w = wf1 + wf2;
-      } else {  // Troe fall-off; 0.67 and 1.27 are single-precision literals in the reference
-        double Prs = wf1 / wf2 * Ctrb;
-        double lfc = log10(cC.fc_troe[j]);
-        double ac = -0.4 - (double)0.67f * lfc;
-        double an = 0.75 - (double)1.27f * lfc;
-        double lpr = log10(Prs);
-        double qq = (lpr + ac) / (an - 0.14 * (lpr + ac));
-        double Fx = pow(10.0, lfc / (1.0 + q2(qq)));
-        w = wf2 * Prs / (1.0 + Prs) * Fx;
-      }
-    }
-    double r;
-    if (cC.rereac == 0) {
-      double dgi = 0.0;
-#pragma unroll
-      for (int i = 0; i < NS; i++) dgi = dgi + gi[i] * (double)(cC.vr[j][i] - cC.vf[j][i]);
-      double kjx = exp(-dgi / T) * powi_rt(Rs * T, -cC.sgm[j]);
-      r = w / kjx;
-    } else if (cC.rereac == 1) {
-      r = cC.ar[j] * pow(T, cC.br[j]) * exp(-cC.er[j] / T);
-    } else {
-      double z = 10000.0 / T;
-      double kj = exp(cC.park[j][0] + cC.park[j][1] * z + cC.park[j][2] * q2(z) + cC.park[j][3] * q3(z) +
-                      cC.park[j][4] * q4(z));
-      if (kj < 1.0e-30) kj = 1.0e-30;
-      r = w / kj;
-    }
-    if (cC.tr_reac[j] == 1 && at != 1) {
-      w = w * Ctrb;
-      r = r * Ctrb;
-    }
-    wf[j] = w;
-    wr[j] = r;
+    for (int i = 0; i < NS; i++) dgi = dgi + gi[i] * (double)(cC.vr[j][i] - cC.vf[j][i]);
+    double kjx = exp(-dgi * rT) * powi_rt(Rs * T, -cC.sgm[j]);
+    r = w / kjx;
+  } else if (cC.rereac == 1) {
+    r = cC.ar[j] * exp(cC.br[j] * lt - cC.er[j] * rT);
+  } else {
+    double z = 10000.0 * rT;
+    double kj = exp(cC.park[j][0] + cC.park[j][1] * z + cC.park[j][2] * q2(z) + cC.park[j][3] * q3(z) +
+                    cC.park[j][4] * q4(z));
+    if (kj < 1.0e-30) kj = 1.0e-30;
+    r = w / kj;
+  }
+  if (tb == 1 && at != 1) {
+    w = w * Ctrb;
+    r = r * Ctrb;
   }
 }
 
+// rate-of-progress factors: w prod c^vf, r prod c^vr (CHEM_reactions.f90:213-218, 245-250)
 template <int NS>
 __device__ __forceinline__ void progress(const double* ci, double wf, double wr, int k, double& wf1, double& wr1) {
   wf1 = wf;
@@ -94,81 +116,128 @@ __device__ __forceinline__ void progress(const double* ci, double wf, double wr,
   }
 }
 
+// Gibbs energies of every species (comput_gibbs) when the reverse rates use Kc
+template <int NS>
+__device__ __forceinline__ void gibbs_all(double T, double lt, double* gi) {
+  if (cC.rereac == 0) {
+    const int jc = trange(T);
+#pragma unroll
+    for (int i = 0; i < NS; i++) gi[i] = dev_gibbs_jc(i, jc, T, lt);
+  }
+}
+
 // Reaction_rate (CHEM_reactions.f90:203-225)
 template <int NS>
 __device__ void reaction_rate(const double* ci, double* ri, double T) {
-  double wf[OCFD_MAX_REAC], wr[OCFD_MAX_REAC];
-  rate_coef<NS>(ci, wf, wr, T);
+  const double lt = log(T), rT = 1.0 / T;
+  double gi[NS];
+  gibbs_all<NS>(T, lt, gi);
 #pragma unroll
   for (int i = 0; i < NS; i++) ri[i] = 0.0;
   for (int k = 0; k < cC.nreac; k++) {
-    double wf1, wr1;
-    progress<NS>(ci, wf[k], wr[k], k, wf1, wr1);
+    double w, r, wf1, wr1;
+    rate_coef_j<NS>(k, ci, gi, T, lt, rT, w, r);
+    progress<NS>(ci, w, r, k, wf1, wr1);
 #pragma unroll
     for (int i = 0; i < NS; i++) ri[i] = ri[i] + (wf1 - wr1) * (double)(cC.vr[k][i] - cC.vf[k][i]);
   }
 }
 
-// Reaction_rate_and_Matrix (CHEM_reactions.f90:230-272); Ar[i*NS+j] = d r_i / d c_j
-template <int NS>
-__device__ void reaction_rate_matrix(const double* ci, double* ri, double* Ar, double T) {
-  double wf[OCFD_MAX_REAC], wr[OCFD_MAX_REAC];
-  rate_coef<NS>(ci, wf, wr, T);
+// Reaction_rate_and_Matrix (CHEM_reactions.f90:230-272): ri and Ar(i, j) = d r_i / d c_j into the
+// thread's slab (Ar[i * NS + j]). The division by c_j + 1e-20 is a multiplication by its
+// reciprocal, formed once per species (the same quantity up to the last place).
+template <int NS, int STRIDE>
+__device__ void reaction_rate_matrix(const double* ci, double* ri, Slab<STRIDE> Ar, double T) {
+  const double lt = log(T), rT = 1.0 / T;
+  double gi[NS], rc[NS];
+  gibbs_all<NS>(T, lt, gi);
+#pragma unroll
   for (int i = 0; i < NS; i++) {
     ri[i] = 0.0;
-    for (int j = 0; j < NS; j++) Ar[i * NS + j] = 0.0;
+    rc[i] = 1.0 / (ci[i] + 1.0e-20);
   }
+#pragma unroll
+  for (int m = 0; m < NS * NS; m++) Ar[m] = 0.0;
   for (int k = 0; k < cC.nreac; k++) {
-    double wf1, wr1;
-    progress<NS>(ci, wf[k], wr[k], k, wf1, wr1);
+    double w, r, wf1, wr1;
+    rate_coef_j<NS>(k, ci, gi, T, lt, rT, w, r);
+    progress<NS>(ci, w, r, k, wf1, wr1);
+    double s[NS];
 #pragma unroll
-    for (int i = 0; i < NS; i++) ri[i] = ri[i] + (wf1 - wr1) * (double)(cC.vr[k][i] - cC.vf[k][i]);
+    for (int i = 0; i < NS; i++) {
+      s[i] = (double)(cC.vr[k][i] - cC.vf[k][i]);
+      ri[i] = ri[i] + (wf1 - wr1) * s[i];
+    }
+#pragma unroll
     for (int j = 0; j < NS; j++) {
-      int a = cC.vf[k][j], b = cC.vr[k][j];
+      const int a = cC.vf[k][j], b = cC.vr[k][j];
       if (a == 0 && b == 0) continue;  // both derivatives are exactly +0: adding them changes nothing
-      double Awf = (double)a * wf1 / (ci[j] + 1.0e-20);
-      double Awr = (double)b * wr1 / (ci[j] + 1.0e-20);
-      double dA = Awf - Awr;
+      const double dA = (double)a * wf1 * rc[j] - (double)b * wr1 * rc[j];
 #pragma unroll
-      for (int i = 0; i < NS; i++) Ar[i * NS + j] = Ar[i * NS + j] + dA * (double)(cC.vr[k][i] - cC.vf[k][i]);
+      for (int i = 0; i < NS; i++) Ar[i * NS + j] = Ar[i * NS + j] + dA * s[i];
+      asm volatile("" ::: "memory");  // one column's loads at a time (keeps the register pressure low)
     }
   }
 }
 
-// Gauss elimination with partial pivoting (CHEM_reactions.f90:523-567); a is row-major NSxNS.
-// Columns left of the pivot are never read again, so only columns >= k are updated.
-template <int NS>
-__device__ void gauss(double* a, double* b, double* x) {
+// Gauss elimination with partial pivoting (CHEM_reactions.f90:523-567) on the thread's slab
+// (row-major NS x NS), right-hand side b in registers, solution into x. Columns left of the pivot
+// are never read again, so only columns >= k are updated. Returns true when a pivot was zero
+// (the reference then divides by zero; so does this, so the values stay the reference's).
+template <int NS, int STRIDE>
+__device__ __forceinline__ bool gauss(Slab<STRIDE> a, double* b, double* x) {
+  bool zero = false;
+#pragma unroll
   for (int k = 0; k < NS - 1; k++) {
     double fmax = fabs(a[k * NS + k]);
     int kk = k;
-    for (int i = k + 1; i < NS; i++)
-      if (fabs(a[i * NS + k]) > fmax) {
-        fmax = fabs(a[i * NS + k]);
+#pragma unroll
+    for (int i = k + 1; i < NS; i++) {
+      const double v = fabs(a[i * NS + k]);
+      if (v > fmax) {
+        fmax = v;
         kk = i;
       }
+    }
+    zero = zero || fmax == 0.0;
     if (kk != k) {
+#pragma unroll
       for (int j = k; j < NS; j++) {
         double t = a[k * NS + j];
         a[k * NS + j] = a[kk * NS + j];
         a[kk * NS + j] = t;
       }
-      double t = b[k];
-      b[k] = b[kk];
-      b[kk] = t;
+#pragma unroll
+      for (int i = k + 1; i < NS; i++)
+        if (i == kk) {
+          double t = b[k];
+          b[k] = b[i];
+          b[i] = t;
+        }
     }
+    double piv[NS];
+#pragma unroll
+    for (int j = k; j < NS; j++) piv[j] = a[k * NS + j];
+#pragma unroll
     for (int i = k + 1; i < NS; i++) {
-      double f = -a[i * NS + k] / a[k * NS + k];
-      for (int j = k; j < NS; j++) a[i * NS + j] = a[i * NS + j] + f * a[k * NS + j];
+      double f = -a[i * NS + k] / piv[k];
+#pragma unroll
+      for (int j = k; j < NS; j++) a[i * NS + j] = a[i * NS + j] + f * piv[j];
       b[i] = b[i] + f * b[k];
+      asm volatile("" ::: "memory");  // one row's loads at a time
     }
   }
-  x[NS - 1] = b[NS - 1] / a[(NS - 1) * NS + NS - 1];
+  const double last = a[(NS - 1) * NS + NS - 1];
+  zero = zero || last == 0.0;
+  x[NS - 1] = b[NS - 1] / last;
+#pragma unroll
   for (int i = NS - 2; i >= 0; i--) {
     double s = b[i];
+#pragma unroll
     for (int j = i + 1; j < NS; j++) s = s - a[i * NS + j] * x[j];
     x[i] = s / a[i * NS + i];
   }
+  return zero;
 }
 
 template <int NS>
@@ -178,11 +247,13 @@ __device__ __forceinline__ double update_et(const double* di, const double* dn, 
   return E;
 }
 
-// chemical_timeAdv (CHEM_reactions.f90:374-390) for one reactor
-template <int NS>
-__device__ void chem_step(double* di, double& E, double dt, int* nfail) {
+// chemical_timeAdv (CHEM_reactions.f90:374-390) for one reactor; returns true when the implicit
+// step met a zero pivot
+template <int NS, int STRIDE>
+__device__ bool chem_step(double* di, double& E, double dt, int* nfail, Slab<STRIDE> sA) {
   double ci[NS], ri[NS], dn[NS];
   const int mode = cC.timeadv;
+  bool zero = false;
   if (mode == 1) {
     double T = dev_T<NS>(di, E, nfail);
 #pragma unroll
@@ -216,6 +287,7 @@ __device__ void chem_step(double* di, double& E, double dt, int* nfail) {
     double d0[NS];
 #pragma unroll
     for (int i = 0; i < NS; i++) d0[i] = di[i];
+#pragma unroll
     for (int krk = 0; krk < 3; krk++) {
       double T = dev_T<NS>(di, E, nfail);
 #pragma unroll
@@ -227,31 +299,47 @@ __device__ void chem_step(double* di, double& E, double dt, int* nfail) {
 #pragma unroll
       for (int i = 0; i < NS; i++) di[i] = dn[i];
     }
-  } else {  // -1: linearised backward Euler
-    double Ar[NS * NS], rhs[NS], dd[NS];
+  } else {  // -1: linearised backward Euler, (I - J (M_i / M_j) dt) dd = r M 1e6 dt
+    double rhs[NS], dd[NS];
     double T = dev_T<NS>(di, E, nfail);
 #pragma unroll
     for (int i = 0; i < NS; i++) ci[i] = di[i] / cC.Mi[i] * 1.0e-6;
-    reaction_rate_matrix<NS>(ci, ri, Ar, T);
-    for (int j = 0; j < NS; j++)
-      for (int i = 0; i < NS; i++) {
-        double a = (i == j) ? 1.0 : 0.0;
-        Ar[i * NS + j] = a - Ar[i * NS + j] * cC.Mi[i] / cC.Mi[j] * dt;
+    reaction_rate_matrix<NS, STRIDE>(ci, ri, sA, T);
+#pragma unroll
+    for (int i = 0; i < NS; i++) {
+#pragma unroll
+      for (int j = 0; j < NS; j++) {
+        const double a = (i == j) ? 1.0 : 0.0;
+        sA[i * NS + j] = a - sA[i * NS + j] * cC.mratio[i][j] * dt;
       }
+      asm volatile("" ::: "memory");
+    }
 #pragma unroll
     for (int i = 0; i < NS; i++) rhs[i] = ri[i] * cC.Mi[i] * 1.0e6 * dt;
-    gauss<NS>(Ar, rhs, dd);
+    zero = gauss<NS, STRIDE>(sA, rhs, dd);
 #pragma unroll
     for (int i = 0; i < NS; i++) dn[i] = di[i] + dd[i];
     E = update_et<NS>(di, dn, E);
 #pragma unroll
     for (int i = 0; i < NS; i++) di[i] = dn[i];
   }
+  return zero;
+}
+
+// a reactor's result is an error when a pivot was zero or a density or the energy is not finite
+template <int NS>
+__device__ __forceinline__ void chem_check(const double* di, double E, bool zero, int* nfail) {
+  bool bad = zero || !isfinite(E);
+#pragma unroll
+  for (int m = 0; m < NS; m++) bad = bad || !isfinite(di[m]);
+  if (bad && nfail) atomicAdd(nfail + 1, 1);
 }
 
 template <int NS>
-__global__ void __launch_bounds__(128, OCFD_CHEM_MINB) k_chem_cells(double* f, double* Et, double* T, double* p, double* di,
-                                                    double dt2, int nsub, int* nfail) {
+__global__ void __launch_bounds__(OCFD_CHEM_TPB, OCFD_CHEM_MINB) k_chem_cells(double* f, double* Et, double* T,
+                                                                             double* p, double* di, double dt2,
+                                                                             int nsub, int* nfail) {
+  __shared__ double sA[NS * NS * OCFD_CHEM_TPB];
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= cC.N) return;
   int i = t % cC.nx + 1, j = (t / cC.nx) % cC.ny + 1, k = t / cC.nx / cC.ny + 1;
@@ -261,11 +349,14 @@ __global__ void __launch_bounds__(128, OCFD_CHEM_MINB) k_chem_cells(double* f, d
   for (int m = 0; m < NS; m++) d1[m] = di[(size_t)m * cC.H + q];
   double e = Et[q];
   double f5 = f[4 * cC.N + t];
+  bool zero = false;
+  const Slab<OCFD_CHEM_TPB> slab{sA + threadIdx.x};
   for (int s = 0; s < nsub; s++) {
     double e0 = e;
-    chem_step<NS>(d1, e, dt2, nfail);
+    zero = chem_step<NS, OCFD_CHEM_TPB>(d1, e, dt2, nfail, slab) || zero;
     f5 = f5 + (e - e0);
   }
+  chem_check<NS>(d1, e, zero, nfail);
 #pragma unroll
   for (int m = 0; m < NS; m++) di[(size_t)m * cC.H + q] = d1[m];
   Et[q] = e;
@@ -302,9 +393,13 @@ static __global__ void k_nsub_scatter(int n, const int* nsub, int* cursor, int n
 }
 
 template <int NS>
-__global__ void __launch_bounds__(128, OCFD_CHEM_MINB) k_chem_batch(int n, double* di, double* e, const double* dt, const int* nsub,
-                                                    const int* perm, int* counter, int* nfail) {
+__global__ void __launch_bounds__(OCFD_CHEM_TPB, OCFD_CHEM_MINB) k_chem_batch(int n, double* di, double* e,
+                                                                             const double* dt, const int* nsub,
+                                                                             const int* perm, int* counter,
+                                                                             int* nfail) {
+  __shared__ double sA[NS * NS * OCFD_CHEM_TPB];
   const int lane = threadIdx.x & 31;
+  const Slab<OCFD_CHEM_TPB> slab{sA + threadIdx.x};
   for (;;) {
     int base = 0;
     if (lane == 0) base = atomicAdd(counter, 32);
@@ -319,7 +414,9 @@ __global__ void __launch_bounds__(128, OCFD_CHEM_MINB) k_chem_batch(int n, doubl
 #pragma unroll
       for (int m = 0; m < NS; m++) d1[m] = di[(size_t)r * NS + m];
       double ee = e[r];
-      for (int s = 0; s < ks; s++) chem_step<NS>(d1, ee, dt2, nfail);
+      bool zero = false;
+      for (int s = 0; s < ks; s++) zero = chem_step<NS, OCFD_CHEM_TPB>(d1, ee, dt2, nfail, slab) || zero;
+      chem_check<NS>(d1, ee, zero, nfail);
 #pragma unroll
       for (int m = 0; m < NS; m++) di[(size_t)r * NS + m] = d1[m];
       e[r] = ee;

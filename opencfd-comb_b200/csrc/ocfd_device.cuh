@@ -37,6 +37,7 @@ struct DevConst {
   double tct[OCFD_NTCT_MAX], tct_max;
   double Mi[OCFD_MAX_SPEC], Ri[OCFD_MAX_SPEC];
   double cf[OCFD_MAX_SPEC][OCFD_NTCT_MAX][8];  // A,B,C,D,E,F,G,Ect
+  double mratio[OCFD_MAX_SPEC][OCFD_MAX_SPEC];  // Mi(i) / Mi(j), for the implicit-Euler matrix
   // transport
   int flag_vis, flag_cond, flag_diff;
   double amu0, pr, sc;
@@ -291,7 +292,27 @@ __device__ __forceinline__ double dev_Cp(double d, const double* di, double T) {
   double t = T <= cC.tct_max ? T : cC.tct_max;
   return (A1 + B1 * t + C1 * q2(t) + D1 * q3(t) + E1 * q4(t)) / d;
 }
-// T from internal energy; Newton (tol 1e-3 K, at most 31 iterations) for the fitted gas
+// the six energy sums of comput_T_rgas for fit range j (CHEM_thermdyn.f90:333-345), species in
+// order, so a range's sums are the same numbers whenever they are formed
+template <int NS>
+__device__ __forceinline__ void e_sums(const double* di, int j, double& a, double& b, double& c, double& d, double& e,
+                                       double& g) {
+  a = 0; b = 0; c = 0; d = 0; e = 0; g = 0;
+#pragma unroll
+  for (int k = 0; k < NS; k++) {
+    const double* cf = cC.cf[k][j];
+    double R1 = cC.Ri[k];
+    a = a + (cf[0] - 1.0) * R1 * di[k];
+    b = b + cf[1] * R1 * di[k];
+    c = c + cf[2] * R1 * di[k];
+    d = d + cf[3] * R1 * di[k];
+    e = e + cf[4] * R1 * di[k];
+    g = g + cf[7] * R1 * di[k];
+  }
+}
+// T from internal energy; Newton (tol 1e-3 K, at most 31 iterations) for the fitted gas. The
+// reference forms the sums of every fit range first; here the sums of the range the iterate is
+// in are formed when it changes (the same values), so nothing is indexed at run time.
 template <int NS>
 __device__ __forceinline__ double dev_T(const double* di, double Ein, int* nfail) {
   if (cC.realgas == 0) {
@@ -300,39 +321,27 @@ __device__ __forceinline__ double dev_T(const double* di, double Ein, int* nfail
     for (int k = 0; k < NS; k++) rcv = rcv + 2.5 * cC.Ri[k] * di[k];
     return Ein / rcv;
   }
-  double A1[OCFD_NTCT_MAX], B1[OCFD_NTCT_MAX], C1[OCFD_NTCT_MAX], D1[OCFD_NTCT_MAX], E1[OCFD_NTCT_MAX],
-      Ec[OCFD_NTCT_MAX];
-  const int nt = cC.n_tct;
-  for (int j = 0; j < nt; j++) {
-    double a = 0, b = 0, c = 0, d = 0, e = 0, g = 0;
-#pragma unroll
-    for (int k = 0; k < NS; k++) {
-      const double* cf = cC.cf[k][j];
-      double R1 = cC.Ri[k];
-      a = a + (cf[0] - 1.0) * R1 * di[k];
-      b = b + cf[1] * R1 * di[k];
-      c = c + cf[2] * R1 * di[k];
-      d = d + cf[3] * R1 * di[k];
-      e = e + cf[4] * R1 * di[k];
-      g = g + cf[7] * R1 * di[k];
-    }
-    A1[j] = a; B1[j] = b; C1[j] = c; D1[j] = d; E1[j] = e; Ec[j] = g;
-  }
-  double T1 = Ein / A1[0], T2 = T1;
+  double A1, B1, C1, D1, E1, Ec;
+  e_sums<NS>(di, 0, A1, B1, C1, D1, E1, Ec);
+  int jcur = 0;
+  double T1 = Ein / A1, T2 = T1;
   int ks = 0;
   bool conv = false;
   while (ks <= 30) {
     int jc = trange(T1);
+    if (jc != jcur) {
+      e_sums<NS>(di, jc, A1, B1, C1, D1, E1, Ec);
+      jcur = jc;
+    }
     double Et1, Ex;
     if (T1 <= cC.tct_max) {
-      Et1 = A1[jc] * T1 + B1[jc] * q2(T1) / 2.0 + C1[jc] * q3(T1) / 3.0 + D1[jc] * q4(T1) / 4.0 +
-            E1[jc] * q5(T1) / 5.0 + Ec[jc];
-      Ex = A1[jc] + B1[jc] * T1 + C1[jc] * q2(T1) + D1[jc] * q3(T1) + E1[jc] * q4(T1);
+      Et1 = A1 * T1 + B1 * q2(T1) / 2.0 + C1 * q3(T1) / 3.0 + D1 * q4(T1) / 4.0 + E1 * q5(T1) / 5.0 + Ec;
+      Ex = A1 + B1 * T1 + C1 * q2(T1) + D1 * q3(T1) + E1 * q4(T1);
     } else {
       double tm = cC.tct_max;
-      Ex = A1[jc] + B1[jc] * tm + C1[jc] * q2(tm) + D1[jc] * q3(tm) + E1[jc] * q4(tm);
-      Et1 = A1[jc] * tm + B1[jc] * q2(tm) / 2.0 + C1[jc] * q3(tm) / 3.0 + D1[jc] * q4(tm) / 4.0 +
-            E1[jc] * q5(tm) / 5.0 + Ec[jc] + Ex * (T1 - tm);
+      Ex = A1 + B1 * tm + C1 * q2(tm) + D1 * q3(tm) + E1 * q4(tm);
+      Et1 = A1 * tm + B1 * q2(tm) / 2.0 + C1 * q3(tm) / 3.0 + D1 * q4(tm) / 4.0 + E1 * q5(tm) / 5.0 + Ec +
+            Ex * (T1 - tm);
     }
     T2 = T1 - (Et1 - Ein) / Ex;
     ks = ks + 1;
@@ -370,8 +379,8 @@ __device__ __forceinline__ double dev_hi(int k, double T) {
           cpm * (T - tm)) *
          cC.Ri[k];
 }
-__device__ __forceinline__ double dev_gibbs(int k, double T, double logT) {
-  int jc = trange(T);
+// comput_gibbs (CHEM_thermdyn.f90:296-319) of species k in fit range jc = trange(T)
+__device__ __forceinline__ double dev_gibbs_jc(int k, int jc, double T, double logT) {
   const double* c = cC.cf[k][jc];
   if (T <= cC.tct_max)
     return c[0] * (1.0 - logT) * T - c[1] * q2(T) / 2.0 - c[2] * q3(T) / 6.0 - c[3] * q4(T) / 12.0 -
@@ -382,6 +391,7 @@ __device__ __forceinline__ double dev_gibbs(int k, double T, double logT) {
   double sm = c[0] * log(tm) + c[1] * tm + c[2] * q2(tm) / 2.0 + c[3] * q3(tm) / 3.0 + c[4] * q4(tm) / 4.0 + c[6];
   return hm + cpm * (T - tm) - T * (sm + cpm * log(T / tm));
 }
+__device__ __forceinline__ double dev_gibbs(int k, double T, double logT) { return dev_gibbs_jc(k, trange(T), T, logT); }
 
 // ---------------------------------------------------------------- transport (TRANSPORT_modules.f90)
 template <int NS>

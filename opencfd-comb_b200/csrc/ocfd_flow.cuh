@@ -22,7 +22,8 @@ struct DevStatus {
   int neg_list[16];       // their interior linear indices (first 16)
   int error;              // OCFD_ERR_* raised on the device
   int nan_count;
-  int newton_fail;
+  int newton_fail;        // Newton T(E) non-converged (chemistry and primitives)
+  int chem_bad;           // chemistry: zero Gauss pivot or non-finite result (follows newton_fail)
   unsigned long long neg_total;
 };
 

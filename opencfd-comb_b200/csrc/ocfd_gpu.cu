@@ -60,10 +60,13 @@ struct CudaError : std::runtime_error {
 #define LAUNCH_CHECK() CK(cudaGetLastError())
 
 // kernel classes for event timing
+// (species work of N_SPEC > 1, by kernel family: transport = k_transport, species_flux = the
+// scalar k_flux sweeps, species_visc = k_ci + k_scal_ev + k_scal_div, species_rk = k_scal_rk)
 enum KClass { KC_FLUX_X = 0, KC_FLUX_Y, KC_FLUX_Z, KC_VISC_EV, KC_VISC_DIV, KC_RK_PRIMS, KC_EXCH, KC_BC, KC_SENSOR,
-              KC_SPECIES, KC_CHEM, KC_OTHER, KC_NUM };
+              KC_TRANSPORT, KC_SPECIES_FLUX, KC_SPECIES_VISC, KC_SPECIES_RK, KC_CHEM, KC_OTHER, KC_NUM };
 const char* kc_names[KC_NUM] = {"flux_x", "flux_y", "flux_z", "visc_ev", "visc_div", "rk_prims", "exchange",
-                                "bc", "sensor", "species", "chem", "other"};
+                                "bc", "sensor", "transport", "species_flux", "species_visc", "species_rk",
+                                "chem", "other"};
 
 struct Lib {
   ocfd_params P{};
@@ -132,6 +135,7 @@ struct Lib {
   double *b_di = nullptr, *b_e = nullptr, *b_dt = nullptr;
   int *b_nsub = nullptr, *b_perm = nullptr, *b_hist = nullptr, *b_counter = nullptr, *b_nfail = nullptr;
   size_t b_cap = 0;
+  int b_last[2] = {0, 0};  // the last batch call's Newton non-convergences and bad reactors
   // profiling
   bool prof = false;
   double kc_ms[KC_NUM] = {};
@@ -224,7 +228,7 @@ void exchange_v(const std::vector<double*>& fields, int dirmask) {
 // ---- flux dispatch (kernels compiled in ocfd_flux_{x,y,z}.cu) ----
 // group = 0: the flow fluxes; else a scalar sweep of every species, group species per block
 void launch_flux(int dir, const FluxArgs& a, int group = 0, int ngroups = 1) {
-  KTimer t(group ? KC_SPECIES : KC_FLUX_X + dir);
+  KTimer t(group ? KC_SPECIES_FLUX : KC_FLUX_X + dir);
   const ocfd_params& P = L->P;
   const bool ch = P.if_scheme_character == 1;
   const int ts = (group == 0 && !ch) ? L->flux_ts[dir] : 0;
@@ -504,7 +508,7 @@ void stage_t(int krk, double dt1) {
     LAUNCH_CHECK();
   }
   if (NS > 1) {
-    KTimer t(KC_SPECIES);
+    KTimer t(KC_TRANSPORT);
     k_transport<NS><<<nblk(N, 32), dim3(32, NS), 0, L->st>>>(L->d, L->T, L->p, L->di, L->amu, L->amk, L->amd);
     LAUNCH_CHECK();
   }
@@ -528,7 +532,7 @@ void stage_t(int krk, double dt1) {
     for (int dd = 0; dd < 3; dd++) launch_flux(dd, fa, grp, NS / grp);
     if (L->P.if_viscous == 1) {
       {
-        KTimer t(KC_SPECIES);
+        KTimer t(KC_SPECIES_VISC);
         k_ci<<<dim3(nblk(H, 256), NS), 256, 0, L->st>>>(L->di, L->d, L->ci, H);
         LAUNCH_CHECK();
         if (L->sep) k_scal_ev<NS, true><<<nblk(N, 32), dim3(32, NS), 0, L->st>>>(L->ci, L->d, L->T, L->amd, L->qp[0], L->qp[1], L->qp[2], L->se[0], L->se[1], L->se[2], L->geo);
@@ -540,13 +544,13 @@ void stage_t(int krk, double dt1) {
         for (int m = 0; m < NS; m++) fl.push_back(L->se[dd] + (size_t)m * H);
         exchange_v(fl, 1 << dd);
       }
-      KTimer t(KC_SPECIES);
+      KTimer t(KC_SPECIES_VISC);
       if (L->sep) k_scal_div<NS, true><<<nblk(N, 32), dim3(32, NS), 0, L->st>>>(L->se[0], L->se[1], L->se[2], L->dus, L->geo);
       else k_scal_div<NS, false><<<nblk(N, 32), dim3(32, NS), 0, L->st>>>(L->se[0], L->se[1], L->se[2], L->dus, L->geo);
       LAUNCH_CHECK();
     }
     {
-      KTimer t(KC_SPECIES);
+      KTimer t(KC_SPECIES_RK);
       k_scal_rk<<<dim3(nblk(N, 256), NS), 256, 0, L->st>>>(krk, dt1, L->dus, L->din, L->di);
       LAUNCH_CHECK();
     }
@@ -881,10 +885,26 @@ int check_status() {
     g_err = e == OCFD_ERR_NEGATIVE_ET ? "Number of Negative Temperature Points > Limit (10)" : "device error";
     return e;
   }
+  if (L->shost->chem_bad) {
+    const int nb = L->shost->chem_bad;
+    CK(cudaMemsetAsync(&L->sdev->chem_bad, 0, sizeof(int), L->st));
+    g_err = "chemistry: " + std::to_string(nb) + " cell(s) with a zero Gauss pivot or a non-finite result";
+    return OCFD_ERR_CHEM;
+  }
   if (L->shost->nan_count) {
     CK(cudaMemsetAsync(&L->sdev->nan_count, 0, sizeof(int), L->st));
     g_err = "NaN in the internal energy";
     return OCFD_ERR_NAN;
+  }
+  return 0;
+}
+
+// outcome of a batched chemistry call from its two error words (Newton, bad reactors)
+int batch_result() {
+  if (L->b_last[1] > 0) {
+    g_err = "chemistry: " + std::to_string(L->b_last[1]) +
+            " reactor(s) with a zero Gauss pivot or a non-finite result (their values are returned as computed)";
+    return OCFD_ERR_CHEM;
   }
   return 0;
 }
@@ -927,6 +947,8 @@ void fill_thermo(DevConst& c, const ocfd_thermo* th, int realgas) {
       c.cf[k][j][7] = ect;
     }
   }
+  for (int i = 0; i < th->n_spec; i++)
+    for (int j = 0; j < th->n_spec; j++) c.mratio[i][j] = th->mi[i] / th->mi[j];
 }
 void fill_kin(DevConst& c, const ocfd_kinetics* kin) {
   c.nreac = kin->n_reac;
@@ -1951,7 +1973,9 @@ int ocfd_gpu_chem_setup(const ocfd_thermo* th, const ocfd_kinetics* kin, int rea
 int ocfd_gpu_chem_batch_device(int n, double* d_di, double* d_e, const double* d_dt, const int* d_nsub) {
   return guarded([&]() -> int {
     if (!L || !L->have_kin) { g_err = "ocfd_gpu_init or ocfd_gpu_chem_setup with a mechanism first"; return OCFD_ERR_STATE; }
-    if (n <= 0) return 0;
+    if (n < 0) { g_err = "ocfd_gpu_chem_batch_device: n = " + std::to_string(n) + " must be >= 0"; return OCFD_ERR_PARAM; }
+    L->b_last[0] = L->b_last[1] = 0;
+    if (n == 0) return 0;
     const int nbins = 1024;
     if ((size_t)n > L->b_cap) {
       if (L->b_di) cudaFree(L->b_di);
@@ -1979,9 +2003,10 @@ int ocfd_gpu_chem_batch_device(int n, double* d_di, double* d_e, const double* d
       launch_chem_batch(L->NS, sms, n, d_di, d_e, d_dt, d_nsub, L->b_perm, L->b_counter, L->b_nfail, L->st);
       LAUNCH_CHECK();
     }
+    CK(cudaMemcpyAsync(L->b_last, L->b_nfail, 2 * sizeof(int), cudaMemcpyDeviceToHost, L->st));
     CK(cudaStreamSynchronize(L->st));
     prof_collect();
-    return 0;
+    return batch_result();
   });
 }
 
@@ -2026,11 +2051,16 @@ extern "C" {
 int ocfd_gpu_chem_batch_noalloc(int n, double* d_di, double* d_e, const double* d_dt, const int* d_nsub) {
   return guarded([&]() -> int {
     if (!L || !L->have_kin) { g_err = "ocfd_gpu_init or ocfd_gpu_chem_setup with a mechanism first"; return OCFD_ERR_STATE; }
-    if (n < 0 || n > OCFD_NOALLOC_MAX_REACTORS) {
+    if (n < 0) {
+      g_err = "ocfd_gpu_chem_batch_noalloc: n = " + std::to_string(n) + " must be >= 0";
+      return OCFD_ERR_PARAM;
+    }
+    if (n > OCFD_NOALLOC_MAX_REACTORS) {
       g_err = "ocfd_gpu_chem_batch_noalloc: n = " + std::to_string(n) + " exceeds the fixed scratch of " +
               std::to_string(OCFD_NOALLOC_MAX_REACTORS) + " reactors (use ocfd_gpu_chem_batch_device)";
       return OCFD_ERR_PARAM;
     }
+    L->b_last[0] = L->b_last[1] = 0;
     if (n == 0) return 0;
     int* perm = noalloc_scratch();
     int* hist = perm + OCFD_NOALLOC_MAX_REACTORS;
@@ -2053,16 +2083,19 @@ int ocfd_gpu_chem_batch_noalloc(int n, double* d_di, double* d_e, const double* 
       launch_chem_batch(L->NS, sms, n, d_di, d_e, d_dt, d_nsub, perm, counter, nfail, L->st);
       LAUNCH_CHECK();
     }
+    CK(cudaMemcpyAsync(L->b_last, nfail, 2 * sizeof(int), cudaMemcpyDeviceToHost, L->st));
     CK(cudaStreamSynchronize(L->st));
     prof_collect();
-    return 0;
+    return batch_result();
   });
 }
 
 int ocfd_gpu_chem_batch(int n, double* di, double* e, const double* dt, const int* nsub) {
   return guarded([&]() -> int {
     if (!L || !L->have_kin) { g_err = "ocfd_gpu_init or ocfd_gpu_chem_setup with a mechanism first"; return OCFD_ERR_STATE; }
-    if (n <= 0) return 0;
+    if (n < 0) { g_err = "ocfd_gpu_chem_batch: n = " + std::to_string(n) + " must be >= 0"; return OCFD_ERR_PARAM; }
+    L->b_last[0] = L->b_last[1] = 0;
+    if (n == 0) return 0;
     const int NS = L->NS;
     double *ddi, *de, *ddt;
     int* dns = nullptr;
@@ -2075,7 +2108,7 @@ int ocfd_gpu_chem_batch(int n, double* di, double* e, const double* dt, const in
     CK(cudaMemcpyAsync(ddt, dt, sizeof(double) * n, cudaMemcpyHostToDevice, L->st));
     if (nsub) CK(cudaMemcpyAsync(dns, nsub, sizeof(int) * n, cudaMemcpyHostToDevice, L->st));
     int rc = ocfd_gpu_chem_batch_device(n, ddi, de, ddt, dns);
-    if (rc) return rc;
+    if (rc != 0 && rc != OCFD_ERR_CHEM) return rc;
     CK(cudaMemcpyAsync(di, ddi, sizeof(double) * (size_t)n * NS, cudaMemcpyDeviceToHost, L->st));
     CK(cudaMemcpyAsync(e, de, sizeof(double) * n, cudaMemcpyDeviceToHost, L->st));
     CK(cudaFreeAsync(ddi, L->st));
@@ -2083,8 +2116,17 @@ int ocfd_gpu_chem_batch(int n, double* di, double* e, const double* dt, const in
     CK(cudaFreeAsync(ddt, L->st));
     if (dns) CK(cudaFreeAsync(dns, L->st));
     CK(cudaStreamSynchronize(L->st));
-    return 0;
+    if (rc) g_err = "chemistry: " + std::to_string(L->b_last[1]) +
+                    " reactor(s) with a zero Gauss pivot or a non-finite result (their values are returned as computed)";
+    return rc;
   });
+}
+
+int ocfd_gpu_chem_batch_status(long long* newton_fail, long long* bad) {
+  if (!L) return OCFD_ERR_STATE;
+  if (newton_fail) *newton_fail = L->b_last[0];
+  if (bad) *bad = L->b_last[1];
+  return 0;
 }
 
 int ocfd_gpu_stats(long long* neg_et, long long* newton_fail) {

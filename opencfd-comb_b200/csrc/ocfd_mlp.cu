@@ -111,12 +111,17 @@ __global__ void __launch_bounds__(THREADS) k_gemm_bf16(GemmArgs g) {
   tc::fence_after();
   const uint32_t tmem = *tslot;
   constexpr uint32_t idesc = tc::idesc_bf16(BM, BN);
+  // Every wait is bounded; the block agrees on its outcome (__syncthreads_and) before it acts on
+  // it, so a thread whose wait ran out never leaves the others at a barrier it skips.
   bool ok = true;
+  int last = -1;  // K block of the last commit
   const int nkb = (g.K + BK - 1) / BK;
-  for (int kb = 0; kb < nkb && ok; kb++) {
+  for (int kb = 0; kb < nkb; kb++) {
     const int buf = kb & 1;
-    if (kb >= 2) ok = tc::mbar_wait(&bar[buf], (uint32_t)(((kb - 2) >> 1) & 1), WAIT_LIMIT);
-    if (!ok) break;
+    if (kb >= 2) {
+      ok = __syncthreads_and(tc::mbar_wait(&bar[buf], (uint32_t)(((kb - 2) >> 1) & 1), WAIT_LIMIT) ? 1 : 0) != 0;
+      if (!ok) break;
+    }
     uint8_t* sA = sm + buf * SM::STAGE;
     uint8_t* sB = sA + SM::A_BYTES;
     stage<BM>(sA, g.A, g.sam, g.sak, m0, g.M, kb * BK, g.K, va);
@@ -134,10 +139,14 @@ __global__ void __launch_bounds__(THREADS) k_gemm_bf16(GemmArgs g) {
       }
       tc::mma_commit(tc::smem_u32(&bar[buf]));
     }
+    last = kb;
   }
   // the last commit covers every MMA issued before it
-  if (ok) ok = tc::mbar_wait(&bar[(nkb - 1) & 1], (uint32_t)(((nkb - 1) >> 1) & 1), WAIT_LIMIT);
+  if (ok)
+    ok = __syncthreads_and(tc::mbar_wait(&bar[(nkb - 1) & 1], (uint32_t)(((nkb - 1) >> 1) & 1), WAIT_LIMIT) ? 1 : 0) != 0;
   if (!ok) {
+    // bounded drain of the MMAs still in flight before the accumulator is freed
+    if (tid == 0 && last >= 0) tc::mbar_wait(&bar[last & 1], (uint32_t)((last >> 1) & 1), WAIT_LIMIT);
     if (lane == 0) atomicExch(g.err, 1);
   } else {
     tc::fence_after();

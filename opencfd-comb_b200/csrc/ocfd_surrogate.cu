@@ -533,9 +533,10 @@ __global__ void k_cell_post(int c0, int rows, double* __restrict__ f, double* __
 // Chemical_time_advance + comput_T_P for the listed cells (k_chem_cells on a cell list whose length
 // is read on the device)
 template <int NS>
-__global__ void __launch_bounds__(128) k_chem_cells_list(const int* __restrict__ list, const int* __restrict__ count,
-                                                         double* f, double* Et, double* T, double* p, double* di,
-                                                         double dt2, int nsub, int* nfail) {
+__global__ void __launch_bounds__(OCFD_CHEM_TPB, OCFD_CHEM_MINB) k_chem_cells_list(
+    const int* __restrict__ list, const int* __restrict__ count, double* f, double* Et, double* T, double* p,
+    double* di, double dt2, int nsub, int* nfail) {
+  __shared__ double sA[NS * NS * OCFD_CHEM_TPB];
   const int idx = blockIdx.x * blockDim.x + threadIdx.x;
   if (idx >= *count) return;
   const int t = list[idx];
@@ -546,11 +547,14 @@ __global__ void __launch_bounds__(128) k_chem_cells_list(const int* __restrict__
   for (int m = 0; m < NS; m++) d1[m] = di[(size_t)m * cC.H + q];
   double e = Et[q];
   double f5 = f[4 * cC.N + t];
+  bool zero = false;
+  const Slab<OCFD_CHEM_TPB> slab{sA + threadIdx.x};
   for (int s = 0; s < nsub; s++) {
     double e0 = e;
-    chem_step<NS>(d1, e, dt2, nfail);
+    zero = chem_step<NS, OCFD_CHEM_TPB>(d1, e, dt2, nfail, slab) || zero;
     f5 = f5 + (e - e0);
   }
+  chem_check<NS>(d1, e, zero, nfail);
 #pragma unroll
   for (int m = 0; m < NS; m++) di[(size_t)m * cC.H + q] = d1[m];
   Et[q] = e;
@@ -588,7 +592,7 @@ void cells_chem_t(double* f, double* Et, double* T, double* p, double* di, doubl
     k_cell_post<NS><<<nb(rows, 128), 128, 0, st>>>((int)c0, rows, f, Et, T, p, di, CS.T0, CS.raw, CS.out, S.d_norm,
                                                   S.d_proj, CS.tol, CS.list, CS.count, nfail);
   }
-  k_chem_cells_list<NS><<<nb(N, 128), 128, 0, st>>>(CS.list, CS.count, f, Et, T, p, di, dt2, nsub, nfail);
+  k_chem_cells_list<NS><<<nb(N, OCFD_CHEM_TPB), OCFD_CHEM_TPB, 0, st>>>(CS.list, CS.count, f, Et, T, p, di, dt2, nsub, nfail);
 }
 
 // mode 1: allocate the chunk buffers for N cells (called outside any stream capture)

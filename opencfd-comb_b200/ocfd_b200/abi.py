@@ -18,6 +18,7 @@ ERR_NEGATIVE_ET = -4
 ERR_STATE = -5
 ERR_TIMEOUT = -6
 ERR_UNSUPPORTED = -7
+ERR_CHEM = -8
 
 SCHEME_WENO5, SCHEME_WENO7, SCHEME_OMP6, SCHEME_UD7L = 1, 2, 3, 4
 SCHEME_CD6, SCHEME_CD8, SCHEME_HYBRID = 5, 6, 10
@@ -155,6 +156,7 @@ GPU_SIGNATURES = {
     "ocfd_gpu_pinned_free": (I, [C.c_void_p]),
     "ocfd_gpu_step_launches": (I, []),
     "ocfd_gpu_chem_batch_noalloc": (I, [I, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "ocfd_gpu_chem_batch_status": (I, [C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)]),
     "ocfd_gpu_gemm_bf16": (I, [I, I, I, C.c_void_p, C.c_longlong, C.c_longlong, C.c_void_p, C.c_longlong,
                                C.c_longlong, C.c_void_p, C.c_longlong, C.c_void_p, I, I]),
     "ocfd_gpu_surrogate_init": (I, [C.c_uint]),

@@ -15,7 +15,13 @@ import numpy as np
 from . import abi
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIBPATH = os.path.join(HERE, "libocfd_gpu.so")
+# libocfd_gpu.so: --fmad=false build (every multiply and add rounded separately, bit-identical to
+# the CPU restatement where no transcendental enters); OCFD_B200_LIB=fma selects
+# libocfd_gpu_fma.so, the same sources with contracted multiply-adds
+VARIANT = os.environ.get("OCFD_B200_LIB", "exact")
+if VARIANT not in ("exact", "fma"):
+    raise ValueError("OCFD_B200_LIB must be 'exact' or 'fma'")
+LIBPATH = os.path.join(HERE, "libocfd_gpu_fma.so" if VARIANT == "fma" else "libocfd_gpu.so")
 
 _lib = None
 
@@ -31,7 +37,8 @@ def lib():
     global _lib
     if _lib is None:
         if not os.path.exists(LIBPATH):
-            raise OcfdError(abi.ERR_CUDA, "libocfd_gpu.so is not built (run make -C opencfd-comb_b200)")
+            raise OcfdError(abi.ERR_CUDA, "%s is not built (run make -C opencfd-comb_b200%s)" %
+                            (os.path.basename(LIBPATH), " fma" if VARIANT == "fma" else ""))
         L = C.CDLL(LIBPATH)
         for name, (res, args) in abi.GPU_SIGNATURES.items():
             fn = getattr(L, name)

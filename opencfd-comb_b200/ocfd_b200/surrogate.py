@@ -94,6 +94,12 @@ class Surrogate:
             g.step(case.dt, 1, case.nsub)
         f, di, prims = g.download_state()
         g.close()
+        return self.samples_from_state(case, di, prims, n_sample, seed)
+
+    def samples_from_state(self, case, di, prims, n_sample, seed=0):
+        """n_sample cells (seeded choice without replacement) of a downloaded flow state (di and
+        the primitives as ocfd_gpu_download_state writes them) as reactors (densities, energy,
+        chemistry time, sub-steps)."""
         L4 = 4
         dii = di[:, L4:-L4, L4:-L4, L4:-L4].reshape(self.ns, -1).T
         E = prims[6][L4:-L4, L4:-L4, L4:-L4].reshape(-1)
