@@ -55,9 +55,16 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=5)
-    ap.add_argument("--sg-train", type=int, default=1 << 21, help="surrogate workload: training reactors")
-    ap.add_argument("--sg-epochs", type=int, default=20, help="surrogate workload: training epochs")
+    ap.add_argument("--sg-train", type=int, default=1 << 22,
+                    help="surrogate workload: C3 reactors drawn (two trajectory states each)")
+    ap.add_argument("--sg-jet-cells", type=int, default=1 << 21, help="surrogate workload: jet snapshot cells")
+    ap.add_argument("--sg-epochs", type=int, default=None,
+                    help="training epochs (default: 20 for the jet's training set, 6 for the surrogate workload)")
+    ap.add_argument("--sg-batch", type=int, default=4096, help="surrogate workload: training batch")
     ap.add_argument("--sg-tol", type=float, default=5.0, help="surrogate workload: gate tolerance on T (K)")
+    ap.add_argument("--const-v", action="store_true",
+                    help="reactors workload: the reference's constant-volume reactor instead of the configured "
+                         "constant-pressure one")
     ap.add_argument("--no-surrogate", action="store_true",
                     help="jet workload: plain FP64 chemistry only (no surrogate training or second run)")
     ap.add_argument("--total-steps", type=int, default=200,
@@ -236,18 +243,20 @@ RUNIT = "Mreactor-solves/s"
 def reactors_reference(a, pyoracle, cores):
     from ocfd_b200 import abi, cases
     n = 8192
+    cp = a.workload == "reactors" and not a.const_v
     names, th, kin, di, E, dt, nsub, T = cases.reactors(n=n, seed=1)
     for s in range(a.warmup):
-        pyoracle.chem_batch(th, kin, 1, abi.CHEM_IMPLICIT, di.copy(), E.copy(), dt, nsub)
+        pyoracle.chem_batch(th, kin, 1, abi.CHEM_IMPLICIT, di.copy(), E.copy(), dt, nsub, const_p=cp)
     t0 = time.perf_counter()
     for s in range(a.steps):
-        pyoracle.chem_batch(th, kin, 1, abi.CHEM_IMPLICIT, di.copy(), E.copy(), dt, nsub)
+        pyoracle.chem_batch(th, kin, 1, abi.CHEM_IMPLICIT, di.copy(), E.copy(), dt, nsub, const_p=cp)
     el = time.perf_counter() - t0
     val = n * a.steps / el / 1e6
     out = {"metric": RMETRIC, "value": val, "unit": RUNIT, "n_gpus": a.gpus, "steps": a.steps, "warmup": a.warmup,
            "ms_per_step": el * 1e3 / a.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
            "dtype": "f64", "data": "synthetic (seeded)", "impl": "reference",
-           "config": {"workload": "reactors-2^20-H2air-9sp-implicitEuler", "sample_reactors": n},
+           "config": {"workload": "reactors-%d-H2air-9sp-implicitEuler-%s" % (n, "constP" if cp else "constV"),
+                      "sample_of": "reactors-2^20-H2air-9sp-implicitEuler", "sample_reactors": n},
            "cpu_baseline": {"value": val, "unit": RUNIT, "cores": cores, "kind": "port",
                             "sample": "per step: %d reactors drawn like the 2^20 workload" % n},
            "e2e": {"value": val, "unit": RUNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -256,7 +265,8 @@ def reactors_reference(a, pyoracle, cores):
 
 
 def main_reactors(a):
-    """2^20 independent constant-volume H2-air reactors through the persistent work-queue kernel
+    """2^20 independent H2-air reactors at 1 atm (constant-pressure as configured, or the
+    reference's constant-volume reactor with --const-v) through the persistent work-queue kernel
     (ocfd_gpu_chem_batch_device); one step = one pass over all reactors."""
     import numpy as np
     import torch
@@ -265,7 +275,8 @@ def main_reactors(a):
     import ctypes as C
     n = 2 ** 20
     names, th, kin, di, E, dt, nsub, T = cases.reactors(n=n, seed=0)
-    solver.chem_setup(th, kin, 1, abi.CHEM_IMPLICIT)
+    cp = not a.const_v
+    solver.chem_setup(th, kin, 1, abi.CHEM_IMPLICIT, const_p=cp)
     dev = torch.device("cuda", 0)
     d_di0, d_e0 = torch.from_numpy(di).to(dev), torch.from_numpy(E).to(dev)
     d_dt, d_ns = torch.from_numpy(dt).to(dev), torch.from_numpy(nsub).to(dev)
@@ -313,7 +324,7 @@ def main_reactors(a):
         m = 8192
         _, _, _, sdi, sE, sdt, sns, _ = cases.reactors(n=m, seed=1)
         t0 = time.perf_counter()
-        pyoracle.chem_batch(th, kin, 1, abi.CHEM_IMPLICIT, sdi.copy(), sE.copy(), sdt, sns)
+        pyoracle.chem_batch(th, kin, 1, abi.CHEM_IMPLICIT, sdi.copy(), sE.copy(), sdt, sns, const_p=cp)
         el = time.perf_counter() - t0
         cpu = {"value": m / el / 1e6, "unit": RUNIT, "cores": cores, "kind": "port",
                "sample": "%d reactors drawn like the 2^20 workload" % m}
@@ -321,7 +332,9 @@ def main_reactors(a):
     out = {"metric": RMETRIC, "value": value, "unit": RUNIT, "n_gpus": 1, "steps": a.steps, "warmup": a.warmup,
            "ms_per_step": ms / a.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
            "dtype": "f64", "data": "synthetic (seeded)",
-           "config": {"workload": "reactors-2^20-H2air-9sp-implicitEuler", "reactors": n, "substeps_total": sub,
+           "config": {"workload": "reactors-2^20-H2air-9sp-implicitEuler-%s" % ("constP" if cp else "constV"),
+                      "reactor": "constant-pressure (p held at constant specific enthalpy after every sub-step)"
+                                 if cp else "constant-volume (the reference's)", "reactors": n, "substeps_total": sub,
                       "substeps_per_s": sub * a.steps / (ms * 1e-3),
                       "l2": "inputs re-copied from a pristine device copy before each pass"},
            "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": None, "clocks": clk.summary()}
@@ -335,8 +348,12 @@ MLP_FLOPS_PER_SAMPLE = 2 * (16 * 256 + 256 * 256 * 2 + 256 * 16)  # padded forwa
 
 
 def main_surrogate(a):
-    """Trains the surrogate on FP64-integrated reactors, then times the plain FP64 batch and the
-    gated surrogate on 2^20 held-out reactors (device-resident inputs restored before every pass)."""
+    """C4: the learned chemistry on its configured state set. 10 x 2^20 states (C3 reactors at two
+    points of their FP64 constant-pressure trajectory, 2^23 states, plus 2^21 cells of two FP64 jet
+    snapshots) are split 90/10 with a seeded permutation; the network is trained on the 90 % with
+    FP64-integrator targets, then the plain FP64 batch and the gated surrogate are timed on the 2^20
+    held-out states (device-resident inputs restored before every pass) and the surrogate's errors
+    against the FP64 integrator and its fallback fraction are taken on them."""
     import numpy as np
     import torch
     import ctypes as C
@@ -344,10 +361,17 @@ def main_surrogate(a):
     sg = surrogate.Surrogate()
     L = sg.L
     t0 = time.perf_counter()
-    hist = sg.train(n=a.sg_train, epochs=a.sg_epochs, batch=1024, lr=2e-3, seed=0)
-    train_s = time.perf_counter() - t0
+    ADI, AE, ADT, ANS, SRC = sg.c4_states(n_reactors=a.sg_train, jet_cells=a.sg_jet_cells, seed=0)
+    ntot = len(AE)
     n = 1 << 20
-    di, E, dt, nsub = sg.reactors(n, 4242)
+    tr, ho = sg.split(ntot, n, seed=0)
+    build_s = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    hist = sg.train_on([(ADI[tr], AE[tr], ADT[tr], ANS[tr])], epochs=a.sg_epochs, batch=a.sg_batch, lr=2e-3, seed=0)
+    train_s = time.perf_counter() - t0
+    di, E, dt, nsub = (np.ascontiguousarray(x[ho]) for x in (ADI, AE, ADT, ANS))
+    held_jet = int(SRC[ho].sum())
+    del ADI, AE, ADT, ANS
     dev = torch.device("cuda")
     p_di, p_e = torch.from_numpy(di).to(dev), torch.from_numpy(E).to(dev)
     d_dt, d_ns = torch.from_numpy(dt).to(dev), torch.from_numpy(nsub).to(dev)
@@ -393,7 +417,7 @@ def main_surrogate(a):
         ms_gated = timed(gated, k)
         profiler(False, a.profile_region)
         ms_net = timed(network, k)
-    acc = sg.evaluate(n=n, seed=4242, tol_T=a.sg_tol)
+    acc = sg.evaluate_on(di, E, dt, nsub, tol_T=a.sg_tol)
     peaks_file = os.path.join(ROOT, "MEASURED_PEAKS.json")
     bf16_peak = None
     if os.path.exists(peaks_file):
@@ -405,8 +429,16 @@ def main_surrogate(a):
     out = {"metric": SMETRIC, "value": n / (ms_gated * 1e-3) / 1e6, "unit": RUNIT, "n_gpus": 1, "steps": k,
            "warmup": a.warmup, "ms_per_step": ms_gated, "higher_is_better": True, "scaling": "weak",
            "vs_baseline": None, "dtype": "bf16 network + f64 fallback", "data": "synthetic (seeded)",
-           "config": {"workload": "reactors-2^20-H2air-9sp gated surrogate (MLP 12-256-256-256-10, GELU)",
-                      "train_reactors": a.sg_train, "epochs": a.sg_epochs, "train_seconds": train_s,
+           "config": {"workload": "surrogate-2^20-held-out-states-H2air-9sp (MLP 12-256-256-256-10, GELU)",
+                      "states": ntot, "train_states": len(tr), "held_out_states": n,
+                      "held_out_from_jet": held_jet, "held_out_from_reactors": n - held_jet,
+                      "state_set": "2 x %d C3 reactor states (draw, and after one FP64 constant-pressure "
+                                   "integration over dt) + %d cells of two FP64 jet snapshots (384x256x256, "
+                                   "steps 8 and 16); seeded 90/10 split" % (a.sg_train, a.sg_jet_cells),
+                      "targets": "FP64 implicit-Euler integrator (constant volume, the operator the surrogate "
+                                 "replaces) over each state's dt",
+                      "epochs": a.sg_epochs, "batch": a.sg_batch, "build_seconds": build_s,
+                      "train_seconds": train_s,
                       "loss_first_last": [float(hist[0]), float(hist[-1])], "tol_T_K": a.sg_tol},
            "plain_fp64": {"value": n / (ms_plain * 1e-3) / 1e6, "ms": ms_plain},
            "speedup_vs_plain": ms_plain / ms_gated,
@@ -900,6 +932,8 @@ def main_ours(a):
 
 if __name__ == "__main__":
     a = parse()
+    if a.sg_epochs is None:
+        a.sg_epochs = 6 if a.workload == "surrogate" else 20
     if a.impl == "reference":
         sys.exit(main_reference(a))
     if a.workload == "reactors":

@@ -224,6 +224,15 @@ int ocfd_gpu_chem_batch(int n, double* di, double* e, const double* dt, const in
 int ocfd_gpu_chem_batch_device(int n, double* d_di, double* d_e, const double* d_dt,
                                const int* d_nsub);
 
+/* Constant-pressure batched reactors (no counterpart in the reference, whose reactor is the flow
+ * solver's constant-volume cell, OCFD_Time_Adv.f90:174-193): on = 1 makes ocfd_gpu_chem_batch*
+ * hold each reactor's initial pressure at constant specific total enthalpy after every sub-step
+ * (mass fractions fixed, Newton on T, density rescaled to the pressure); on = 0 restores the
+ * reference's constant-volume reactor (default); on < 0 returns the setting. The flow solver's
+ * cells stay constant-volume either way, and ocfd_gpu_chem_batch_surrogate refuses constant-pressure
+ * batches (OCFD_ERR_UNSUPPORTED). */
+int ocfd_gpu_chem_constant_pressure(int on);
+
 /* The last batched chemistry call's counts: reactors whose Newton T(E) iteration did not converge
  * (comput_T_rgas, CHEM_thermdyn.f90:327-382, at most 31 iterations) and reactors reported by
  * OCFD_ERR_CHEM (zero pivot or non-finite result). Either pointer may be NULL. */

@@ -20,6 +20,7 @@
 // k_chem_batch : independent 0-D reactors as a persistent work queue. Reactors are visited in
 //                descending order of their sub-step count (counting sort on the device), so the
 //                32 reactors of a warp carry near-equal work and long reactors start first.
+//                Constant-volume (the reference's reactor) or, on request, constant-pressure.
 //
 // Error words (nfail points at two ints): nfail[0] counts Newton T(E) iterations that did not
 // converge (comput_T_rgas, CHEM_thermdyn.f90:327-382), nfail[1] reactors whose Gauss elimination
@@ -326,6 +327,52 @@ __device__ bool chem_step(double* di, double& E, double dt, int* nfail, Slab<STR
   return zero;
 }
 
+// Constant-pressure reactors (an extension for batched 0-D reactors; the reference's reactor and the
+// flow solver's cells are constant-volume, OCFD_Time_Adv.f90:174-193). A reactor keeps its initial
+// pressure p0 and specific total enthalpy h0 = (E + sum d_k R_k F_k + p) / rho (F_k the formation
+// term that update_Et books). After each constant-volume sub-step the mixture is brought back to
+// p0 at h0 with the mass fractions fixed: Newton on T for e(T, Y) + R T + sum Y_k R_k F_k = h0 (e
+// from comput_E with Y as densities, derivative the mass-specific Cp), stopped when |dT| <= 1e-10 T
+// (at most 50 iterations), then rho = p0 / (R T), d = Y rho, E = comput_E(d, T). The oracle applies
+// the identical operations.
+template <int NS>
+__device__ __forceinline__ void cp_reference(const double* di, double Et, double& h0, double& p0, int* nfail) {
+  const double T = dev_T<NS>(di, Et, nfail);
+  p0 = dev_P<NS>(di, T);
+  double rho = 0.0, cf = 0.0;
+#pragma unroll
+  for (int k = 0; k < NS; k++) {
+    rho = rho + di[k];
+    cf = cf + di[k] * cC.Ri[k] * cC.cf[k][0][5];
+  }
+  h0 = (Et + cf + p0) / rho;
+}
+template <int NS>
+__device__ __forceinline__ void cp_restore(double* di, double& Et, double h0, double p0, int* nfail) {
+  double rho = 0.0;
+#pragma unroll
+  for (int k = 0; k < NS; k++) rho = rho + di[k];
+  double Y[NS];
+  double R1 = 0.0, cf = 0.0;
+#pragma unroll
+  for (int k = 0; k < NS; k++) {
+    Y[k] = di[k] / rho;
+    R1 = R1 + cC.Ri[k] * Y[k];
+    cf = cf + Y[k] * cC.Ri[k] * cC.cf[k][0][5];
+  }
+  double T = dev_T<NS>(di, Et, nfail);
+  for (int it = 0; it < 50; it++) {
+    const double g = dev_E<NS>(Y, T) + R1 * T + cf - h0;
+    const double dT = g / dev_Cp<NS>(1.0, Y, T);
+    T = T - dT;
+    if (fabs(dT) <= 1.0e-10 * T) break;
+  }
+  const double r1 = p0 / (R1 * T);
+#pragma unroll
+  for (int k = 0; k < NS; k++) di[k] = Y[k] * r1;
+  Et = dev_E<NS>(di, T);
+}
+
 // a reactor's result is an error when a pivot was zero or a density or the energy is not finite
 template <int NS>
 __device__ __forceinline__ void chem_check(const double* di, double E, bool zero, int* nfail) {
@@ -415,7 +462,16 @@ __global__ void __launch_bounds__(OCFD_CHEM_TPB, OCFD_CHEM_MINB) k_chem_batch(in
       for (int m = 0; m < NS; m++) d1[m] = di[(size_t)r * NS + m];
       double ee = e[r];
       bool zero = false;
-      for (int s = 0; s < ks; s++) zero = chem_step<NS, OCFD_CHEM_TPB>(d1, ee, dt2, nfail, slab) || zero;
+      if (cC.const_p) {
+        double h0, p0;
+        cp_reference<NS>(d1, ee, h0, p0, nfail);
+        for (int s = 0; s < ks; s++) {
+          zero = chem_step<NS, OCFD_CHEM_TPB>(d1, ee, dt2, nfail, slab) || zero;
+          cp_restore<NS>(d1, ee, h0, p0, nfail);
+        }
+      } else {
+        for (int s = 0; s < ks; s++) zero = chem_step<NS, OCFD_CHEM_TPB>(d1, ee, dt2, nfail, slab) || zero;
+      }
       chem_check<NS>(d1, ee, zero, nfail);
 #pragma unroll
       for (int m = 0; m < NS; m++) di[(size_t)r * NS + m] = d1[m];

@@ -50,6 +50,7 @@ struct DevConst {
   double wk_c[OCFD_MAX_SPEC][OCFD_MAX_SPEC], wk_binv[OCFD_MAX_SPEC][OCFD_MAX_SPEC];
   // kinetics
   int nreac, rereac, timeadv;
+  int const_p;  // batched reactors: hold each reactor's pressure (extension; the reference is constant-volume)
   int af_type[OCFD_MAX_REAC], tr_reac[OCFD_MAX_REAC];
   double fc_troe[OCFD_MAX_REAC];
   double af[OCFD_MAX_REAC][2], bf[OCFD_MAX_REAC][2], ef[OCFD_MAX_REAC][2];

@@ -1252,6 +1252,7 @@ namespace ocfd {
 // the species count and the stream of the current set-up (ocfd_gpu_init or ocfd_gpu_chem_setup),
 // for the surrogate module
 int current_nspec() { return L && L->have_kin ? L->NS : 0; }
+int current_const_p() { return L && L->have_kin ? L->hc.const_p : 0; }
 cudaStream_t current_stream() { return L ? L->st : nullptr; }
 }  // namespace ocfd
 
@@ -1964,6 +1965,7 @@ int ocfd_gpu_chem_setup(const ocfd_thermo* th, const ocfd_kinetics* kin, int rea
     fill_kin(L->hc, kin);
     L->hc.timeadv = timeadv;
     L->hc.ns = th->n_spec;
+    L->hc.const_p = 0;  // the reference's constant-volume reactor unless ocfd_gpu_chem_constant_pressure(1)
     L->have_kin = true;
     CK(cudaMemcpyToSymbol(cC, &L->hc, sizeof(DevConst)));
     return 0;
@@ -2119,6 +2121,16 @@ int ocfd_gpu_chem_batch(int n, double* di, double* e, const double* dt, const in
     if (rc) g_err = "chemistry: " + std::to_string(L->b_last[1]) +
                     " reactor(s) with a zero Gauss pivot or a non-finite result (their values are returned as computed)";
     return rc;
+  });
+}
+
+int ocfd_gpu_chem_constant_pressure(int on) {
+  return guarded([&]() -> int {
+    if (!L || !L->have_kin) { g_err = "ocfd_gpu_init or ocfd_gpu_chem_setup with a mechanism first"; return OCFD_ERR_STATE; }
+    if (on < 0) return L->hc.const_p;
+    L->hc.const_p = on ? 1 : 0;
+    CK(cudaMemcpyToSymbol(cC, &L->hc, sizeof(DevConst)));
+    return 0;
   });
 }
 

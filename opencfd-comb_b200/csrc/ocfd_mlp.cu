@@ -20,10 +20,20 @@ namespace mlp {
 constexpr int BM = 128, BK = 64, THREADS = 128;
 constexpr long long WAIT_LIMIT = 1LL << 24;  // mbarrier polls before the kernel reports a timeout
 
-__device__ __forceinline__ float gelu(float x) { return 0.5f * x * (1.0f + erff(x * 0.70710678118654752f)); }
-// d GELU / dx = Phi(x) + x phi(x)
+// GELU in its tanh form: 0.5 x (1 + tanh(u)) = x sigmoid(2 u), u = sqrt(2 / pi) (x + 0.044715 x^3),
+// evaluated with the hardware exponential and a fast division (relative error ~1e-6, far below the
+// BF16 rounding of the activations); one exponential and one reciprocal per element instead of
+// erf's polynomial, which made the epilogue the bottleneck of the fused network
+__device__ __forceinline__ float gelu(float x) {
+  const float u2 = 1.5957691216057308f * x * (1.0f + 0.044715f * x * x);  // 2 u
+  return __fdividef(x, 1.0f + __expf(-u2));
+}
+// d GELU / dx = s + x s (1 - s) (2 u)', s = sigmoid(2 u)
 __device__ __forceinline__ float gelu_grad(float x) {
-  return 0.5f * (1.0f + erff(x * 0.70710678118654752f)) + x * 0.39894228040143268f * expf(-0.5f * x * x);
+  const float x2 = x * x;
+  const float u2 = 1.5957691216057308f * x * (1.0f + 0.044715f * x2);
+  const float sg = __fdividef(1.0f, 1.0f + __expf(-u2));
+  return sg + x * sg * (1.0f - sg) * (1.5957691216057308f * (1.0f + 0.134145f * x2));
 }
 
 template <int BN>
@@ -237,8 +247,8 @@ int launch_gemm(const GemmArgs& g, cudaStream_t st) {
 // the epilogues evaluate the same expressions.
 namespace fused {
 constexpr int MT = 128, THR = 256, KCH = 16, NKC = 256 / KCH, NBUF = 4, CHUNK = 256 * KCH * 2;
-constexpr int ACT_BYTES = MT * 256 * 2, X_BYTES = MT * 16 * 2;
-constexpr int BYTES = ACT_BYTES + X_BYTES + NBUF * CHUNK + 128;
+constexpr int ACT_BYTES = MT * 256 * 2, X_BYTES = MT * 16 * 2, BIAS_BYTES = (3 * 256 + 16) * 4;
+constexpr int BYTES = ACT_BYTES + X_BYTES + NBUF * CHUNK + BIAS_BYTES + 128;
 static_assert(2 * BYTES <= 226 * 1024, "two blocks per SM");
 static_assert(MLP_PACK_BYTES == (2 + 2 * NKC) * CHUNK, "packed weight layout");
 // byte offsets of the packed images: W0 (256 x 16), the 16 chunks of W1 and of W2 (256 x 16
@@ -307,13 +317,15 @@ __global__ void __launch_bounds__(fused::THR, 2) k_mlp_fused(MlpArgs a) {
   uint8_t* act = sm;               // 128 x 256 activations, K-major
   uint8_t* xin = sm + ACT_BYTES;   // 128 x 16 inputs
   uint8_t* wbase = xin + X_BYTES;  // NBUF weight chunk buffers of CHUNK bytes
-  uint64_t* tb = reinterpret_cast<uint64_t*>(wbase + NBUF * CHUNK);  // chunk landed (bulk copy)
+  float* sbias = reinterpret_cast<float*>(wbase + NBUF * CHUNK);     // b0, b1, b2 (256 each), b3 (16)
+  uint64_t* tb = reinterpret_cast<uint64_t*>(wbase + NBUF * CHUNK + BIAS_BYTES);  // chunk landed (bulk copy)
   uint64_t* mb = tb + NBUF;                                          // MMAs reading the chunk done
   uint32_t* tslot = reinterpret_cast<uint32_t*>(mb + NBUF);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int m0 = blockIdx.x * MT;
 
   if (warp == 0) tc::tmem_alloc(tslot, 256);
+  for (int e = tid; e < 3 * 256 + 16; e += THR) sbias[e] = e < 768 ? a.b[e >> 8][e & 255] : a.b[3][e - 768];
   if (tid == 0) {
     for (int b = 0; b < NBUF; b++) {
       tc::mbar_init(&tb[b], 1);
@@ -351,10 +363,16 @@ __global__ void __launch_bounds__(fused::THR, 2) k_mlp_fused(MlpArgs a) {
       tc::tmem_ld32(tmem + ((uint32_t)(32 * (warp & 3)) << 16) + (uint32_t)c0, v);
 #pragma unroll
       for (int q = 0; q < 4; q++) {
-        __align__(16) __nv_bfloat16 pk[8];
+        uint4 pk;
+        uint32_t* pw = reinterpret_cast<uint32_t*>(&pk);
 #pragma unroll
-        for (int j = 0; j < 8; j++) pk[j] = __float2bfloat16(gelu(v[q * 8 + j] + bias[c0 + q * 8 + j]));
-        *reinterpret_cast<uint4*>(act + tc::kmajor_off(rl, c0 + q * 8, MT)) = *reinterpret_cast<const uint4*>(pk);
+        for (int j = 0; j < 4; j++) {
+          const int c = q * 8 + 2 * j;
+          const __nv_bfloat162 h2 =
+              __floats2bfloat162_rn(gelu(v[c] + bias[c0 + c]), gelu(v[c + 1] + bias[c0 + c + 1]));
+          pw[j] = *reinterpret_cast<const uint32_t*>(&h2);
+        }
+        *reinterpret_cast<uint4*>(act + tc::kmajor_off(rl, c0 + q * 8, MT)) = pk;
       }
     }
     tc::fence_proxy_async();  // generic shared-memory writes -> operands of the next MMAs
@@ -381,7 +399,7 @@ __global__ void __launch_bounds__(fused::THR, 2) k_mlp_fused(MlpArgs a) {
       for (int c = 0; c < NBUF - 1; c++) fetch(c, pack_chunk(1, c));
   }
   bool all = agree();
-  if (all) hidden_epilogue(a.b[0]);
+  if (all) hidden_epilogue(sbias);
 
   // layers 1, 2: 256 -> 256, sixteen K = 16 chunks through the NBUF buffers
   for (int l = 1; l <= 2 && all; l++) {
@@ -411,7 +429,7 @@ __global__ void __launch_bounds__(fused::THR, 2) k_mlp_fused(MlpArgs a) {
       }
     }
     all = agree();
-    if (all) hidden_epilogue(a.b[l]);
+    if (all) hidden_epilogue(sbias + 256 * l);
   }
 
   // layer 3: 256 -> 16, sixteen K = 16 MMAs of N = 16 on the whole W3 image
@@ -441,8 +459,8 @@ __global__ void __launch_bounds__(fused::THR, 2) k_mlp_fused(MlpArgs a) {
         float4* o = reinterpret_cast<float4*>(a.out + (long long)row * 16);
 #pragma unroll
         for (int q = 0; q < 4; q++)
-          o[q] = make_float4(v[4 * q] + a.b[3][4 * q], v[4 * q + 1] + a.b[3][4 * q + 1], v[4 * q + 2] + a.b[3][4 * q + 2],
-                             v[4 * q + 3] + a.b[3][4 * q + 3]);
+          o[q] = make_float4(v[4 * q] + sbias[768 + 4 * q], v[4 * q + 1] + sbias[769 + 4 * q],
+                             v[4 * q + 2] + sbias[770 + 4 * q], v[4 * q + 3] + sbias[771 + 4 * q]);
       }
     }
   } else if (tid == 0) {

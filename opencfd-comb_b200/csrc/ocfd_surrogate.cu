@@ -28,6 +28,7 @@ namespace ocfd {
 void launch_chem_batch(int ns, int sms, int n, double* di, double* e, const double* dt, const int* nsub,
                        const int* perm, int* counter, int* nfail, cudaStream_t st);
 int current_nspec();
+int current_const_p();
 cudaStream_t current_stream();
 
 namespace sg {
@@ -894,6 +895,7 @@ int ocfd_gpu_surrogate_predict(int n, const double* d_di, const double* d_e, con
 int ocfd_gpu_chem_batch_surrogate(int n, double* d_di, double* d_e, const double* d_dt, const int* d_nsub,
                                   double tol_T, int* n_fallback) {
   if (n <= 0) return 0;
+  if (current_const_p()) return -7;  // the network replaces the constant-volume integrator only
   return run_surrogate(n, 1, d_di, d_e, d_dt, d_nsub, tol_T, nullptr, nullptr, nullptr, nullptr, n_fallback);
 }
 

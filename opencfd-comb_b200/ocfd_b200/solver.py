@@ -273,8 +273,12 @@ class Solver:
         lib().ocfd_gpu_finalize()
 
 
-def chem_setup(thermo, kin, realgas=1, timeadv=abi.CHEM_IMPLICIT):
+def chem_setup(thermo, kin, realgas=1, timeadv=abi.CHEM_IMPLICIT, const_p=False):
+    """Chemistry tables for the batched reactors; const_p: constant-pressure reactors (an extension,
+    ocfd_gpu_chem_constant_pressure) instead of the reference's constant-volume one."""
     _chk(lib().ocfd_gpu_chem_setup(C.byref(thermo), C.byref(kin), realgas, timeadv))
+    if const_p:
+        _chk(lib().ocfd_gpu_chem_constant_pressure(1))
 
 
 def chem_batch(di, e, dt, nsub=None):

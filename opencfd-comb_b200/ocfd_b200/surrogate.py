@@ -109,6 +109,40 @@ class Surrogate:
         return (np.ascontiguousarray(dii[idx]), np.ascontiguousarray(E[idx]), np.full(n, case.dt),
                 np.full(n, case.nsub, dtype=np.int32))
 
+    def c4_states(self, n_reactors=1 << 22, jet_cells=1 << 21, seed=0, jet_shape=(384, 256, 256)):
+        """The learned-chemistry state set: C3 reactors (seeded draws: T 900-2200 K, equivalence ratio
+        0.3-3, product fraction 0-0.5, dt log-uniform in 1e-8..1e-6 s, 1 atm) at two points of their
+        trajectory (the draw and the state after one FP64 constant-pressure integration over dt),
+        plus cells of two FP64 snapshots of the reacting jet (after 8 and 16 steps). With the
+        defaults: 2 x 2^22 reactor states + 2^21 jet cells = 10 x 2^20 states. Returns
+        (di, E, dt, nsub, source) with source 0 = reactor, 1 = jet."""
+        di, E, dt, nsub = self.reactors(n_reactors, seed)
+        solver.chem_setup(self.th, self.kin, 1, abi.CHEM_IMPLICIT, const_p=True)
+        d1, e1 = self.fp64(di, E, dt, nsub)
+        solver.chem_setup(self.th, self.kin, 1, abi.CHEM_IMPLICIT)
+        parts = [(di, E, dt, nsub), (d1.cpu().numpy(), e1.cpu().numpy(), dt, nsub)]
+        del d1, e1
+        case = cases.jet(*jet_shape)
+        g = solver.Solver(case)
+        g.init_state()
+        L = solver.lib()
+        for s0, s1, sd in ((0, 8, seed + 1), (8, 16, seed + 2)):
+            solver._chk(L.ocfd_gpu_run(case.dt, s0 * case.dt, s1 - s0, 1, case.nsub))
+            _, dj, pj = g.download_state()
+            parts.append(self.samples_from_state(case, dj, pj, jet_cells // 2, sd))
+            del dj, pj
+        g.close()
+        solver.chem_setup(self.th, self.kin, 1, abi.CHEM_IMPLICIT)
+        src = np.concatenate([np.full(len(p[1]), 0 if k < 2 else 1, np.int8) for k, p in enumerate(parts)])
+        return (np.concatenate([p[0] for p in parts]), np.concatenate([p[1] for p in parts]),
+                np.concatenate([p[2] for p in parts]), np.concatenate([p[3] for p in parts]).astype(np.int32), src)
+
+    @staticmethod
+    def split(n, n_hold, seed=0):
+        """Seeded split of n states into (train index, held-out index) with n_hold held out."""
+        perm = np.random.default_rng(seed).permutation(n)
+        return np.sort(perm[n_hold:]), np.sort(perm[:n_hold])
+
     def train_on(self, parts, epochs=20, batch=1024, lr=2e-3, seed=0):
         """Trains on the concatenation of (di, E, dt, nsub) reactor sets, targets from the FP64
         integrator."""
@@ -132,8 +166,13 @@ class Surrogate:
     def evaluate(self, n=1 << 16, seed=12345, tol_T=5.0):
         """Held-out reactors: errors of the ungated network and of the gated surrogate against the
         FP64 integrator, the fallback fraction and the element-conservation residual."""
-        t = self.torch
         di, E, dt, nsub = self.reactors(n, seed)
+        return self.evaluate_on(di, E, dt, nsub, tol_T)
+
+    def evaluate_on(self, di, E, dt, nsub, tol_T=5.0):
+        """The same on given states (di (n, Ns), E, dt, nsub)."""
+        t = self.torch
+        n = len(E)
         d_di, d_e, d_dt, d_ns = _dev(t, di), _dev(t, E), _dev(t, dt), _dev(t, nsub)
         f_di, f_e = self.fp64(di, E, dt, nsub)
         T_ref = self.temperature(f_di, f_e)

@@ -1530,9 +1530,10 @@ int ocfd_cpu_diag(double* e_mean, double* k_mean) {
 }
 
 /* Batched 0-D reactors: chemical_timeAdv applied nsub[r] times with dt[r]/nsub[r]. Standalone:
- * needs only thermo + kinetics (no grid). */
+ * needs only thermo + kinetics (no grid). const_p = 1: constant-pressure reactors (cp_restore
+ * after every sub-step), 0: the reference's constant-volume reactor. */
 int ocfd_cpu_chem_batch(const ocfd_thermo* th, const ocfd_kinetics* kin, int realgas, int timeadv, int n,
-                        double* di, double* e, const double* dt, const int* nsub, int nthreads) {
+                        double* di, double* e, const double* dt, const int* nsub, int nthreads, int const_p) {
   static Chem ch;
   ch.set_thermo(th, realgas);
   ch.kin = *kin;
@@ -1548,7 +1549,12 @@ int ocfd_cpu_chem_batch(const ocfd_thermo* th, const ocfd_kinetics* kin, int rea
     int ks = nsub ? nsub[r] : 1;
     double dt2 = dt[r] / ks;
     double* dr = di + (long)r * ns;
-    for (int s = 0; s < ks; s++) ch.time_adv(dr, e[r], dt2);
+    double h0 = 0.0, p0 = 0.0;
+    if (const_p) ch.cp_reference(dr, e[r], h0, p0);
+    for (int s = 0; s < ks; s++) {
+      ch.time_adv(dr, e[r], dt2);
+      if (const_p) ch.cp_restore(dr, e[r], h0, p0);
+    }
   }
   return 0;
 }

@@ -214,6 +214,46 @@ struct Chem {
     return e;
   }
 
+  /* Constant-pressure reactor (an extension: the reference's reactor is constant-volume,
+   * OCFD_Time_Adv.f90:174-193). The reactor keeps its initial pressure p0 and specific total
+   * enthalpy h0 = (E + sum d_k R_k F_k + p) / rho, E the sensible energy of comput_E and F_k the
+   * formation term that update_Et (CHEM_thermdyn.f90:184-196) books. After every constant-volume
+   * sub-step the mixture (mass fractions Y fixed) is brought back to p0 at h0: Newton on T for
+   * e(T, Y) + R T + sum Y_k R_k F_k = h0 (e from comput_E with Y as densities, derivative the
+   * mass-specific Cp), stopped when |dT| <= 1e-10 T (at most 50 iterations), then
+   * rho = p0 / (R T), d = Y rho, E = comput_E(d, T). The GPU applies the identical operations. */
+  void cp_reference(const double* di, double Et, double& h0, double& p0) const {
+    double T = T_of_E(di, Et);
+    p0 = P(di, T);
+    double rho = 0.0, cf = 0.0;
+    for (int k = 0; k < ns; k++) {
+      rho = rho + di[k];
+      cf = cf + di[k] * Ri[k] * F[k][0];
+    }
+    h0 = (Et + cf + p0) / rho;
+  }
+  void cp_restore(double* di, double& Et, double h0, double p0) const {
+    double rho = 0.0;
+    for (int k = 0; k < ns; k++) rho = rho + di[k];
+    double Y[OCFD_MAX_SPEC];
+    double R1 = 0.0, cf = 0.0;
+    for (int k = 0; k < ns; k++) {
+      Y[k] = di[k] / rho;
+      R1 = R1 + Ri[k] * Y[k];
+      cf = cf + Y[k] * Ri[k] * F[k][0];
+    }
+    double T = T_of_E(di, Et);
+    for (int it = 0; it < 50; it++) {
+      double g = E_of_T(Y, T) + R1 * T + cf - h0;
+      double dT = g / Cp(1.0, Y, T);
+      T = T - dT;
+      if (std::fabs(dT) <= 1.0e-10 * T) break;
+    }
+    double r1 = p0 / (R1 * T);
+    for (int k = 0; k < ns; k++) di[k] = Y[k] * r1;
+    Et = E_of_T(di, T);
+  }
+
   /* ---------------- transport (TRANSPORT_modules.f90) ---------------- */
   double viscosity(double T, const double* Xi) const {
     if (tr.flag_vis == 0) {

@@ -21,16 +21,23 @@ def bf16(a):
     return (r & 0xFFFFFFFF).astype(np.uint32).view(np.float32).astype(np.float64)
 
 
-def _erf(x):
-    return np.vectorize(math.erf)(x)
+K2 = 2.0 * math.sqrt(2.0 / math.pi)  # 2 sqrt(2 / pi)
+
+
+def _sig2u(x):
+    """sigmoid(2 u), u = sqrt(2 / pi) (x + 0.044715 x^3)"""
+    with np.errstate(over="ignore"):
+        return 1.0 / (1.0 + np.exp(-K2 * x * (1.0 + 0.044715 * x * x)))
 
 
 def gelu(x):
-    return 0.5 * x * (1.0 + _erf(x / math.sqrt(2.0)))
+    """GELU in its tanh form, 0.5 x (1 + tanh(u)) = x sigmoid(2 u)."""
+    return x * _sig2u(x)
 
 
 def gelu_grad(x):
-    return 0.5 * (1.0 + _erf(x / math.sqrt(2.0))) + x * np.exp(-0.5 * x * x) / math.sqrt(2.0 * math.pi)
+    s = _sig2u(x)
+    return s + x * s * (1.0 - s) * K2 * (1.0 + 3.0 * 0.044715 * x * x)
 
 
 def unpack(blob):

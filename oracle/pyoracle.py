@@ -44,7 +44,7 @@ def lib():
             "ocfd_cpu_download_metrics": (C.c_int, [PD]),
             "ocfd_cpu_diag": (C.c_int, [PD, PD]),
             "ocfd_cpu_chem_batch": (C.c_int, [C.POINTER(abi.Thermo), C.POINTER(abi.Kinetics), C.c_int, C.c_int,
-                                              C.c_int, PD, PD, PD, PI, C.c_int]),
+                                              C.c_int, PD, PD, PD, PI, C.c_int, C.c_int]),
             "ocfd_cpu_probe": (C.c_double, [C.POINTER(abi.Thermo), C.c_int, C.c_int, PD, C.c_double]),
             "ocfd_cpu_set_threads": (C.c_int, [C.c_int]),
             "ocfd_cpu_flux_line": (C.c_int, [C.c_int, C.c_int, PD, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, PI,
@@ -167,11 +167,13 @@ class OracleSolver:
         lib().ocfd_cpu_finalize()
 
 
-def chem_batch(thermo, kin, realgas, timeadv, di, e, dt, nsub=None, threads=0):
-    """Batched 0-D reactors on the CPU; di (n, Ns) and e (n) are updated in place."""
+def chem_batch(thermo, kin, realgas, timeadv, di, e, dt, nsub=None, threads=0, const_p=False):
+    """Batched 0-D reactors on the CPU; di (n, Ns) and e (n) are updated in place. const_p: hold
+    each reactor's initial pressure at constant specific enthalpy after every sub-step (an
+    extension; the reference's reactor is constant-volume)."""
     n = len(e)
     _chk(lib().ocfd_cpu_chem_batch(C.byref(thermo), C.byref(kin), realgas, timeadv, n, abi.dptr(di), abi.dptr(e),
-                                   abi.dptr(dt), abi.iptr(nsub), threads))
+                                   abi.dptr(dt), abi.iptr(nsub), threads, 1 if const_p else 0))
 
 
 def flux_line(scheme, plus, f, bnd=(0, 0), sb=(0, 0), scm=None, ud7l_diss=1.0, theta=(1.0, 1.0)):

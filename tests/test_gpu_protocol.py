@@ -38,8 +38,9 @@ def rel_linf(a, b):
 
 
 def decisions(c, rh):
-    """Per-interface scheme index of HYBRID in each direction: R = max(R_i, R_i+1) against
-    theta1 / theta2 (OCFD_Schemes.f90:329-370, set_hybrid_scheme OCFD_SetHybrid.f90:2-15)."""
+    """Per-interface scheme of HYBRID in each direction: R = max(R_i, R_i+1) against theta1 / theta2
+    (OCFD_Schemes.f90:329-370, set_hybrid_scheme OCFD_SetHybrid.f90:2-15); 0 = UD7L, 1 = WENO7,
+    2 = WENO5."""
     th1, th2 = c.params.hybrid_para[1], c.params.hybrid_para[2]
     r = interior(rh)
     out = []
@@ -162,7 +163,7 @@ def test_hybrid_sensor2_with_forced_patches(oracle, gpu):
         # the patches hold Rhybrid >= 100 (the most robust scheme) inside their boxes
         r = interior(rg)
         assert r[1:5, 0:6, 2:9].min() >= 100.0 and r[0:12, 9:20, 19:30].min() >= 100.0
-    assert used == {1, 2, 3}
+    assert used == {0, 1, 2}  # UD7L, WENO7 and WENO5 interfaces all occur
     assert_bitwise(o.download_state(), g.download_state())
     o.close()
     g.close()
@@ -277,3 +278,28 @@ def test_chem_batch_full_size(oracle, gpu):
     assert err.max() <= TOL, err.max()
     assert np.abs(eg - eo).max() <= TOL * np.abs(eo).max()
     assert np.abs(dig - di).max() > 0
+
+
+def test_chem_batch_constant_pressure(oracle, gpu):
+    """C3's constant-pressure reactors (an extension of the reference's constant-volume reactor):
+    the GPU applies the oracle's pressure-restoring rule after every sub-step; the reactors keep
+    their initial pressure and specific total enthalpy."""
+    names, th, kin, di, E, dt, nsub, T = cases.reactors(n=8192, seed=4)
+    dio, eo = di.copy(), E.copy()
+    oracle.chem_batch(th, kin, 1, abi.CHEM_IMPLICIT, dio, eo, dt, nsub, threads=os.cpu_count() or 1, const_p=True)
+    gpu.chem_setup(th, kin, 1, abi.CHEM_IMPLICIT, const_p=True)
+    assert gpu.lib().ocfd_gpu_chem_constant_pressure(-1) == 1
+    dig, eg = di.copy(), E.copy()
+    gpu.chem_batch(dig, eg, dt, nsub)
+    gpu.chem_setup(th, kin, 1, abi.CHEM_IMPLICIT)  # back to the reference's reactor
+    assert gpu.lib().ocfd_gpu_chem_constant_pressure(-1) == 0
+    scale = np.abs(dio).max(axis=1, keepdims=True)
+    assert (np.abs(dig - dio) / scale).max() <= TOL
+    assert np.abs(eg - eo).max() <= TOL * np.abs(eo).max()
+    # pressure held: p = sum R_k d_k T before and after, for a sample of reactors
+    for r in range(0, 8192, 512):
+        T0 = oracle.probe(th, 1, 1, di[r], E[r])
+        T1 = oracle.probe(th, 1, 1, dig[r], eg[r])
+        p0, p1 = oracle.probe(th, 1, 2, di[r], T0), oracle.probe(th, 1, 2, dig[r], T1)
+        assert abs(p1 - p0) <= 1e-10 * p0
+    assert np.abs(dig.sum(axis=1) - di.sum(axis=1)).max() > 0  # the density moved to hold p
