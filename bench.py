@@ -635,8 +635,9 @@ def jet_roofline(prof, nsteps, ncell):
     if os.path.exists(tfile):
         with open(tfile) as fh:
             tr = json.load(fh)
-        if dom in tr:
-            traffic = tr[dom] * ncell
+        if dom in tr:  # per launch; the file holds one stage's bytes for the classes of several launches
+            per_stage = dom in ("species_flux", "species_visc")
+            traffic = tr[dom] * ncell / (launches / JET_STAGES_PER_STEP if per_stage else 1.0)
     return {"bound": "hbm", "kernel": dom, "achieved": d["achieved_gbs"], "peak": hbm, "unit": "GB/s",
             "frac": d["frac"], "traffic": traffic, "peak_kind": hbm_kind,
             "alg_bytes_per_launch": d["alg_bytes_per_step"] / launches,

@@ -6,7 +6,7 @@
  *
  * The Fortran driver of the reference keeps parsing its control files and
  * keeps its output formats; it replaces the two hot call sites of its time
- * loop with the entry points below (bind(C) interface in INTEGRATION.md):
+ * loop with the entry points below (through an iso_c_binding interface module):
  *
  *   code/flow-solver/OCFD_NS_Solver.f90:28,37  call flow_time_advance(dt1)
  *        -> ocfd_gpu_flow_advance(dt1, tt)
@@ -150,7 +150,10 @@ typedef struct ocfd_bcdata {
  * them; the library applies the periodic exchange, the periodic coordinate shift, the Jacobian
  * (comput_Jacobian3d, OCFD_mesh.f90:60-107) and Akx1..Asz1 on the device. metrics (optional,
  * NULL = compute) = Akx,Aky,Akz,Aix,Aiy,Aiz,Asx,Asy,Asz,Ajac (10 halo arrays) as for
- * Iflag_Gridtype=31. kin may be NULL when chemistry is off; bc may be NULL for BC_NONE. */
+ * Iflag_Gridtype=31. kin may be NULL when chemistry is off; bc may be NULL for BC_NONE.
+ * Differs from a call that would hand over all 19 metric arrays: the library derives the nine
+ * Akx1..Asz1 (= A / Ajac) itself, and on a tensor-product grid it keeps the metrics as 1-D
+ * derivatives, so the caller passes the coordinates (plus, optionally, the 10 arrays it read). */
 int ocfd_gpu_init(const ocfd_params* p, const ocfd_thermo* th, const ocfd_kinetics* kin,
                   const ocfd_transport* tr, const ocfd_bcdata* bc,
                   const double* coords, const double* metrics);
@@ -162,11 +165,14 @@ int ocfd_gpu_init(const ocfd_params* p, const ocfd_thermo* th, const ocfd_kineti
  * arrays. Halo points take allocate_flow_data's initial values (OCFD_allocate_data.f90:53-67). */
 int ocfd_gpu_init_state(const double* prim5, const double* di, double tt);
 
-/* Uploads the Fortran module state: f (N*5), di (H*Ns), prims (7*H: d,u,v,w,T,p,Et). */
+/* Uploads the Fortran module state: f (N*5), di (H*Ns), prims (7*H: d,u,v,w,T,p,Et). The
+ * restart's tt and Istep stay with the caller (tt is an argument of the advancing calls). */
 int ocfd_gpu_upload_state(const double* f, const double* di, const double* prims);
 
 /* flow_time_advance(dt1) (code/flow-solver/OCFD_Time_Adv.f90:7-92): 3 RK stages; tt is the
- * solver time at the call (used by the wall disturbance, OCFD_BC_Boundarylayers.f90:147). */
+ * solver time at the call (used by the wall disturbance, OCFD_BC_Boundarylayers.f90:147). The
+ * reference routine takes dt1 alone and reads tt from the module flow_para; a C library has no
+ * such module, so the caller passes its tt. */
 int ocfd_gpu_flow_advance(double dt1, double tt);
 
 /* nsub x Chemical_time_advance(dt2) (OCFD_Time_Adv.f90:169-196) followed by comput_T_P
@@ -183,7 +189,9 @@ int ocfd_gpu_step(double dt, double tt, int if_reaction, int nsub);
  * captured step as a child graph, the step's wall-disturbance time taken on the device). */
 int ocfd_gpu_run(double dt, double tt0, int nsteps, int if_reaction, int nsub);
 
-/* Downloads the state; any pointer may be NULL to skip that part. */
+/* Downloads the state; any pointer may be NULL to skip that part. The mixture viscosity Amu is
+ * not part of it: the analysis that reads Amu (ana_box) runs on the device
+ * (ocfd_gpu_keep_viscosity, ocfd_gpu_ana_box). */
 int ocfd_gpu_download_state(double* f, double* di, double* prims);
 
 /* show_flow_msg reductions (OCFD_Time_Adv.f90:210-223): mean total and kinetic energy. */
@@ -378,7 +386,10 @@ int ocfd_gpu_chem_temperature(int n, const double* d_di, const double* d_e, doub
  * setting. */
 int ocfd_gpu_surrogate_fused(int on);
 
-/* Chemistry of the flow solver's Strang step (ocfd_gpu_step, ocfd_gpu_run, ocfd_gpu_chem_advance):
+/* Chemistry of the flow solver's Strang step (ocfd_gpu_step, ocfd_gpu_run, ocfd_gpu_chem_advance).
+ * The network is not read from a weights file here: it is trained on the device
+ * (ocfd_gpu_surrogate_train) or loaded from floats (ocfd_gpu_surrogate_blob, set = 1), and this
+ * call takes the gate tolerance instead of a path:
  * mode 0 the FP64 integrator of Chemical_time_advance (default), mode 1 the gated surrogate, whose
  * rejected cells (|T_energy - T_pred| > tol_T, negative composition, outside the training range)
  * take the FP64 sub-steps; the step stays one CUDA graph. Mode 1 needs a trained or loaded

@@ -4,6 +4,7 @@
 #include "ocfd_launch.h"
 
 namespace ocfd {
+int current_const_p();  // the batched reactors' form (ocfd_gpu.cu): 1 constant pressure, 0 constant volume
 
 #define NS_CASES(...)                                          \
   switch (ns) {                                                \
@@ -27,11 +28,18 @@ void launch_chem_cells(int ns, long long ncell, double* f, double* Et, double* T
 
 void launch_chem_batch(int ns, int sms, int n, double* di, double* e, const double* dt, const int* nsub,
                        const int* perm, int* counter, int* nfail, cudaStream_t st) {
+  const bool cp = current_const_p() != 0;
   NS_CASES({
     int per = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_chem_batch<NSV>, OCFD_CHEM_TPB, 0);
-    if (per < 1) per = 1;
-    k_chem_batch<NSV><<<sms * per, OCFD_CHEM_TPB, 0, st>>>(n, di, e, dt, nsub, perm, counter, nfail);
+    if (cp) {
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_chem_batch<NSV, true>, OCFD_CHEM_TPB, 0);
+      if (per < 1) per = 1;
+      k_chem_batch<NSV, true><<<sms * per, OCFD_CHEM_TPB, 0, st>>>(n, di, e, dt, nsub, perm, counter, nfail);
+    } else {
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_chem_batch<NSV, false>, OCFD_CHEM_TPB, 0);
+      if (per < 1) per = 1;
+      k_chem_batch<NSV, false><<<sms * per, OCFD_CHEM_TPB, 0, st>>>(n, di, e, dt, nsub, perm, counter, nfail);
+    }
   });
 }
 }  // namespace ocfd

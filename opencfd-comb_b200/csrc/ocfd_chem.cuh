@@ -439,7 +439,9 @@ static __global__ void k_nsub_scatter(int n, const int* nsub, int* cursor, int n
   perm[pos] = t;
 }
 
-template <int NS>
+// CP: constant-pressure reactors (a template parameter, so the reference's constant-volume form
+// carries none of the pressure-restoring code in its registers)
+template <int NS, bool CP>
 __global__ void __launch_bounds__(OCFD_CHEM_TPB, OCFD_CHEM_MINB) k_chem_batch(int n, double* di, double* e,
                                                                              const double* dt, const int* nsub,
                                                                              const int* perm, int* counter,
@@ -462,7 +464,7 @@ __global__ void __launch_bounds__(OCFD_CHEM_TPB, OCFD_CHEM_MINB) k_chem_batch(in
       for (int m = 0; m < NS; m++) d1[m] = di[(size_t)r * NS + m];
       double ee = e[r];
       bool zero = false;
-      if (cC.const_p) {
+      if (CP) {
         double h0, p0;
         cp_reference<NS>(d1, ee, h0, p0, nfail);
         for (int s = 0; s < ks; s++) {

@@ -48,6 +48,8 @@ struct DevConst {
   double wk_a[OCFD_MAX_SPEC][OCFD_MAX_SPEC], wk_b[OCFD_MAX_SPEC][OCFD_MAX_SPEC];
   // the same pair constants for the multi-species transport kernel: sqrt(wk_a) and 1 / wk_b
   double wk_c[OCFD_MAX_SPEC][OCFD_MAX_SPEC], wk_binv[OCFD_MAX_SPEC][OCFD_MAX_SPEC];
+  // species pairs (a, b), a < b, enumerated a-major: pair p = (pair_a[p], pair_b[p])
+  unsigned char pair_a[OCFD_MAX_SPEC * (OCFD_MAX_SPEC - 1) / 2], pair_b[OCFD_MAX_SPEC * (OCFD_MAX_SPEC - 1) / 2];
   // kinetics
   int nreac, rereac, timeadv;
   int const_p;  // batched reactors: hold each reactor's pressure (extension; the reference is constant-volume)

@@ -916,8 +916,10 @@ static __global__ void k_scal_rk(int krk, double dt, const double* dus, const do
 // binary-diffusion pairs are spread over a cell's NS threads; every sum is taken from shared
 // memory in the reference's order. The divisions and square roots of the pair terms are
 // restated as products (square roots of the viscosities per species, reciprocal pair constants
-// from the host, 1 / D2 as exp(-poly) * 1e4): the same quantities up to last-place rounding,
-// which the transcendental functions of this path already make inexact against the oracle.
+// from the host, 1 / D2 as exp(-poly) * 1e4, 1 / kappa_k formed by species k's thread): the same
+// quantities up to last-place rounding, which the transcendental functions of this path already
+// make inexact against the oracle. ln T is formed once per cell; the species pairs come from a
+// table.
 // k_transport runs one block more than k_scal_ev: at 4 blocks of 9 species it needs 56 registers
 // and spills only 32 bytes (k_scal_ev would spill 120-280), measured 504 -> 495.5 ms per jet step
 #ifndef OCFD_TRANSPORT_MINB
@@ -929,6 +931,7 @@ __global__ void __launch_bounds__(32 * NS, OCFD_TRANSPORT_MINB) k_transport(cons
   constexpr int NP = NS * (NS - 1) / 2;
   __shared__ double sX[NS][32], sD0[NS][32], sMu[NS][32], sK[NS][32], sW[NS][32], sD2[NP > 0 ? NP : 1][32];
   __shared__ double sSq[NS][32], sRs[NS][32];  // sqrt(mu_k), 1 / sqrt(mu_k)
+  __shared__ double sKr[NS][32], sL[32];       // 1 / kappa_k; ln T of the cell (formed once)
   const int ks = threadIdx.y, lane = threadIdx.x;
   int i, j, k;
   const bool ok = cell_of((long long)blockIdx.x * 32 + lane, i, j, k);
@@ -939,6 +942,7 @@ __global__ void __launch_bounds__(32 * NS, OCFD_TRANSPORT_MINB) k_transport(cons
     sD0[ks][lane] = d0;
     sX[ks][lane] = d0 / cC.Mi[ks];
   }
+  if (ks == NS - 1) sL[lane] = log(Tq);
   __syncthreads();
   {
     double X0 = 0.0;
@@ -950,7 +954,7 @@ __global__ void __launch_bounds__(32 * NS, OCFD_TRANSPORT_MINB) k_transport(cons
   double Xi[NS];
 #pragma unroll
   for (int m = 0; m < NS; m++) Xi[m] = sW[m][lane];
-  const double L = log(Tq);
+  const double L = sL[lane];
   if (cC.flag_vis != 0) {
     const double muk = exp(cC.mu_an[ks][0] + cC.mu_an[ks][1] * L + cC.mu_an[ks][2] * q2(L) + cC.mu_an[ks][3] * q3(L)) * 0.1;
     sMu[ks][lane] = muk;
@@ -958,13 +962,14 @@ __global__ void __launch_bounds__(32 * NS, OCFD_TRANSPORT_MINB) k_transport(cons
     sSq[ks][lane] = sq;
     sRs[ks][lane] = 1.0 / sq;
   }
-  if (cC.flag_cond != 0)
-    sK[ks][lane] = exp(cC.k_an[ks][0] + cC.k_an[ks][1] * L + cC.k_an[ks][2] * q2(L) + cC.k_an[ks][3] * q3(L)) * 1.0e-5;
+  if (cC.flag_cond != 0) {
+    const double kk = exp(cC.k_an[ks][0] + cC.k_an[ks][1] * L + cC.k_an[ks][2] * q2(L) + cC.k_an[ks][3] * q3(L)) * 1.0e-5;
+    sK[ks][lane] = kk;
+    sKr[ks][lane] = 1.0 / kk;  // the species' own thread forms the reciprocal for the harmonic sum
+  }
   if (cC.flag_diff != 0) {
     for (int pi = ks; pi < NP; pi += NS) {  // pair pi = (a, b), a < b, enumerated a-major
-      int a = 0, r = pi;
-      while (r >= NS - 1 - a) { r -= NS - 1 - a; a++; }
-      const int b = a + 1 + r;
+      const int a = cC.pair_a[pi], b = cC.pair_b[pi];
       // 1 / D2 of the pair: exp(-poly) * 1e4 (the reciprocal of exp(poly) * 1e-4 up to rounding)
       sD2[pi][lane] =
           exp(-(cC.d_an[a][b][0] + cC.d_an[a][b][1] * L + cC.d_an[a][b][2] * q2(L) + cC.d_an[a][b][3] * q3(L))) * 1.0e4;
@@ -1010,9 +1015,8 @@ __global__ void __launch_bounds__(32 * NS, OCFD_TRANSPORT_MINB) k_transport(cons
       double a1 = 0.0, a2 = 0.0;
 #pragma unroll
       for (int m = 0; m < NS; m++) {
-        const double ki = sK[m][lane];
-        a1 = a1 + Xi[m] * ki;
-        a2 = a2 + Xi[m] / ki;
+        a1 = a1 + Xi[m] * sK[m][lane];
+        a2 = a2 + Xi[m] * sKr[m][lane];  // X_m / kappa_m as X_m (1 / kappa_m): the same up to the last place
       }
       kk = 0.5 * (a1 + 1.0 / a2);
     }

@@ -27,6 +27,7 @@ int sg_cells_chem(int ns, double* f, double* Et, double* T, double* p, double* d
                   cudaStream_t st);
 int sg_cells_setup(int ns, long long N, double tol);
 long long sg_cells_rejected(long long* reasons);
+int sg_device_error(cudaStream_t st);
 // set-up kernels (defined below) that the tile autotuner also launches
 __global__ void k_fill(double* p, long long n, double v);
 __global__ void k_jacobian(const double* X, const double* Y, const double* Z, double* const* m);
@@ -593,8 +594,9 @@ template <int NS>
 void chem_t(double dt2, int nsub) {
   KTimer t(KC_CHEM);
   if (L->chem_mode == 1) {
-    if (sg_cells_chem(NS, L->f, L->Et[L->cur], L->T, L->p, L->di, dt2, nsub, &L->sdev->newton_fail, L->st) != 0)
-      throw std::runtime_error("surrogate chemistry not set up for this grid and mechanism");
+    const int rc = sg_cells_chem(NS, L->f, L->Et[L->cur], L->T, L->p, L->di, dt2, nsub, &L->sdev->newton_fail, L->st);
+    if (rc == -5) throw std::runtime_error("surrogate chemistry not set up for this grid and mechanism");
+    if (rc != 0) throw CudaError("surrogate chemistry: the network launch failed", OCFD_ERR_CUDA);
   } else {
     launch_chem_cells(NS, L->hc.N, L->f, L->Et[L->cur], L->T, L->p, L->di, dt2, nsub, &L->sdev->newton_fail, L->st);
   }
@@ -885,6 +887,10 @@ int check_status() {
     g_err = e == OCFD_ERR_NEGATIVE_ET ? "Number of Negative Temperature Points > Limit (10)" : "device error";
     return e;
   }
+  if (L->chem_mode == 1 && sg_device_error(L->st)) {
+    g_err = "surrogate chemistry: a bounded wait of the network kernel ran out";
+    return OCFD_ERR_TIMEOUT;
+  }
   if (L->shost->chem_bad) {
     const int nb = L->shost->chem_bad;
     CK(cudaMemsetAsync(&L->sdev->chem_bad, 0, sizeof(int), L->st));
@@ -987,6 +993,13 @@ void fill_trans(DevConst& c, const ocfd_transport* tr, int ns) {
       c.wk_b[k][j] = std::sqrt(8.0 * (1.0 + c.Mi[k] / c.Mi[j]));
       c.wk_c[k][j] = std::sqrt(c.wk_a[k][j]);
       c.wk_binv[k][j] = 1.0 / c.wk_b[k][j];
+    }
+  int np = 0;
+  for (int a = 0; a < ns; a++)
+    for (int b = a + 1; b < ns; b++) {
+      c.pair_a[np] = (unsigned char)a;
+      c.pair_b[np] = (unsigned char)b;
+      np++;
     }
 }
 

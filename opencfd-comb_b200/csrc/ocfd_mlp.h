@@ -42,6 +42,8 @@ struct MlpArgs {
 constexpr int MLP_PACK_BYTES = (2 + 2 * 16) * 8192;  // W0, 16 + 16 chunks of W1 / W2, W3
 // packs the weights (launch on the same stream before the kernel), then runs the kernel
 int launch_mlp_fused(const MlpArgs& a, cudaStream_t st);
+// one-time kernel attribute set-up of the fused kernel (call outside stream capture)
+int prepare_mlp_fused();
 
 }  // namespace mlp
 }  // namespace ocfd

@@ -579,8 +579,8 @@ struct Cells {
 Cells CS;
 
 template <int NS>
-void cells_chem_t(double* f, double* Et, double* T, double* p, double* di, double dt2, int nsub, int* nfail,
-                  cudaStream_t st) {
+int cells_chem_t(double* f, double* Et, double* T, double* p, double* di, double dt2, int nsub, int* nfail,
+                 cudaStream_t st) {
   const long long N = CS.N;
   cudaMemsetAsync(CS.count, 0, 8 * sizeof(int), st);
   Gemm gemm;
@@ -590,15 +590,18 @@ void cells_chem_t(double* f, double* Et, double* T, double* p, double* di, doubl
     k_cell_inputs<NS><<<nb(rows, 128), 128, 0, st>>>((int)c0, rows, di, Et, dt2 * nsub, S.d_norm, S.nin, CS.raw,
                                                     CS.T0, CS.xb, nfail);
     forward(gemm, rows, CS.xb, hs, nullptr, CS.out, st);
+    if (gemm.rc) return gemm.rc;  // the network did not run: its outputs would be stale
     k_cell_post<NS><<<nb(rows, 128), 128, 0, st>>>((int)c0, rows, f, Et, T, p, di, CS.T0, CS.raw, CS.out, S.d_norm,
                                                   S.d_proj, CS.tol, CS.list, CS.count, nfail);
   }
   k_chem_cells_list<NS><<<nb(N, OCFD_CHEM_TPB), OCFD_CHEM_TPB, 0, st>>>(CS.list, CS.count, f, Et, T, p, di, dt2, nsub, nfail);
+  return 0;
 }
 
 // mode 1: allocate the chunk buffers for N cells (called outside any stream capture)
 int cells_setup(long long N, double tol) {
   if (!S.trained) return -5;
+  if (g_fused && mlp::prepare_mlp_fused() != 0) return -2;
   if (CS.N != N) {
     void* ptrs[] = {CS.raw, CS.T0, CS.xb, CS.hA, CS.hB, CS.out, CS.list, CS.count};
     for (void* q : ptrs)
@@ -623,8 +626,19 @@ int sg_cells_chem(int ns, double* f, double* Et, double* T, double* p, double* d
                   cudaStream_t st) {
   using namespace sg;
   if (!S.trained || S.ns != ns || CS.N <= 0) return -5;
-  SG_DISPATCH(ns, cells_chem_t<NSC>(f, Et, T, p, di, dt2, nsub, nfail, st));
-  return 0;
+  int rc = 0;
+  SG_DISPATCH(ns, rc = cells_chem_t<NSC>(f, Et, T, p, di, dt2, nsub, nfail, st));
+  return rc;
+}
+// 1 when a network kernel ran out of a bounded wait since the last call (the word is cleared)
+int sg_device_error(cudaStream_t st) {
+  using namespace sg;
+  if (!S.d_err) return 0;
+  int h = 0;
+  cudaMemcpyAsync(&h, S.d_err, sizeof(int), cudaMemcpyDeviceToHost, st);
+  cudaStreamSynchronize(st);
+  if (h) cudaMemsetAsync(S.d_err, 0, sizeof(int), st);
+  return h ? 1 : 0;
 }
 int sg_cells_setup(int ns, long long N, double tol) {
   using namespace sg;

@@ -33,4 +33,6 @@ def main(ref):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit("usage: python make_data.py <path of the OpenCFD-Comb source tree (holds cases/jet)>")
+    main(sys.argv[1])

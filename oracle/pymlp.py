@@ -24,20 +24,19 @@ def bf16(a):
 K2 = 2.0 * math.sqrt(2.0 / math.pi)  # 2 sqrt(2 / pi)
 
 
-def _sig2u(x):
-    """sigmoid(2 u), u = sqrt(2 / pi) (x + 0.044715 x^3)"""
-    with np.errstate(over="ignore"):
-        return 1.0 / (1.0 + np.exp(-K2 * x * (1.0 + 0.044715 * x * x)))
+def _tanh_u(x):
+    """tanh(u), u = sqrt(2 / pi) (x + 0.044715 x^3)"""
+    return np.tanh(0.5 * K2 * x * (1.0 + 0.044715 * x * x))
 
 
 def gelu(x):
-    """GELU in its tanh form, 0.5 x (1 + tanh(u)) = x sigmoid(2 u)."""
-    return x * _sig2u(x)
+    """GELU in its tanh form, 0.5 x (1 + tanh(u)) (the GPU evaluates tanh in hardware)."""
+    return 0.5 * x * (1.0 + _tanh_u(x))
 
 
 def gelu_grad(x):
-    s = _sig2u(x)
-    return s + x * s * (1.0 - s) * K2 * (1.0 + 3.0 * 0.044715 * x * x)
+    t = _tanh_u(x)
+    return 0.5 * (1.0 + t) + 0.5 * x * (1.0 - t * t) * 0.5 * K2 * (1.0 + 3.0 * 0.044715 * x * x)
 
 
 def unpack(blob):
