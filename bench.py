@@ -47,6 +47,10 @@ def parse():
     ap.add_argument("--steps", type=int, default=40)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--lib", default="fma", choices=["fma", "exact"],
+                    help="library build: fma = contracted multiply-adds (libocfd_gpu_fma.so, checked against the "
+                         "CPU restatement to 1e-10 after ten steps with identical HYBRID decisions), exact = "
+                         "--fmad=false (libocfd_gpu.so, bit-identical to it where no transcendental enters)")
     ap.add_argument("--workload", default="jet", choices=["jet", "flatplate", "isotropic", "reactors", "surrogate"],
                     help="jet = the metric's configuration (384x256x256 reacting H2 jet, plain FP64 and gated "
                          "surrogate chemistry); flatplate, isotropic, reactors and surrogate are the other "
@@ -793,6 +797,7 @@ def main_jet(a):
                "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
                "value_form": "plain FP64 chemistry (implicit Euler + Gauss, the reference's integrator)",
                "config": {"workload": name, "cells_per_gpu": N, "dt": dt, "steps_per_run": total,
+                          "library": os.path.basename(solver.LIBPATH),
                           "chemistry": "plain FP64 implicit Euler, %d sub-step per step; surrogate run: gated BF16 "
                                        "MLP with FP64 fallback" % nsub,
                           "parallelism": "replicas x%d (no data-path collective)" % ranks.world,
@@ -920,7 +925,8 @@ def main_ours(a):
         out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps,
                "warmup": a.warmup, "ms_per_step": el_ms / a.steps, "higher_is_better": True, "scaling": "weak",
                "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
-               "config": {"workload": name, "cells_per_gpu": c.ncell, "dt": dt, "chemistry": ("plain FP64 implicit Euler, %d sub-step(s) per step" % nsub) if reac else "off (non-reacting air)",
+               "config": {"workload": name, "cells_per_gpu": c.ncell, "dt": dt,
+                          "library": os.path.basename(solver.LIBPATH), "chemistry": ("plain FP64 implicit Euler, %d sub-step(s) per step" % nsub) if reac else "off (non-reacting air)",
                           "parallelism": "replicas x%d (no data-path collective)" % world,
                           "tiles": tiles,
                           "l2": "device state %.1f GB per GPU >> 126 MB L2; no flush between steps" % state_gb},
@@ -933,6 +939,7 @@ def main_ours(a):
 
 if __name__ == "__main__":
     a = parse()
+    os.environ["OCFD_B200_LIB"] = a.lib  # read when ocfd_b200.solver is first imported
     if a.sg_epochs is None:
         a.sg_epochs = 6 if a.workload == "surrogate" else 20
     if a.impl == "reference":

@@ -482,4 +482,242 @@ __global__ void __launch_bounds__(OCFD_CHEM_TPB, OCFD_CHEM_MINB) k_chem_batch(in
   }
 }
 
+// ---- warp-cooperative implicit Euler (batched reactors) ----
+// The same linearised backward-Euler step, one reactor per group of NS lanes (lane s of a group
+// owns species s: its density, row s of the matrix and of the right-hand side); 32 / NS reactors per
+// warp. The reactions are spread over the group's lanes (lane s evaluates reactions s, s + NS, ...)
+// and their rates of progress exchanged through shared memory; each lane then accumulates its own
+// row of the Jacobian in registers, over the reactions in order, with the serial kernel's
+// expressions; the pivot search, the row swap and the pivot row of the Gauss elimination go through
+// shared memory, and the back substitution keeps the serial order. Every value is formed by the same
+// operations in the same order as in chem_step, so both kernels give the same numbers bit for bit.
+// Per reactor it has a fraction of the serial kernel's latency per sub-step, which decides the time
+// of a batch too small to fill the GPU (a few stiff reactors with many sub-steps, such as the
+// reactors the surrogate's gate rejects: the gated pass of 2^20 reactor states 9.45 -> 4.65 ms);
+// its throughput on batches that fill the GPU is a fifth of the serial kernel's, which therefore
+// keeps those (launch_chem_batch picks by the batch size).
+// The group's lanes run warp-synchronously: every lane of the warp executes every sub-step (a warp
+// loops to the largest sub-step count of its reactors; reactors with fewer sub-steps, and the idle
+// lanes above 32 / NS groups, compute without keeping the result).
+template <int NS>
+struct CoopArea {
+  double d[NS], rc[NS], gi[NS], col[NS], x[NS], dn[NS];
+  double rowA[NS + 1], rowB[NS + 1], piv[NS + 1];
+  double wf[OCFD_MAX_REAC], wr[OCFD_MAX_REAC];
+};
+constexpr int COOP_THREADS = 64;  // two warps: the areas of 32 / NS reactors per warp stay small
+
+template <int NS>
+__device__ __forceinline__ void coop_implicit_step(CoopArea<NS>& A, int s, double& d_own, double& E, double dt,
+                                                   bool live, bool& zero, int* nfail) {
+  // every lane of the group gathers the reactor's densities
+  A.d[s] = d_own;
+  __syncwarp();
+  double d[NS];
+#pragma unroll
+  for (int k = 0; k < NS; k++) d[k] = A.d[k];
+  const double T = dev_T<NS>(d, E, (live && s == 0) ? nfail : nullptr);
+  double ci[NS];
+#pragma unroll
+  for (int i = 0; i < NS; i++) ci[i] = d[i] / cC.Mi[i] * 1.0e-6;
+  const double lt = log(T), rT = 1.0 / T;
+  A.rc[s] = 1.0 / (ci[s] + 1.0e-20);
+  if (cC.rereac == 0) A.gi[s] = dev_gibbs_jc(s, trange(T), T, lt);
+  __syncwarp();
+  double gi[NS];
+#pragma unroll
+  for (int i = 0; i < NS; i++) gi[i] = A.gi[i];
+  // the group's reactions, spread over its lanes
+  for (int k = s; k < cC.nreac; k += NS) {
+    double w, r, wf1, wr1;
+    rate_coef_j<NS>(k, ci, gi, T, lt, rT, w, r);
+    progress<NS>(ci, w, r, k, wf1, wr1);
+    A.wf[k] = wf1;
+    A.wr[k] = wr1;
+  }
+  __syncwarp();
+  double rc[NS];
+#pragma unroll
+  for (int j = 0; j < NS; j++) rc[j] = A.rc[j];
+  // row s of Reaction_rate_and_Matrix, reactions in order
+  double ri = 0.0, row[NS];
+#pragma unroll
+  for (int j = 0; j < NS; j++) row[j] = 0.0;
+  for (int k = 0; k < cC.nreac; k++) {
+    const double wf1 = A.wf[k], wr1 = A.wr[k];
+    const double si = (double)(cC.vr[k][s] - cC.vf[k][s]);
+    ri = ri + (wf1 - wr1) * si;
+#pragma unroll
+    for (int j = 0; j < NS; j++) {
+      const int a = cC.vf[k][j], b = cC.vr[k][j];
+      if (a == 0 && b == 0) continue;
+      const double dA = (double)a * wf1 * rc[j] - (double)b * wr1 * rc[j];
+      row[j] = row[j] + dA * si;
+    }
+  }
+#pragma unroll
+  for (int j = 0; j < NS; j++) {
+    const double a = (s == j) ? 1.0 : 0.0;
+    row[j] = a - row[j] * cC.mratio[s][j] * dt;
+  }
+  double rhs = ri * cC.Mi[s] * 1.0e6 * dt;
+  // Gauss elimination with partial pivoting across the group's rows
+#pragma unroll
+  for (int k = 0; k < NS - 1; k++) {
+    A.col[s] = fabs(row[k]);
+    __syncwarp();
+    double fmax = A.col[k];
+    int kk = k;
+#pragma unroll
+    for (int i = k + 1; i < NS; i++) {
+      const double v = A.col[i];
+      if (v > fmax) {
+        fmax = v;
+        kk = i;
+      }
+    }
+    zero = zero || fmax == 0.0;
+    if (kk != k) {  // rows k and kk trade places (columns >= k and the right-hand side)
+      if (s == k) {
+#pragma unroll
+        for (int j = k; j < NS; j++) A.rowA[j] = row[j];
+        A.rowA[NS] = rhs;
+      }
+      if (s == kk) {
+#pragma unroll
+        for (int j = k; j < NS; j++) A.rowB[j] = row[j];
+        A.rowB[NS] = rhs;
+      }
+    }
+    __syncwarp();
+    if (kk != k) {
+      if (s == k) {
+#pragma unroll
+        for (int j = k; j < NS; j++) row[j] = A.rowB[j];
+        rhs = A.rowB[NS];
+      }
+      if (s == kk) {
+#pragma unroll
+        for (int j = k; j < NS; j++) row[j] = A.rowA[j];
+        rhs = A.rowA[NS];
+      }
+    }
+    if (s == k) {
+#pragma unroll
+      for (int j = k; j < NS; j++) A.piv[j] = row[j];
+      A.piv[NS] = rhs;
+    }
+    __syncwarp();
+    if (s > k) {
+      const double f = -row[k] / A.piv[k];
+#pragma unroll
+      for (int j = k; j < NS; j++) row[j] = row[j] + f * A.piv[j];
+      rhs = rhs + f * A.piv[NS];
+    }
+    __syncwarp();
+  }
+  // back substitution in the serial order: x(NS-1), then x(i) = (b(i) - sum_j>i a(i,j) x(j)) / a(i,i)
+  if (s == NS - 1) A.x[NS - 1] = rhs / row[NS - 1];
+  __syncwarp();
+#pragma unroll
+  for (int i = NS - 2; i >= 0; i--) {
+    if (s == i) {
+      double sacc = rhs;
+#pragma unroll
+      for (int j = i + 1; j < NS; j++) sacc = sacc - row[j] * A.x[j];
+      A.x[i] = sacc / row[i];
+    }
+    __syncwarp();
+  }
+  {
+    // the last pivot's test (made by lane NS-1 above) for the whole group
+    A.col[s] = (s == NS - 1 && row[NS - 1] == 0.0) ? 1.0 : 0.0;
+    __syncwarp();
+    zero = zero || A.col[NS - 1] != 0.0;
+  }
+  const double dn = d_own + A.x[s];
+  A.dn[s] = dn;
+  __syncwarp();
+  double En = E;
+#pragma unroll
+  for (int i = 0; i < NS; i++) En = En - (A.dn[i] - d[i]) * cC.Ri[i] * cC.cf[i][0][5];
+  __syncwarp();  // the area is rewritten by the next sub-step
+  if (live) {
+    d_own = dn;
+    E = En;
+  }
+}
+
+template <int NS, bool CP>
+__global__ void __launch_bounds__(COOP_THREADS) k_chem_batch_coop(int n, double* di, double* e, const double* dt,
+                                                                  const int* nsub, const int* perm, int* counter,
+                                                                  int* nfail) {
+  constexpr int G = 32 / NS;  // reactors per warp
+  __shared__ CoopArea<NS> area[COOP_THREADS / 32][G + 1];  // the last area is the idle lanes' sink
+  const int lane = threadIdx.x & 31, wq = threadIdx.x >> 5;
+  const int g = lane / NS, s = lane - g * NS;
+  const bool lane_ok = g < G;
+  CoopArea<NS>& A = area[wq][lane_ok ? g : G];
+  for (;;) {
+    int base = 0;
+    if (lane == 0) base = atomicAdd(counter, G);
+    base = __shfl_sync(0xffffffffu, base, 0);
+    if (base >= n) break;
+    const int idx = base + g;
+    const bool act = lane_ok && idx < n;
+    const int r = act ? perm[idx] : 0;
+    const int ks = act ? (nsub ? nsub[r] : 1) : 0;
+    int kmax = ks;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) kmax = max(kmax, __shfl_xor_sync(0xffffffffu, kmax, o));
+    const double dt2 = act ? dt[r] / ks : 0.0;
+    double d_own = act ? di[(size_t)r * NS + s] : 1.0;
+    double E = act ? e[r] : 1.0;
+    double h0 = 0.0, p0 = 0.0;
+    int* nf0 = (act && s == 0) ? nfail : nullptr;  // one lane per reactor counts Newton failures
+    if (CP) {
+      A.d[s] = d_own;
+      __syncwarp();
+      double d[NS];
+#pragma unroll
+      for (int k = 0; k < NS; k++) d[k] = A.d[k];
+      __syncwarp();
+      cp_reference<NS>(d, E, h0, p0, nf0);
+    }
+    bool zero = false;
+    for (int st = 0; st < kmax; st++) {
+      const bool live = act && st < ks;
+      coop_implicit_step<NS>(A, s, d_own, E, dt2, live, zero, nfail);
+      if (CP) {
+        A.d[s] = d_own;
+        __syncwarp();
+        double d[NS];
+#pragma unroll
+        for (int k = 0; k < NS; k++) d[k] = A.d[k];
+        __syncwarp();
+        double Ec = E;
+        cp_restore<NS>(d, Ec, h0, p0, live ? nf0 : nullptr);
+        if (live) {
+          d_own = d[s];
+          E = Ec;
+        }
+      }
+    }
+    // error check of the reactor: zero pivot or a non-finite density / energy in the group
+    A.col[s] = (isfinite(d_own) && isfinite(E)) ? 0.0 : 1.0;
+    __syncwarp();
+    bool bad = zero;
+#pragma unroll
+    for (int k = 0; k < NS; k++) bad = bad || A.col[k] != 0.0;
+    __syncwarp();
+    if (act) {
+      di[(size_t)r * NS + s] = d_own;
+      if (s == 0) {
+        e[r] = E;
+        if (bad && nfail) atomicAdd(nfail + 1, 1);
+      }
+    }
+  }
+}
+
 }  // namespace ocfd

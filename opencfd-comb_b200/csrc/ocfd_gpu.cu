@@ -100,6 +100,11 @@ struct Lib {
   // second stream of a stage: k_visc_ev and its halo exchange run beside the flux sweeps
   cudaStream_t st2 = nullptr;
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+  // third stream of a stage with species (N_SPEC > 1): the species sweeps, the species viscous
+  // divergence and the species RK update run beside the transport, Qp and flow kernels
+  cudaStream_t st3 = nullptr;
+  cudaEvent_t ev_sp_fork = nullptr, ev_se_done = nullptr, ev_sp_join = nullptr;
+  bool fork_species = true;
   bool fork_visc = true;
   cudaGraph_t gstep = nullptr;
   int* ht_counter = nullptr;
@@ -524,14 +529,54 @@ void stage_t(int krk, double dt1) {
     exchange({L->Rh}, 7);
   }
   FluxArgs fa = flow_flux_args();
-  if (NS > 1) {
-    // every species at once (du_scaler_invis / du_scaler_viscous / Scalar_time_adv_RK3 of the
-    // reference's species loop): Dus of species m is dus + m N
+  // Species (every species at once: du_scaler_invis / du_scaler_viscous / Scalar_time_adv_RK3 of
+  // the reference's species loop; Dus of species m is dus + m N). The species sweeps read only di
+  // and the velocities and write only Dus, and nothing of the flow part reads di, so the sweeps,
+  // the species divergence (after the species viscous fluxes) and the species RK update run on a
+  // third stream beside k_ci / k_scal_ev and the flow part (branches of the step's graph), joined
+  // before k_rk_prims, which reads the updated di. Each kernel writes what it wrote before, so the
+  // results do not depend on the overlap. The per-kernel timing mode keeps everything in order.
+  const bool spfork = NS > 1 && L->fork_species && !L->prof && L->st3;
+  auto on_st3 = [&](auto&& body) {  // launches of body go to the third stream
+    std::swap(L->st, L->st3);
+    try {
+      body();
+    } catch (...) {
+      std::swap(L->st, L->st3);
+      throw;
+    }
+    std::swap(L->st, L->st3);
+  };
+  const bool sp_visc = NS > 1 && L->P.if_viscous == 1;
+  auto species_sweeps = [&]() {
     const int grp = NS % 3 == 0 ? 3 : 1;
-    fa.fs = L->di;
-    fa.out = L->dus;
-    for (int dd = 0; dd < 3; dd++) launch_flux(dd, fa, grp, NS / grp);
-    if (L->P.if_viscous == 1) {
+    FluxArgs fs = fa;
+    fs.fs = L->di;
+    fs.out = L->dus;
+    for (int dd = 0; dd < 3; dd++) launch_flux(dd, fs, grp, NS / grp);
+  };
+  auto species_div_rk = [&]() {
+    if (sp_visc) {
+      KTimer t(KC_SPECIES_VISC);
+      if (L->sep) k_scal_div<NS, true><<<nblk(N, 32), dim3(32, NS), 0, L->st>>>(L->se[0], L->se[1], L->se[2], L->dus, L->geo);
+      else k_scal_div<NS, false><<<nblk(N, 32), dim3(32, NS), 0, L->st>>>(L->se[0], L->se[1], L->se[2], L->dus, L->geo);
+      LAUNCH_CHECK();
+    }
+    {
+      KTimer t(KC_SPECIES_RK);
+      k_scal_rk<<<dim3(nblk(N, 256), NS), 256, 0, L->st>>>(krk, dt1, L->dus, L->din, L->di);
+      LAUNCH_CHECK();
+    }
+  };
+  if (NS > 1) {
+    if (spfork) {
+      CK(cudaEventRecord(L->ev_sp_fork, L->st));
+      CK(cudaStreamWaitEvent(L->st3, L->ev_sp_fork, 0));
+      on_st3(species_sweeps);
+    } else {
+      species_sweeps();
+    }
+    if (sp_visc) {
       {
         KTimer t(KC_SPECIES_VISC);
         k_ci<<<dim3(nblk(H, 256), NS), 256, 0, L->st>>>(L->di, L->d, L->ci, H);
@@ -545,20 +590,22 @@ void stage_t(int krk, double dt1) {
         for (int m = 0; m < NS; m++) fl.push_back(L->se[dd] + (size_t)m * H);
         exchange_v(fl, 1 << dd);
       }
-      KTimer t(KC_SPECIES_VISC);
-      if (L->sep) k_scal_div<NS, true><<<nblk(N, 32), dim3(32, NS), 0, L->st>>>(L->se[0], L->se[1], L->se[2], L->dus, L->geo);
-      else k_scal_div<NS, false><<<nblk(N, 32), dim3(32, NS), 0, L->st>>>(L->se[0], L->se[1], L->se[2], L->dus, L->geo);
-      LAUNCH_CHECK();
     }
-    {
-      KTimer t(KC_SPECIES_RK);
-      k_scal_rk<<<dim3(nblk(N, 256), NS), 256, 0, L->st>>>(krk, dt1, L->dus, L->din, L->di);
-      LAUNCH_CHECK();
+    if (spfork) {
+      CK(cudaEventRecord(L->ev_se_done, L->st));
+      on_st3([&]() {
+        CK(cudaStreamWaitEvent(L->st, L->ev_se_done, 0));
+        species_div_rk();
+        CK(cudaEventRecord(L->ev_sp_join, L->st));
+      });
+    } else {
+      species_div_rk();
     }
   }
   fa.fs = nullptr;
   fa.out = L->du;
   flow_rhs_t<NS>(fa);
+  if (spfork) CK(cudaStreamWaitEvent(L->st, L->ev_sp_join, 0));
   // N_SPEC = 1: di = d over the whole array (OCFD_Time_Adv.f90:45-52). Nothing between the stage
   // start and here reads di, and the inline transport of k_visc_ev must see the previous stage's
   // di (comput_Amu_Amk_AMD runs before the copy in the reference), so the copy happens here.
@@ -1037,6 +1084,10 @@ void release() {
   if (L->ev_fork) cudaEventDestroy(L->ev_fork);
   if (L->ev_join) cudaEventDestroy(L->ev_join);
   if (L->st2) cudaStreamDestroy(L->st2);
+  if (L->ev_sp_fork) cudaEventDestroy(L->ev_sp_fork);
+  if (L->ev_se_done) cudaEventDestroy(L->ev_se_done);
+  if (L->ev_sp_join) cudaEventDestroy(L->ev_sp_join);
+  if (L->st3) cudaStreamDestroy(L->st3);
   if (L->st) cudaStreamDestroy(L->st);
   delete L;
   L = nullptr;
@@ -1266,6 +1317,7 @@ namespace ocfd {
 // for the surrogate module
 int current_nspec() { return L && L->have_kin ? L->NS : 0; }
 int current_const_p() { return L && L->have_kin ? L->hc.const_p : 0; }
+int current_timeadv() { return L ? L->hc.timeadv : 0; }
 cudaStream_t current_stream() { return L ? L->st : nullptr; }
 }  // namespace ocfd
 
@@ -1346,6 +1398,10 @@ int ocfd_gpu_init(const ocfd_params* p, const ocfd_thermo* th, const ocfd_kineti
     CK(cudaStreamCreateWithFlags(&L->st2, cudaStreamNonBlocking));
     CK(cudaEventCreateWithFlags(&L->ev_fork, cudaEventDisableTiming));
     CK(cudaEventCreateWithFlags(&L->ev_join, cudaEventDisableTiming));
+    CK(cudaStreamCreateWithFlags(&L->st3, cudaStreamNonBlocking));
+    CK(cudaEventCreateWithFlags(&L->ev_sp_fork, cudaEventDisableTiming));
+    CK(cudaEventCreateWithFlags(&L->ev_se_done, cudaEventDisableTiming));
+    CK(cudaEventCreateWithFlags(&L->ev_sp_join, cudaEventDisableTiming));
     DevConst& c = L->hc;
     c.nx = p->nx; c.ny = p->ny; c.nz = p->nz; c.ns = p->n_spec;
     c.HX = p->nx + 2 * OCFD_L; c.HY = p->ny + 2 * OCFD_L; c.HZ = p->nz + 2 * OCFD_L;
