@@ -642,8 +642,23 @@ def jet_roofline(prof, nsteps, ncell):
         if dom in tr:  # per launch; the file holds one stage's bytes for the classes of several launches
             per_stage = dom in ("species_flux", "species_visc")
             traffic = tr[dom] * ncell / (launches / JET_STAGES_PER_STEP if per_stage else 1.0)
+    # the same class against the measured FP64 peak (FMA = 2 FLOP), with the executed FP64 operations
+    # per cell that ncu counted for it (the kernels of this path are FP64-issue or latency bound)
+    fp64 = None
+    ffile = os.path.join(ROOT, "profiles", "fp64_flops_per_cell_jet.json")
+    if os.path.exists(ffile):
+        from ocfd_b200 import solver
+        with open(ffile) as fh:
+            fl = json.load(fh)
+        if dom in fl:
+            per_stage = dom in ("species_flux", "species_visc")
+            flops_step = fl[dom] * ncell * (JET_STAGES_PER_STEP if per_stage else launches)
+            ach = flops_step / (d["ms_per_step"] * 1e-3) / 1e9
+            pk = solver.fp64_peak_gflops()
+            fp64 = {"achieved": round(ach, 1), "peak": round(pk, 1), "unit": "GFLOP/s", "frac": round(ach / pk, 4),
+                    "flops_per_step": flops_step, "peak_kind": "measured FP64 FMA loop (FMA = 2 FLOP)"}
     return {"bound": "hbm", "kernel": dom, "achieved": d["achieved_gbs"], "peak": hbm, "unit": "GB/s",
-            "frac": d["frac"], "traffic": traffic, "peak_kind": hbm_kind,
+            "frac": d["frac"], "traffic": traffic, "peak_kind": hbm_kind, "fp64": fp64,
             "alg_bytes_per_launch": d["alg_bytes_per_step"] / launches,
             "avg_launch_ms": d["ms_per_step"] / launches, "share_of_step": d["share_of_step"],
             "note": "a class of several kernels (species_flux, species_visc) counts one stage's launches "

@@ -819,32 +819,18 @@ __global__ void __launch_bounds__(32 * NS, OCFD_SPECIES_MINB) k_scal_ev(const do
                                                      const double* amd, double* qpx, double* qpy, double* qpz,
                                                      double* e1, double* e2, double* e3, Geo g) {
   __shared__ double sq[3][NS][32];
-  __shared__ double sm[18][32];  // Akx..Asz and Akx1..Asz1 of the block's 32 cells
   const int ks = threadIdx.y, lane = threadIdx.x;
   int i, j, k;
   const bool ok = cell_of((long long)blockIdx.x * 32 + lane, i, j, k);
-  // the metrics of a cell are the same for every species: one thread per cell evaluates them
-  if (ok && ks == 0) {
-    double A[9], A1[9];
-    metric_all<SEP>(g, i, j, k, hidx(i, j, k), A, A1);
-#pragma unroll
-    for (int m = 0; m < 9; m++) {
-      sm[m][lane] = A[m];
-      sm[9 + m][lane] = A1[m];
-    }
-  }
-  __syncthreads();
   int nn = 0;
   if (ok) {
     const int q = hidx(i, j, k);
     nn = nidx(i, j, k);
     const long long H = cC.H, N = cC.N;
+    // every species' thread evaluates its cell's metrics (the same values): the FP64 pipe has room
+    // for the repeated work, and the block does not wait for one warp at a barrier
     double A[9], A1[9];
-#pragma unroll
-    for (int m = 0; m < 9; m++) {
-      A[m] = sm[m][lane];
-      A1[m] = sm[9 + m][lane];
-    }
+    metric_all<SEP>(g, i, j, k, q, A, A1);
     const double* c = ci + (size_t)ks * H;
     double uk = cdiff(c, q, 0, i, cC.nx), ui = cdiff(c, q, 1, j, cC.ny), us = cdiff(c, q, 2, k, cC.nz);
     double hi = dev_hi(ks, T[q]);
@@ -885,18 +871,16 @@ __global__ void __launch_bounds__(32 * NS, OCFD_SPECIES_MINB) k_scal_ev(const do
 template <int NS, bool SEP>
 __global__ void __launch_bounds__(32 * NS, OCFD_SCAL_DIV_MINB) k_scal_div(const double* e1, const double* e2,
                                                                           const double* e3, double* dus, Geo g) {
-  __shared__ double sjac[32];
   const int ks = threadIdx.y;
   int i, j, k;
   const bool ok = cell_of((long long)blockIdx.x * 32 + threadIdx.x, i, j, k);
-  if (ok && ks == 0) sjac[threadIdx.x] = metric_jac<SEP>(g, i, j, k, hidx(i, j, k));  // once per cell
-  __syncthreads();
   if (!ok) return;
   const int q = hidx(i, j, k), nn = nidx(i, j, k);
+  const double jac = metric_jac<SEP>(g, i, j, k, q);  // every species' thread (no barrier)
   const size_t o = (size_t)ks * cC.H;
   double uk = cdiff(e1 + o, q, 0, i, cC.nx), ui = cdiff(e2 + o, q, 1, j, cC.ny), us = cdiff(e3 + o, q, 2, k, cC.nz);
   double* du = dus + (size_t)ks * cC.N + nn;
-  *du = *du + (uk + ui + us) * sjac[threadIdx.x];
+  *du = *du + (uk + ui + us) * jac;
 }
 // Scalar_time_adv_RK3 (OCFD_Time_Adv.f90:134-166), blockIdx.y = species
 static __global__ void k_scal_rk(int krk, double dt, const double* dus, const double* din, double* di) {

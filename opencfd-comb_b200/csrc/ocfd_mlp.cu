@@ -246,13 +246,14 @@ int launch_gemm(const GemmArgs& g, cudaStream_t st) {
 // back to shared memory in the K-major layout, where they are the next layer's A operand, so only
 // the 16 inputs and 16 outputs of a row touch global memory. The weights are packed beforehand
 // (k_pack_mlp) into the exact shared-memory image of each 16-wide K chunk, so one thread brings a
-// chunk in with a single bulk copy whose completion lands on a transaction mbarrier: four chunk
-// buffers keep three chunks in flight while an MMA runs, and the next layer's first chunks are
-// fetched during the current epilogue. All CTAs read the same 272 KB of packed weights, which stay
+// chunk in with a single bulk copy whose completion lands on a transaction mbarrier: five chunk
+// buffers keep three chunks in flight ahead of the MMA being issued, a buffer being refilled two
+// chunks after its MMA was issued (so the issue of the next MMA never waits for the previous one to
+// complete), and the next layer's first chunks are fetched during the current epilogue. All CTAs read the same 272 KB of packed weights, which stay
 // in L2. Each layer issues the same K = 16 MMAs in the same order as the layer-by-layer GEMMs and
 // the epilogues evaluate the same expressions.
 namespace fused {
-constexpr int MT = 128, THR = 256, KCH = 16, NKC = 256 / KCH, NBUF = 4, CHUNK = 256 * KCH * 2;
+constexpr int MT = 128, THR = 256, KCH = 16, NKC = 256 / KCH, NBUF = 5, CHUNK = 256 * KCH * 2;
 constexpr int ACT_BYTES = MT * 256 * 2, X_BYTES = MT * 16 * 2, BIAS_BYTES = (3 * 256 + 16) * 4;
 constexpr int BYTES = ACT_BYTES + X_BYTES + NBUF * CHUNK + BIAS_BYTES + 128;
 static_assert(2 * BYTES <= 226 * 1024, "two blocks per SM");
@@ -344,7 +345,7 @@ __global__ void __launch_bounds__(fused::THR, 2) k_mlp_fused(MlpArgs a) {
   tc::fence_after();
   const uint32_t tmem = *tslot;
   // thread 0 drives the pipeline: completions of each barrier waited for so far
-  int ntb[NBUF] = {0, 0, 0, 0}, nmb[NBUF] = {0, 0, 0, 0};
+  int ntb[NBUF] = {}, nmb[NBUF] = {};
   bool ok = true;
   auto buf = [&](int c) { return wbase + (c % NBUF) * CHUNK; };
   auto fetch = [&](int c, int off) {  // chunk image at pack + off into buffer c % NBUF
@@ -421,9 +422,12 @@ __global__ void __launch_bounds__(fused::THR, 2) k_mlp_fused(MlpArgs a) {
         const uint64_t bd = tc::smem_desc(tc::smem_u32(buf(c)), 256 * 16, 128);
         tc::mma_bf16(tmem, ad, bd, id256, c > 0 ? 1u : 0u);
         tc::mma_commit(tc::smem_u32(&mb[b]));
-        const int nx = c + NBUF - 1;  // refill the buffer of chunk c - 1 once its MMA is done
-        if (nx < NKC) {
-          if (c >= 1) ok = wait_m((c - 1) % NBUF);
+        // refill the buffer of chunk c - 2 with chunk c + NBUF - 2: that MMA has (almost always)
+        // finished by now, so the wait does not hold the issue of the next MMA behind an mbarrier
+        // round trip, as waiting for chunk c - 1 did (chunk NBUF - 1 goes to the unused last buffer)
+        const int nx = c + NBUF - 2;
+        if (c >= 1 && nx < NKC) {
+          if (c >= 2) ok = wait_m((c - 2) % NBUF);
           if (ok) fetch(nx, pack_chunk(l, nx));
         }
       }
