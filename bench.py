@@ -714,7 +714,9 @@ def main_jet(a):
     tiles = {"mode": a.tiles, "choice": g.tiles()}
     if a.tiles == "auto":
         choice, tms = g.autotune(reps=5)
-        tiles = {"mode": "auto", "choice": choice}
+        tiles = {"mode": "auto", "choice": choice,
+                 "flow_rhs_visc_after_beside_ms": tms[23:25],
+                 "stage_rhs_species_in_order_beside_ms": tms[25:27]}
     elif a.tiles != "default":
         g.set_tiles([int(x) for x in a.tiles.split(",")])
         tiles = {"mode": "given", "choice": g.tiles()}
@@ -859,10 +861,11 @@ def main_ours(a):
                                   "visc_ev_kc8_16_32_64": tms[9:13],
                                   "visc_div_kc8_16_32_64_percell": tms[13:18],
                                   "stored_metrics_flux_xyz_ev_div": tms[18:23],
-                                  "flow_rhs_visc_after_beside": tms[23:25]},
+                                  "flow_rhs_visc_after_beside": tms[23:25],
+                                  "stage_rhs_species_in_order_beside": tms[25:27]},
                  "choice_keys": ["flux_x_shape", "flux_y_shape", "flux_z_shape", "visc_ev_kc", "visc_div_kc",
                                  "flux_stored_metrics", "visc_ev_stored_metrics", "visc_div_stored_metrics",
-                                 "visc_ev_second_stream"]}
+                                 "stream_switches (1 visc_ev beside the flux sweeps, 2 species chain on a third stream)"]}
     chk(L.ocfd_gpu_run(dt, tt, a.warmup, reac, nsub))
     tt += a.warmup * dt
 

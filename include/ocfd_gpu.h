@@ -241,6 +241,17 @@ int ocfd_gpu_chem_batch_device(int n, double* d_di, double* d_e, const double* d
  * batches (OCFD_ERR_UNSUPPORTED). */
 int ocfd_gpu_chem_constant_pressure(int on);
 
+/* Compiled mechanism kernels (no counterpart in the reference, which interprets its mechanism
+ * tables in every reaction loop, CHEM_reactions.f90:130-272): the library carries the 9-species
+ * H2-air mechanism of the jet case as straight-line rate and Jacobian code
+ * (opencfd-comb_b200/csrc/ocfd_mech_h2air9.cuh, generated from its data file). When the loaded
+ * mechanism has exactly that structure (species count, reactions, stoichiometry, rate forms,
+ * third-body flags) and CHEM_TimeAdv = -1, the flow step's chemistry and the batched reactors
+ * run it; its numbers equal the generic kernels' bit for bit on finite states. on = 0 keeps the
+ * generic kernels, on = 1 allows the compiled ones (default), on < 0 changes nothing. Returns 1
+ * when the compiled kernels are in use for the current set-up, else 0. */
+int ocfd_gpu_chem_compiled_mechanism(int on);
+
 /* The last batched chemistry call's counts: reactors whose Newton T(E) iteration did not converge
  * (comput_T_rgas, CHEM_thermdyn.f90:327-382, at most 31 iterations) and reactors reported by
  * OCFD_ERR_CHEM (zero pivot or non-finite result). Either pointer may be NULL. */
@@ -287,18 +298,23 @@ int ocfd_gpu_ana_average(int upload, double* fields, int* k_average, double* t_a
  * the viscous-flux kernel and of its divergence kernel; metric form of the flux sweeps, the
  * viscous-flux kernel and the divergence kernel (0 computed from the 1-D grid derivatives of a
  * tensor-product grid, 1 read from the 19 stored arrays, which are then computed once; a general
- * grid always reads them); 1 = the viscous-flux kernel runs beside the flux sweeps on a second
- * stream (a parallel branch of the step's graph), 0 = after them}. Shapes (cells along the sweep x pencils): x 56x4, 120x2, 24x8;
- * y / z 24x16, 24x8, 56x8. Every choice gives bit-identical results.
+ * grid always reads them); stream switches, bit 0: the viscous-flux kernel runs beside the flux
+ * sweeps on a second stream (a parallel branch of the step's graph) instead of after them, bit 1:
+ * the species chain (species sweeps, then divergence and RK update) runs on a third stream beside
+ * the species viscous fluxes and the flow part instead of in order}. Shapes (cells along the
+ * sweep x pencils): x 56x4, 120x2, 24x8; y / z 24x16, 24x8, 56x8. Every choice gives
+ * bit-identical results.
  * ocfd_gpu_autotune times each candidate on the current state (after ocfd_gpu_init_state) over reps
  * launches, applies the fastest and remembers it for this configuration (grid, schemes, species)
  * in the process; reps = 0 applies a remembered choice without timing when there is one. choice
- * (may be NULL) receives the choice; ms (may be NULL, 25 doubles) the mean ms per launch of each
+ * (may be NULL) receives the choice; ms (may be NULL, 27 doubles) the mean ms per launch of each
  * candidate: flux x, y, z shapes 0..2, k_visc_ev at 8, 16, 32, 64 planes, k_visc_div at 8, 16,
  * 32, 64 planes and in its per-cell form (k planes 0), then with the stored metric arrays at the
  * best tiles: flux x, y, z, k_visc_ev, k_visc_div, then the flow right-hand side of a stage with
- * the viscous flux after and beside the flux sweeps (-1 where not timed). The launches write only
- * scratch arrays, so the solution is unchanged. Default choice {0, 0, 0, 16, 16, 0, 0, 0, 1}. */
+ * the viscous flux after and beside the flux sweeps, then a stage's right-hand sides without the
+ * species RK update with the species chain in order and on the third stream (-1 where not timed).
+ * The launches write only scratch arrays, so the solution is unchanged. Default choice
+ * {0, 0, 0, 16, 16, 0, 0, 0, 3}. */
 int ocfd_gpu_autotune(int reps, int* choice, double* ms);
 int ocfd_gpu_set_tiles(const int* choice);
 int ocfd_gpu_get_tiles(int* choice);

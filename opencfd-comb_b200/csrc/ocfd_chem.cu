@@ -6,6 +6,22 @@
 namespace ocfd {
 int current_const_p();  // the batched reactors' form (ocfd_gpu.cu): 1 constant pressure, 0 constant volume
 int current_timeadv();  // CHEM_TimeAdv of the current set-up
+int current_mech();     // the mechanism form of the chemistry kernels (MECH_GENERIC or a compiled one)
+
+int mech_match(const DevConst& c) {
+  namespace m = mech_h2air9;
+  if (c.ns != m::NS || c.nreac != m::NR || c.rereac != m::REREAC) return MECH_GENERIC;
+  for (int j = 0; j < m::NR; j++) {
+    if (c.af_type[j] != m::AF_TYPE[j] || c.tr_reac[j] != m::TR_REAC[j]) return MECH_GENERIC;
+    int sg = 0;
+    for (int i = 0; i < m::NS; i++) {
+      if (c.vf[j][i] != m::VF[j][i] || c.vr[j][i] != m::VR[j][i]) return MECH_GENERIC;
+      sg += m::VR[j][i] - m::VF[j][i];
+    }
+    if (c.sgm[j] != sg) return MECH_GENERIC;
+  }
+  return MECH_H2AIR9;
+}
 
 #define NS_CASES(...)                                          \
   switch (ns) {                                                \
@@ -24,6 +40,10 @@ int current_timeadv();  // CHEM_TimeAdv of the current set-up
 void launch_chem_cells(int ns, long long ncell, double* f, double* Et, double* T, double* p, double* di, double dt2,
                        int nsub, int* nfail, cudaStream_t st) {
   unsigned nb = (unsigned)((ncell + OCFD_CHEM_TPB - 1) / OCFD_CHEM_TPB);
+  if (ns == mech_h2air9::NS && current_timeadv() == -1 && current_mech() == MECH_H2AIR9) {
+    k_chem_cells<mech_h2air9::NS, MECH_H2AIR9><<<nb, OCFD_CHEM_TPB, 0, st>>>(f, Et, T, p, di, dt2, nsub, nfail);
+    return;
+  }
   NS_CASES(k_chem_cells<NSV><<<nb, OCFD_CHEM_TPB, 0, st>>>(f, Et, T, p, di, dt2, nsub, nfail));
 }
 
@@ -60,17 +80,21 @@ void launch_chem_batch(int ns, int sms, int n, double* di, double* e, const doub
     });
     return;
   }
-  NS_CASES({
+  auto serial = [&](auto kern) {
     int per = 0;
-    if (cp) {
-      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_chem_batch<NSV, true>, OCFD_CHEM_TPB, 0);
-      if (per < 1) per = 1;
-      k_chem_batch<NSV, true><<<sms * per, OCFD_CHEM_TPB, 0, st>>>(n, di, e, dt, nsub, perm, counter, nfail);
-    } else {
-      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_chem_batch<NSV, false>, OCFD_CHEM_TPB, 0);
-      if (per < 1) per = 1;
-      k_chem_batch<NSV, false><<<sms * per, OCFD_CHEM_TPB, 0, st>>>(n, di, e, dt, nsub, perm, counter, nfail);
-    }
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kern, OCFD_CHEM_TPB, 0);
+    if (per < 1) per = 1;
+    kern<<<sms * per, OCFD_CHEM_TPB, 0, st>>>(n, di, e, dt, nsub, perm, counter, nfail);
+  };
+  if (ns == mech_h2air9::NS && current_timeadv() == -1 && current_mech() == MECH_H2AIR9) {
+    constexpr int M = mech_h2air9::NS;
+    if (cp) serial(k_chem_batch<M, true, MECH_H2AIR9>);
+    else serial(k_chem_batch<M, false, MECH_H2AIR9>);
+    return;
+  }
+  NS_CASES({
+    if (cp) serial(k_chem_batch<NSV, true>);
+    else serial(k_chem_batch<NSV, false>);
   });
 }
 }  // namespace ocfd

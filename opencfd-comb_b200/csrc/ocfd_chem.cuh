@@ -53,18 +53,19 @@ struct Slab {
 // CHEM_reactions.f90:130-197), three-body factor included. Arrhenius A T^b exp(-E/T) is evaluated
 // as A exp(b ln T - E (1/T)) with ln T and 1/T formed once per reactor: the same quantity, one
 // exponential instead of a power and an exponential. 0.67 and 1.27 of the Troe form are
-// single-precision literals in the reference.
-template <int NS>
-__device__ __forceinline__ void rate_coef_j(int j, const double* ci, const double* gi, double T, double lt, double rT,
-                                            double& w, double& r) {
+// single-precision literals in the reference. The reaction's structure (third-body flag tb, rate
+// form at, reverse-rate form rereac, stoichiometric sum sgm) comes in as arguments: values read
+// from the constant block in the generic kernels, literals in a compiled mechanism. dgi() returns
+// sum_i g_i (vr_i - vf_i) (called when rereac = 0, where the reference forms it).
+template <int NS, class DG>
+__device__ __forceinline__ void rate_coef_core(int j, int tb, int at, int rereac, int sgm, const double* ci, DG dgi,
+                                               double T, double lt, double rT, double& w, double& r) {
   double Ctrb = 0.0;
-  const int tb = cC.tr_reac[j];
   if (tb == 1) {
 #pragma unroll
     for (int i = 0; i < NS; i++) Ctrb = Ctrb + ci[i] * cC.treff[j][i];
   }
   const double wf1 = cC.af[j][0] * exp(cC.bf[j][0] * lt - cC.ef[j][0] * rT);
-  const int at = cC.af_type[j];
   if (at == 0) {
     w = wf1;
   } else {
@@ -82,14 +83,11 @@ __device__ __forceinline__ void rate_coef_j(int j, const double* ci, const doubl
       w = wf2 * Prs / (1.0 + Prs) * Fx;
     }
   }
-  if (cC.rereac == 0) {
+  if (rereac == 0) {
     const double Rs = 8.314 / 1.013e5 * 1.0e6;
-    double dgi = 0.0;
-#pragma unroll
-    for (int i = 0; i < NS; i++) dgi = dgi + gi[i] * (double)(cC.vr[j][i] - cC.vf[j][i]);
-    double kjx = exp(-dgi * rT) * powi_rt(Rs * T, -cC.sgm[j]);
+    double kjx = exp(-dgi() * rT) * powi_rt(Rs * T, -sgm);
     r = w / kjx;
-  } else if (cC.rereac == 1) {
+  } else if (rereac == 1) {
     r = cC.ar[j] * exp(cC.br[j] * lt - cC.er[j] * rT);
   } else {
     double z = 10000.0 * rT;
@@ -102,6 +100,17 @@ __device__ __forceinline__ void rate_coef_j(int j, const double* ci, const doubl
     w = w * Ctrb;
     r = r * Ctrb;
   }
+}
+template <int NS>
+__device__ __forceinline__ void rate_coef_j(int j, const double* ci, const double* gi, double T, double lt, double rT,
+                                            double& w, double& r) {
+  auto dgi = [&]() {
+    double s = 0.0;
+#pragma unroll
+    for (int i = 0; i < NS; i++) s = s + gi[i] * (double)(cC.vr[j][i] - cC.vf[j][i]);
+    return s;
+  };
+  rate_coef_core<NS>(j, cC.tr_reac[j], cC.af_type[j], cC.rereac, cC.sgm[j], ci, dgi, T, lt, rT, w, r);
 }
 
 // rate-of-progress factors: w prod c^vf, r prod c^vr (CHEM_reactions.f90:213-218, 245-250)
@@ -127,12 +136,25 @@ __device__ __forceinline__ void gibbs_all(double T, double lt, double* gi) {
   }
 }
 
+}  // namespace ocfd
+#include "ocfd_mech_h2air9.cuh"
+namespace ocfd {
+
+// Mechanism forms of the kernels: MECH_GENERIC reads the mechanism's structure from the constant
+// block; MECH_H2AIR9 runs the compiled 9-species H2-air code (ocfd_mech_h2air9.cuh), which the
+// host selects only when the loaded mechanism has exactly that structure.
+constexpr int MECH_GENERIC = 0, MECH_H2AIR9 = 1;
+
 // Reaction_rate (CHEM_reactions.f90:203-225)
-template <int NS>
+template <int NS, int MECH = MECH_GENERIC>
 __device__ void reaction_rate(const double* ci, double* ri, double T) {
   const double lt = log(T), rT = 1.0 / T;
   double gi[NS];
   gibbs_all<NS>(T, lt, gi);
+  if constexpr (MECH == MECH_H2AIR9 && NS == mech_h2air9::NS) {
+    mech_h2air9::rates(ci, ri, gi, T, lt, rT);
+    return;
+  }
 #pragma unroll
   for (int i = 0; i < NS; i++) ri[i] = 0.0;
   for (int k = 0; k < cC.nreac; k++) {
@@ -147,7 +169,7 @@ __device__ void reaction_rate(const double* ci, double* ri, double T) {
 // Reaction_rate_and_Matrix (CHEM_reactions.f90:230-272): ri and Ar(i, j) = d r_i / d c_j into the
 // thread's slab (Ar[i * NS + j]). The division by c_j + 1e-20 is a multiplication by its
 // reciprocal, formed once per species (the same quantity up to the last place).
-template <int NS, int STRIDE>
+template <int NS, int STRIDE, int MECH = MECH_GENERIC>
 __device__ void reaction_rate_matrix(const double* ci, double* ri, Slab<STRIDE> Ar, double T) {
   const double lt = log(T), rT = 1.0 / T;
   double gi[NS], rc[NS];
@@ -159,6 +181,10 @@ __device__ void reaction_rate_matrix(const double* ci, double* ri, Slab<STRIDE> 
   }
 #pragma unroll
   for (int m = 0; m < NS * NS; m++) Ar[m] = 0.0;
+  if constexpr (MECH == MECH_H2AIR9 && NS == mech_h2air9::NS) {
+    mech_h2air9::rates_matrix<STRIDE>(ci, rc, ri, Ar, gi, T, lt, rT);
+    return;
+  }
   for (int k = 0; k < cC.nreac; k++) {
     double w, r, wf1, wr1;
     rate_coef_j<NS>(k, ci, gi, T, lt, rT, w, r);
@@ -249,17 +275,19 @@ __device__ __forceinline__ double update_et(const double* di, const double* dn, 
 }
 
 // chemical_timeAdv (CHEM_reactions.f90:374-390) for one reactor; returns true when the implicit
-// step met a zero pivot
-template <int NS, int STRIDE>
-__device__ bool chem_step(double* di, double& E, double dt, int* nfail, Slab<STRIDE> sA) {
+// step met a zero pivot. A compiled mechanism (MECH != MECH_GENERIC) carries only the linearised
+// implicit Euler (the host runs it for CHEM_TimeAdv = -1 alone): its straight-line reaction code
+// appears once in the kernel.
+template <int NS, int STRIDE, int MECH = MECH_GENERIC>
+__device__ __forceinline__ bool chem_step(double* di, double& E, double dt, int* nfail, Slab<STRIDE> sA) {
   double ci[NS], ri[NS], dn[NS];
-  const int mode = cC.timeadv;
+  const int mode = MECH == MECH_GENERIC ? cC.timeadv : -1;
   bool zero = false;
   if (mode == 1) {
     double T = dev_T<NS>(di, E, nfail);
 #pragma unroll
     for (int i = 0; i < NS; i++) ci[i] = di[i] / cC.Mi[i] * 1.0e-6;
-    reaction_rate<NS>(ci, ri, T);
+    reaction_rate<NS, MECH>(ci, ri, T);
 #pragma unroll
     for (int i = 0; i < NS; i++) dn[i] = di[i] + ri[i] * cC.Mi[i] * 1.0e6 * dt;
     E = update_et<NS>(di, dn, E);
@@ -270,14 +298,14 @@ __device__ bool chem_step(double* di, double& E, double dt, int* nfail, Slab<STR
     double T = dev_T<NS>(di, E, nfail);
 #pragma unroll
     for (int i = 0; i < NS; i++) ci[i] = di[i] / cC.Mi[i] * 1.0e-6;
-    reaction_rate<NS>(ci, ri, T);
+    reaction_rate<NS, MECH>(ci, ri, T);
 #pragma unroll
     for (int i = 0; i < NS; i++) d1[i] = di[i] + ri[i] * cC.Mi[i] * 1.0e6 * dt;
     E = update_et<NS>(di, d1, E);
     T = dev_T<NS>(di, E, nfail);  // the reference takes T from the old densities here
 #pragma unroll
     for (int i = 0; i < NS; i++) ci[i] = d1[i] / cC.Mi[i] * 1.0e-6;
-    reaction_rate<NS>(ci, ri, T);
+    reaction_rate<NS, MECH>(ci, ri, T);
 #pragma unroll
     for (int i = 0; i < NS; i++) dn[i] = 0.5 * di[i] + 0.5 * d1[i] + 0.5 * ri[i] * cC.Mi[i] * 1.0e6 * dt;
     E = update_et<NS>(d1, dn, E);
@@ -293,7 +321,7 @@ __device__ bool chem_step(double* di, double& E, double dt, int* nfail, Slab<STR
       double T = dev_T<NS>(di, E, nfail);
 #pragma unroll
       for (int i = 0; i < NS; i++) ci[i] = di[i] / cC.Mi[i] * 1.0e-6;
-      reaction_rate<NS>(ci, ri, T);
+      reaction_rate<NS, MECH>(ci, ri, T);
 #pragma unroll
       for (int i = 0; i < NS; i++) dn[i] = ra[krk] * d0[i] + rb[krk] * (di[i] + ri[i] * cC.Mi[i] * 1.0e6 * dt);
       E = update_et<NS>(di, dn, E);
@@ -305,7 +333,7 @@ __device__ bool chem_step(double* di, double& E, double dt, int* nfail, Slab<STR
     double T = dev_T<NS>(di, E, nfail);
 #pragma unroll
     for (int i = 0; i < NS; i++) ci[i] = di[i] / cC.Mi[i] * 1.0e-6;
-    reaction_rate_matrix<NS, STRIDE>(ci, ri, sA, T);
+    reaction_rate_matrix<NS, STRIDE, MECH>(ci, ri, sA, T);
 #pragma unroll
     for (int i = 0; i < NS; i++) {
 #pragma unroll
@@ -382,7 +410,7 @@ __device__ __forceinline__ void chem_check(const double* di, double E, bool zero
   if (bad && nfail) atomicAdd(nfail + 1, 1);
 }
 
-template <int NS>
+template <int NS, int MECH = MECH_GENERIC>
 __global__ void __launch_bounds__(OCFD_CHEM_TPB, OCFD_CHEM_MINB) k_chem_cells(double* f, double* Et, double* T,
                                                                              double* p, double* di, double dt2,
                                                                              int nsub, int* nfail) {
@@ -400,7 +428,7 @@ __global__ void __launch_bounds__(OCFD_CHEM_TPB, OCFD_CHEM_MINB) k_chem_cells(do
   const Slab<OCFD_CHEM_TPB> slab{sA + threadIdx.x};
   for (int s = 0; s < nsub; s++) {
     double e0 = e;
-    zero = chem_step<NS, OCFD_CHEM_TPB>(d1, e, dt2, nfail, slab) || zero;
+    zero = chem_step<NS, OCFD_CHEM_TPB, MECH>(d1, e, dt2, nfail, slab) || zero;
     f5 = f5 + (e - e0);
   }
   chem_check<NS>(d1, e, zero, nfail);
@@ -441,7 +469,7 @@ static __global__ void k_nsub_scatter(int n, const int* nsub, int* cursor, int n
 
 // CP: constant-pressure reactors (a template parameter, so the reference's constant-volume form
 // carries none of the pressure-restoring code in its registers)
-template <int NS, bool CP>
+template <int NS, bool CP, int MECH = MECH_GENERIC>
 __global__ void __launch_bounds__(OCFD_CHEM_TPB, OCFD_CHEM_MINB) k_chem_batch(int n, double* di, double* e,
                                                                              const double* dt, const int* nsub,
                                                                              const int* perm, int* counter,
@@ -468,11 +496,11 @@ __global__ void __launch_bounds__(OCFD_CHEM_TPB, OCFD_CHEM_MINB) k_chem_batch(in
         double h0, p0;
         cp_reference<NS>(d1, ee, h0, p0, nfail);
         for (int s = 0; s < ks; s++) {
-          zero = chem_step<NS, OCFD_CHEM_TPB>(d1, ee, dt2, nfail, slab) || zero;
+          zero = chem_step<NS, OCFD_CHEM_TPB, MECH>(d1, ee, dt2, nfail, slab) || zero;
           cp_restore<NS>(d1, ee, h0, p0, nfail);
         }
       } else {
-        for (int s = 0; s < ks; s++) zero = chem_step<NS, OCFD_CHEM_TPB>(d1, ee, dt2, nfail, slab) || zero;
+        for (int s = 0; s < ks; s++) zero = chem_step<NS, OCFD_CHEM_TPB, MECH>(d1, ee, dt2, nfail, slab) || zero;
       }
       chem_check<NS>(d1, ee, zero, nfail);
 #pragma unroll

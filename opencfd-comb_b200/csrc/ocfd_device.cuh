@@ -466,39 +466,77 @@ __device__ __forceinline__ void dev_diffusion(double* amd, double amu, double T,
 }
 
 // ---------------------------------------------------------------- reconstructions
+#ifndef OCFD_FMA_BUILD
+#define OCFD_FMA_BUILD 0
+#endif
+#if OCFD_FMA_BUILD
+// WENO5 nonlinear weights with one division instead of four (contracted build only): the weights
+// a_k = C_k / t_k, t_k = (ep + S_k)^2, and their sum are all multiplied by t0 t1 t2, which leaves
+// the normalised weights unchanged and differs from the reference's operation order by rounding
+// only. With ep = 1e-6 every t_k >= 1e-12, and the products stay in range while the split fluxes
+// are below about 1e30 in magnitude.
+__device__ __forceinline__ double weno5_fold(double C03, double C13, double C23, double t0, double t1, double t2,
+                                             double q0, double q1, double q2_) {
+  const double b0 = C03 * (t1 * t2), b1 = C13 * (t0 * t2), b2 = C23 * (t0 * t1);
+  return (b0 * q0 + b1 * q1 + b2 * q2_) / (b0 + b1 + b2);
+}
+#endif
 // single interface; v points at the stencil centre v(i) (OCFD_Schemes.f90 / OCFD_Schemes_1.f90).
 // VS is the element stride of v (1 when v is contiguous, the line count in shared memory otherwise).
-template <int VS>
-__device__ __forceinline__ double weno5P(const double* v) {
+// 13/12 (a - 2 b + c)^2, the second-difference part of a WENO5 smoothness indicator: sub-stencils
+// of neighbouring interfaces with the same centre share it (the same expression on the same values)
+__device__ __forceinline__ double w5d(double a, double b, double c) { return 13.0 / 12.0 * q2(a - 2.0 * b + c); }
+// WENO5 flux+ from its five values and the second-difference terms of its three sub-stencils
+// (D0 centred on v1, D1 on v0, D2 on vm1)
+__device__ __forceinline__ double weno5P_v(double vm2, double vm1, double v0, double v1, double v2, double D0,
+                                           double D1, double D2) {
   const double ep = 1.0e-6, C03 = 3.0 / 10.0, C13 = 3.0 / 5.0, C23 = 1.0 / 10.0;
-  const double vm2 = v[-2 * VS], vm1 = v[-VS], v0 = v[0], v1 = v[VS], v2 = v[2 * VS];
-  double S0 = 13.0 / 12.0 * q2(v0 - 2.0 * v1 + v2) + 1.0 / 4.0 * q2(3.0 * v0 - 4.0 * v1 + v2);
-  double S1 = 13.0 / 12.0 * q2(vm1 - 2.0 * v0 + v1) + 1.0 / 4.0 * q2(vm1 - v1);
-  double S2 = 13.0 / 12.0 * q2(vm2 - 2.0 * vm1 + v0) + 1.0 / 4.0 * q2(vm2 - 4.0 * vm1 + 3.0 * v0);
-  double a0 = C03 / q2(ep + S0);
-  double a1 = C13 / q2(ep + S1);
-  double a2 = C23 / q2(ep + S2);
-  double am = a0 + a1 + a2;
+  double S0 = D0 + 1.0 / 4.0 * q2(3.0 * v0 - 4.0 * v1 + v2);
+  double S1 = D1 + 1.0 / 4.0 * q2(vm1 - v1);
+  double S2 = D2 + 1.0 / 4.0 * q2(vm2 - 4.0 * vm1 + 3.0 * v0);
   double q03 = 1.0 / 3.0 * v0 + 5.0 / 6.0 * v1 - 1.0 / 6.0 * v2;
   double q13 = -(1.0 / 6.0 * vm1) + 5.0 / 6.0 * v0 + 1.0 / 3.0 * v1;
   double q23 = 1.0 / 3.0 * vm2 - 7.0 / 6.0 * vm1 + 11.0 / 6.0 * v0;
-  return (a0 * q03 + a1 * q13 + a2 * q23) / am;
-}
-template <int VS>
-__device__ __forceinline__ double weno5M(const double* v) {
-  const double ep = 1.0e-6, C03 = 3.0 / 10.0, C13 = 3.0 / 5.0, C23 = 1.0 / 10.0;
-  const double vm1 = v[-VS], v0 = v[0], v1 = v[VS], v2 = v[2 * VS], v3 = v[3 * VS];
-  double S0 = 13.0 / 12.0 * q2(v1 - 2.0 * v0 + vm1) + 1.0 / 4.0 * q2(3.0 * v1 - 4.0 * v0 + vm1);
-  double S1 = 13.0 / 12.0 * q2(v2 - 2.0 * v1 + v0) + 1.0 / 4.0 * q2(v2 - v0);
-  double S2 = 13.0 / 12.0 * q2(v3 - 2.0 * v2 + v1) + 1.0 / 4.0 * q2(v3 - 4.0 * v2 + 3.0 * v1);
+#if OCFD_FMA_BUILD
+  return weno5_fold(C03, C13, C23, q2(ep + S0), q2(ep + S1), q2(ep + S2), q03, q13, q23);
+#else
   double a0 = C03 / q2(ep + S0);
   double a1 = C13 / q2(ep + S1);
   double a2 = C23 / q2(ep + S2);
   double am = a0 + a1 + a2;
+  return (a0 * q03 + a1 * q13 + a2 * q23) / am;
+#endif
+}
+// WENO5 flux- from its five values and the second-difference terms (D0 centred on v0, D1 on v1,
+// D2 on v2)
+__device__ __forceinline__ double weno5M_v(double vm1, double v0, double v1, double v2, double v3, double D0,
+                                           double D1, double D2) {
+  const double ep = 1.0e-6, C03 = 3.0 / 10.0, C13 = 3.0 / 5.0, C23 = 1.0 / 10.0;
+  double S0 = D0 + 1.0 / 4.0 * q2(3.0 * v1 - 4.0 * v0 + vm1);
+  double S1 = D1 + 1.0 / 4.0 * q2(v2 - v0);
+  double S2 = D2 + 1.0 / 4.0 * q2(v3 - 4.0 * v2 + 3.0 * v1);
   double q03 = 1.0 / 3.0 * v1 + 5.0 / 6.0 * v0 - 1.0 / 6.0 * vm1;
   double q13 = -(1.0 / 6.0 * v2) + 5.0 / 6.0 * v1 + 1.0 / 3.0 * v0;
   double q23 = 1.0 / 3.0 * v3 - 7.0 / 6.0 * v2 + 11.0 / 6.0 * v1;
+#if OCFD_FMA_BUILD
+  return weno5_fold(C03, C13, C23, q2(ep + S0), q2(ep + S1), q2(ep + S2), q03, q13, q23);
+#else
+  double a0 = C03 / q2(ep + S0);
+  double a1 = C13 / q2(ep + S1);
+  double a2 = C23 / q2(ep + S2);
+  double am = a0 + a1 + a2;
   return (a0 * q03 + a1 * q13 + a2 * q23) / am;
+#endif
+}
+template <int VS>
+__device__ __forceinline__ double weno5P(const double* v) {
+  const double vm2 = v[-2 * VS], vm1 = v[-VS], v0 = v[0], v1 = v[VS], v2 = v[2 * VS];
+  return weno5P_v(vm2, vm1, v0, v1, v2, w5d(v0, v1, v2), w5d(vm1, v0, v1), w5d(vm2, vm1, v0));
+}
+template <int VS>
+__device__ __forceinline__ double weno5M(const double* v) {
+  const double vm1 = v[-VS], v0 = v[0], v1 = v[VS], v2 = v[2 * VS], v3 = v[3 * VS];
+  return weno5M_v(vm1, v0, v1, v2, v3, w5d(v1, v0, vm1), w5d(v2, v1, v0), w5d(v3, v2, v1));
 }
 // WENO5 with the out-of-domain sub-stencil removed; del 1 = left, 2 = right (DEL_LIFT / DEL_RIGHT)
 template <int VS>
@@ -579,16 +617,25 @@ __device__ __forceinline__ double weno7_core(double w0, double w1, double w2, do
   double S1 = S11 * S11 + d12 * S21 * S21 + d13 * S31 * S31 + d14 * S11 * S31;
   double S2 = S12 * S12 + d12 * S22 * S22 + d13 * S32 * S32 + d14 * S12 * S32;
   double S3 = S13 * S13 + d12 * S23 * S23 + d13 * S33 * S33 + d14 * S13 * S33;
+  double q0 = e11 * w0 + e12 * w1 + e13 * w2 + e14 * w3;
+  double q1 = e21 * w1 + e22 * w2 + e23 * w3 + e24 * w4;
+  double q2_ = e31 * w2 + e32 * w3 + e33 * w4 + e34 * w5;
+  double q3_ = e41 * w3 + e42 * w4 + e43 * w5 + e44 * w6;
+#if OCFD_FMA_BUILD
+  // one division: every weight multiplied by the product of the four (ep + S)^2 (in range while
+  // the split fluxes are below about 1e20 in magnitude; ep = 1e-8 keeps every factor >= 1e-16)
+  const double t0 = q2(ep + S0), t1 = q2(ep + S1), t2 = q2(ep + S2), t3 = q2(ep + S3);
+  const double p01 = t0 * t1, p23 = t2 * t3;
+  const double b0 = C0 * t1 * p23, b1 = C1 * t0 * p23, b2 = C2 * p01 * t3, b3 = C3 * p01 * t2;
+  return (b0 * q0 + b1 * q1 + b2 * q2_ + b3 * q3_) / ((b0 + b1) + (b2 + b3));
+#else
   double a0 = C0 / q2(ep + S0);
   double a1 = C1 / q2(ep + S1);
   double a2 = C2 / q2(ep + S2);
   double a3 = C3 / q2(ep + S3);
   double am = a0 + a1 + a2 + a3;
-  double q0 = e11 * w0 + e12 * w1 + e13 * w2 + e14 * w3;
-  double q1 = e21 * w1 + e22 * w2 + e23 * w3 + e24 * w4;
-  double q2_ = e31 * w2 + e32 * w3 + e33 * w4 + e34 * w5;
-  double q3_ = e41 * w3 + e42 * w4 + e43 * w5 + e44 * w6;
   return (a0 * q0 + a1 * q1 + a2 * q2_ + a3 * q3_) / am;
+#endif
 }
 template <int VS>
 __device__ __forceinline__ double weno7P(const double* v) {

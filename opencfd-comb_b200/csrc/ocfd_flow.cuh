@@ -12,6 +12,7 @@
 //  k_repair_et   handle_NegativeEt replay (OCFD_handle_NegativeT.f90).
 //  k_bc_*        OCFD_bc, ocfd_bc_BoundaryLayer, Flow_Ghost_Extent_2nd.
 #pragma once
+#include <type_traits>
 #include "ocfd_device.cuh"
 
 namespace ocfd {
@@ -345,6 +346,54 @@ __global__ void __launch_bounds__(FLUX_THREADS, SCALAR ? OCFD_SCALAR_FLUX_MINB :
         if (line_ok && t0 + q <= ncell && sfast[ii]) sh[cs * NI + ii] = h[q];
       }
     }
+  } else if constexpr (!HYB && SCHEME == OCFD_SCHEME_WENO5) {
+    // WENO5 in runs of R = 3 consecutive interfaces of one pencil and (component, sign), items
+    // laid out like the UD7L runs above: the R + 4 split fluxes of a run are loaded once, and the
+    // second-difference terms of the smoothness indicators, which neighbouring interfaces share,
+    // are formed once per point (each the expression the single-interface form evaluates, so the
+    // results are the same). A run that touches a boundary closure, or the last run of a pencil
+    // when 3 does not divide its C + 1 interfaces, goes interface by interface. (Runs of 5 made
+    // the 64-register species sweeps spill.)
+    constexpr int R = 3, NR = (C + R) / R, NH = NC * NL * NR;
+    auto run = [&](auto plus_c, int cs, int t0, int l) {
+      constexpr bool PLUS = decltype(plus_c)::value;
+      double* hs = sh + cs * NI;
+      const int tl = min(t0 + R - 1, ncell);
+      if (t0 + R - 1 > C || closure_zone(s0 - 1 + t0, n, DIR) || closure_zone(s0 - 1 + tl, n, DIR)) {
+        for (int t = t0; t <= tl; t++)
+          hs[iidx(t, l)] = interface_flux<SCHEME, PLUS, VS>(sf + sidx(cs, t + 3, l), s0 - 1 + t, n, DIR, 0);
+        return;
+      }
+      // flux+: f(i0-2) .. f(i0+R+1); flux-: f(i0-1) .. f(i0+R+2), i0 the run's first left cell
+      const double* x = sf + sidx(cs, t0 + (PLUS ? 1 : 2), l);
+      double w[R + 4], D[R + 3];
+#pragma unroll
+      for (int m = 0; m < R + 4; m++) w[m] = x[m * VS];
+#pragma unroll
+      for (int m = 1; m < R + 3; m++) D[m] = PLUS ? w5d(w[m - 1], w[m], w[m + 1]) : w5d(w[m + 1], w[m], w[m - 1]);
+#pragma unroll
+      for (int q = 0; q < R; q++) {
+        const double h = PLUS ? weno5P_v(w[q], w[q + 1], w[q + 2], w[q + 3], w[q + 4], D[q + 3], D[q + 2], D[q + 1])
+                              : weno5M_v(w[q], w[q + 1], w[q + 2], w[q + 3], w[q + 4], D[q + 1], D[q + 2], D[q + 3]);
+        if (t0 + q <= ncell) hs[iidx(t0 + q, l)] = h;
+      }
+    };
+    for (int it = threadIdx.x; it < 2 * NH; it += FLUX_THREADS) {
+      const bool plus = it < NH;
+      const int jt = plus ? it : it - NH;
+      int c, l, r;
+      if (DIR == 0) {  // lanes across pencils (odd pitch: no bank conflicts)
+        const int cl = jt % (NC * NL);
+        r = jt / (NC * NL); c = cl / NL; l = cl - c * NL;
+      } else {         // lanes along the contiguous i-lines
+        l = jt % NL;
+        const int rc = jt / NL;
+        r = rc % NR; c = rc / NR;
+      }
+      if (l0 + l > nl_max || r * R > ncell) continue;
+      if (plus) run(std::true_type{}, c, r * R, l);
+      else run(std::false_type{}, NC + c, r * R, l);
+    }
   } else {
     // two independent items per iteration, so that their dependent FP64 chains overlap
     for (int idx = threadIdx.x; idx < nfast; idx += 2 * FLUX_THREADS) {
@@ -447,6 +496,44 @@ __device__ __forceinline__ double cdiff_g(F f, int dir, int ii, int n) {
 __device__ __forceinline__ double cdiff(const double* __restrict__ f, int q, int dir, int ii, int n) {
   const int s = hstride(dir);
   return cdiff_g<0>([&](int m) { return f[q + m * s]; }, dir, ii, n);
+}
+// true when cdiff takes its interior formula at sweep index ii of n in direction dir (periodic,
+// or away from the one-sided and reduced closures of both faces)
+__device__ __forceinline__ bool cdiff_interior(int dir, int ii, int n) {
+  if (cC.iper[dir]) return true;
+  const int e = cC.cd8_on ? 4 : 3;
+  return ii > e && ii < n + 1 - e;
+}
+// d fx / dx, d fy / dy, d fz / dz at (i, j, k) / q with cdiff's expressions; a cell whose three
+// directions are all interior (most cells) takes one straight-line path, so the 18 (CD6) or 24
+// (CD8) stencil loads are issued together instead of behind each direction's closure branches
+__device__ __forceinline__ void cdiff3(const double* __restrict__ fx, const double* __restrict__ fy,
+                                       const double* __restrict__ fz, int q, int i, int j, int k, double& dk,
+                                       double& di, double& ds) {
+  if (cdiff_interior(0, i, cC.nx) && cdiff_interior(1, j, cC.ny) && cdiff_interior(2, k, cC.nz)) {
+    const int sy = hstride(1), sz = hstride(2);
+    if (cC.cd8_on) {
+      auto c8 = [&](const double* __restrict__ f, int dir, int s) {
+        const double* c = cC.cd8[dir];
+        const double fm1 = __ldg(f + q - s), fp1 = __ldg(f + q + s), fm2 = __ldg(f + q - 2 * s), fp2 = __ldg(f + q + 2 * s);
+        const double fm3 = __ldg(f + q - 3 * s), fp3 = __ldg(f + q + 3 * s), fm4 = __ldg(f + q - 4 * s), fp4 = __ldg(f + q + 4 * s);
+        return c[0] * (fp1 - fm1) + c[1] * (fp2 - fm2) + c[2] * (fp3 - fm3) + c[3] * (fp4 - fm4);
+      };
+      dk = c8(fx, 0, 1); di = c8(fy, 1, sy); ds = c8(fz, 2, sz);
+    } else {
+      auto c6 = [&](const double* __restrict__ f, int dir, int s) {
+        const double* a = cC.cd6[dir];
+        const double fm1 = __ldg(f + q - s), fp1 = __ldg(f + q + s), fm2 = __ldg(f + q - 2 * s), fp2 = __ldg(f + q + 2 * s);
+        const double fm3 = __ldg(f + q - 3 * s), fp3 = __ldg(f + q + 3 * s);
+        return a[0] * (fp3 - fm3) + a[1] * (fp2 - fm2) + a[2] * (fp1 - fm1);
+      };
+      dk = c6(fx, 0, 1); di = c6(fy, 1, sy); ds = c6(fz, 2, sz);
+    }
+    return;
+  }
+  dk = cdiff(fx, q, 0, i, cC.nx);
+  di = cdiff(fy, q, 1, j, cC.ny);
+  ds = cdiff(fz, q, 2, k, cC.nz);
 }
 
 // interior cell of a linear thread index (32-bit arithmetic: the library rejects grids whose
@@ -832,7 +919,8 @@ __global__ void __launch_bounds__(32 * NS, OCFD_SPECIES_MINB) k_scal_ev(const do
     double A[9], A1[9];
     metric_all<SEP>(g, i, j, k, q, A, A1);
     const double* c = ci + (size_t)ks * H;
-    double uk = cdiff(c, q, 0, i, cC.nx), ui = cdiff(c, q, 1, j, cC.ny), us = cdiff(c, q, 2, k, cC.nz);
+    double uk, ui, us;
+    cdiff3(c, c, c, q, i, j, k, uk, ui, us);
     double hi = dev_hi(ks, T[q]);
     double cix = uk * A[0] + ui * A[3] + us * A[6];
     double ciy = uk * A[1] + ui * A[4] + us * A[7];
@@ -878,7 +966,8 @@ __global__ void __launch_bounds__(32 * NS, OCFD_SCAL_DIV_MINB) k_scal_div(const 
   const int q = hidx(i, j, k), nn = nidx(i, j, k);
   const double jac = metric_jac<SEP>(g, i, j, k, q);  // every species' thread (no barrier)
   const size_t o = (size_t)ks * cC.H;
-  double uk = cdiff(e1 + o, q, 0, i, cC.nx), ui = cdiff(e2 + o, q, 1, j, cC.ny), us = cdiff(e3 + o, q, 2, k, cC.nz);
+  double uk, ui, us;
+  cdiff3(e1 + o, e2 + o, e3 + o, q, i, j, k, uk, ui, us);
   double* du = dus + (size_t)ks * cC.N + nn;
   *du = *du + (uk + ui + us) * jac;
 }

@@ -74,6 +74,7 @@ struct Lib {
   DevConst hc{};
   int NS = 1;
   bool sep = false, have_kin = false, flow_ready = false;
+  bool mech_on = true;  // run the compiled mechanism kernels when the loaded mechanism matches
   cudaStream_t st = nullptr;
   char* arena = nullptr;
   size_t arena_size = 0, arena_used = 0;
@@ -505,6 +506,9 @@ void flow_rhs_t(const FluxArgs& fa) {
 }
 
 template <int NS>
+void stage_rhs_t(int krk, double dt1, bool rk);
+
+template <int NS>
 void stage_t(int krk, double dt1) {
   const long long N = L->hc.N, H = L->hc.H;
   double* Etc = L->Et[L->cur];
@@ -528,6 +532,26 @@ void stage_t(int krk, double dt1) {
     sensor();
     exchange({L->Rh}, 7);
   }
+  stage_rhs_t<NS>(krk, dt1, true);
+  // N_SPEC = 1: di = d over the whole array (OCFD_Time_Adv.f90:45-52). Nothing between the stage
+  // start and here reads di, and the inline transport of k_visc_ev must see the previous stage's
+  // di (comput_Amu_Amk_AMD runs before the copy in the reference), so the copy happens here.
+  if (NS == 1) {
+    KTimer t(KC_EXCH);
+    k_copy<<<nblk(H, 256), 256, 0, L->st>>>(L->d, L->di, H);
+    LAUNCH_CHECK();
+  }
+  prims_t<NS>(krk, dt1);
+  ocfd_bc_t<NS>();
+}
+
+// The right-hand sides of a stage: the species (inviscid sweeps, viscous fluxes and their
+// divergence, and with rk the species RK update) and the flow (flow_rhs_t). Without rk it writes
+// only arrays that every stage recomputes before reading them (Dus, ci, the species viscous
+// fluxes, Qp, du, Ev), which the tuner uses to time it on the current state.
+template <int NS>
+void stage_rhs_t(int krk, double dt1, bool rk) {
+  const long long N = L->hc.N, H = L->hc.H;
   FluxArgs fa = flow_flux_args();
   // Species (every species at once: du_scaler_invis / du_scaler_viscous / Scalar_time_adv_RK3 of
   // the reference's species loop; Dus of species m is dus + m N). The species sweeps read only di
@@ -562,7 +586,7 @@ void stage_t(int krk, double dt1) {
       else k_scal_div<NS, false><<<nblk(N, 32), dim3(32, NS), 0, L->st>>>(L->se[0], L->se[1], L->se[2], L->dus, L->geo);
       LAUNCH_CHECK();
     }
-    {
+    if (rk) {
       KTimer t(KC_SPECIES_RK);
       k_scal_rk<<<dim3(nblk(N, 256), NS), 256, 0, L->st>>>(krk, dt1, L->dus, L->din, L->di);
       LAUNCH_CHECK();
@@ -606,16 +630,6 @@ void stage_t(int krk, double dt1) {
   fa.out = L->du;
   flow_rhs_t<NS>(fa);
   if (spfork) CK(cudaStreamWaitEvent(L->st, L->ev_sp_join, 0));
-  // N_SPEC = 1: di = d over the whole array (OCFD_Time_Adv.f90:45-52). Nothing between the stage
-  // start and here reads di, and the inline transport of k_visc_ev must see the previous stage's
-  // di (comput_Amu_Amk_AMD runs before the copy in the reference), so the copy happens here.
-  if (NS == 1) {
-    KTimer t(KC_EXCH);
-    k_copy<<<nblk(H, 256), 256, 0, L->st>>>(L->d, L->di, H);
-    LAUNCH_CHECK();
-  }
-  prims_t<NS>(krk, dt1);
-  ocfd_bc_t<NS>();
 }
 
 template <int NS>
@@ -657,7 +671,7 @@ void chem_t(double dt2, int nsub) {
 // which block computes a point, not how; the stored metric arrays hold the values the separable
 // form computes), so the tuner is free to pick by time alone. Choices are remembered per
 // configuration in the process.
-constexpr int TUNE_N = 9, TUNE_TIMES = 3 * FLUX_TILE_SHAPES + 9 + 5 + 2;
+constexpr int TUNE_N = 9, TUNE_TIMES = 3 * FLUX_TILE_SHAPES + 9 + 5 + 2 + 2;
 std::map<std::string, std::array<int, TUNE_N>> g_tune_cache;
 
 std::string tune_key() {
@@ -708,7 +722,8 @@ void apply_tiles(const int* c) {
   L->met_flux = c[5] != 0;
   L->met_ev = c[6] != 0;
   L->met_div = c[7] != 0;
-  L->fork_visc = c[8] != 0;
+  L->fork_visc = (c[8] & 1) != 0;
+  L->fork_species = (c[8] & 2) != 0;
   drop_graphs();  // the captured step holds the old launches
 }
 
@@ -752,7 +767,7 @@ void tune_t(int reps, int* best, double* ms) {
     }
     best[3] = best[4] = VE_KC;
     best[5] = best[6] = best[7] = L->sep ? 0 : 1;
-    best[8] = 1;
+    best[8] = NS > 1 ? 3 : 1;
     for (int m = 3 * FLUX_TILE_SHAPES; m < TUNE_TIMES; m++) ms[m] = -1.0;
     if (P.if_viscous == 1) {
       double t_ev = 1e300, t_div = 1e300;
@@ -822,6 +837,23 @@ void tune_t(int reps, int* best, double* ms) {
       L->fork_visc = true;
       ms[M1 + 1] = timed([&] { flow_rhs_t<NS>(fr); });
       best[8] = ms[M1 + 1] < ms[M1] ? 1 : 0;
+      L->fork_visc = best[8] != 0;
+    }
+    if (NS > 1) {  // the species chain on the third stream or in order: a stage's right-hand
+                   // sides without the species RK update, both ways
+      const int M2 = 3 * FLUX_TILE_SHAPES + 9 + 5 + 2;
+      for (int d = 0; d < 3; d++) L->flux_ts[d] = best[d];
+      L->kc_ev = best[3];
+      L->kc_div = best[4];
+      L->met_flux = best[5] && L->sep;
+      L->met_ev = best[6] && L->sep;
+      L->met_div = best[7] && L->sep;
+      L->fork_visc = (best[8] & 1) != 0;
+      L->fork_species = false;
+      ms[M2] = timed([&] { stage_rhs_t<NS>(1, 0.0, false); });
+      L->fork_species = true;
+      ms[M2 + 1] = timed([&] { stage_rhs_t<NS>(1, 0.0, false); });
+      best[8] = (best[8] & 1) | (ms[M2 + 1] < ms[M2] ? 2 : 0);
     }
   } catch (...) {
     cudaEventDestroy(e0);
@@ -1317,6 +1349,7 @@ namespace ocfd {
 // for the surrogate module
 int current_nspec() { return L && L->have_kin ? L->NS : 0; }
 int current_const_p() { return L && L->have_kin ? L->hc.const_p : 0; }
+int current_mech() { return L && L->have_kin && L->mech_on ? mech_match(L->hc) : 0; }
 int current_timeadv() { return L ? L->hc.timeadv : 0; }
 cudaStream_t current_stream() { return L ? L->st : nullptr; }
 }  // namespace ocfd
@@ -2193,6 +2226,14 @@ int ocfd_gpu_chem_batch(int n, double* di, double* e, const double* dt, const in
   });
 }
 
+int ocfd_gpu_chem_compiled_mechanism(int on) {
+  return guarded([&]() -> int {
+    if (!L || !L->have_kin) { g_err = "ocfd_gpu_init or ocfd_gpu_chem_setup with a mechanism first"; return OCFD_ERR_STATE; }
+    if (on >= 0) L->mech_on = on != 0;
+    return L->hc.timeadv == -1 && current_mech() != 0 ? 1 : 0;
+  });
+}
+
 int ocfd_gpu_chem_constant_pressure(int on) {
   return guarded([&]() -> int {
     if (!L || !L->have_kin) { g_err = "ocfd_gpu_init or ocfd_gpu_chem_setup with a mechanism first"; return OCFD_ERR_STATE; }
@@ -2384,11 +2425,15 @@ int ocfd_gpu_set_tiles(const int* choice) {
       g_err = "k planes per block must be >= 1 (k_visc_div: >= 0, 0 = per-cell form)";
       return OCFD_ERR_PARAM;
     }
-    for (int m = 5; m < 9; m++)
+    for (int m = 5; m < 8; m++)
       if (choice[m] != 0 && choice[m] != 1) {
-        g_err = "metric forms and the second-stream switch must be 0 or 1";
+        g_err = "metric forms must be 0 or 1";
         return OCFD_ERR_PARAM;
       }
+    if (choice[8] < 0 || choice[8] > 3) {
+      g_err = "the stream switches (choice[8]) must be 0..3";
+      return OCFD_ERR_PARAM;
+    }
     apply_tiles(choice);
     return 0;
   });
@@ -2402,7 +2447,7 @@ int ocfd_gpu_get_tiles(int* choice) {
   choice[5] = L->sep ? (int)L->met_flux : 1;
   choice[6] = L->sep ? (int)L->met_ev : 1;
   choice[7] = L->sep ? (int)L->met_div : 1;
-  choice[8] = (int)L->fork_visc;
+  choice[8] = (int)L->fork_visc | (int)L->fork_species << 1;
   return 0;
 }
 

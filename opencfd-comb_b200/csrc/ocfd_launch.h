@@ -29,4 +29,7 @@ void launch_chem_cells(int ns, long long ncell, double* f, double* Et, double* T
                        int nsub, int* nfail, cudaStream_t st);
 void launch_chem_batch(int ns, int sms, int n, double* di, double* e, const double* dt, const int* nsub,
                        const int* perm, int* counter, int* nfail, cudaStream_t st);
+// the compiled mechanism whose structure the constant block's mechanism has (MECH_H2AIR9), else
+// MECH_GENERIC (ocfd_chem.cu)
+int mech_match(const DevConst& c);
 }  // namespace ocfd

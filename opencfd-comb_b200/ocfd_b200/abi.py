@@ -158,6 +158,7 @@ GPU_SIGNATURES = {
     "ocfd_gpu_chem_batch_noalloc": (I, [I, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "ocfd_gpu_chem_batch_status": (I, [C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)]),
     "ocfd_gpu_chem_constant_pressure": (I, [I]),
+    "ocfd_gpu_chem_compiled_mechanism": (I, [I]),
     "ocfd_gpu_gemm_bf16": (I, [I, I, I, C.c_void_p, C.c_longlong, C.c_longlong, C.c_void_p, C.c_longlong,
                                C.c_longlong, C.c_void_p, C.c_longlong, C.c_void_p, I, I]),
     "ocfd_gpu_surrogate_init": (I, [C.c_uint]),

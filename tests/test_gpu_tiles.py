@@ -11,8 +11,8 @@ pytestmark = pytest.mark.gpu
 CHOICES = [
     [0, 0, 0, 16, 16, 0, 0, 0, 0],  # everything on one stream
     [1, 1, 1, 8, 32, 0, 0, 0, 1],
-    [2, 2, 2, 64, 8, 1, 0, 1, 1],
-    [1, 2, 0, 3, 5, 0, 1, 0, 0],  # k chunks that do not divide nz
+    [2, 2, 2, 64, 8, 1, 0, 1, 3],  # both side streams
+    [1, 2, 0, 3, 5, 0, 1, 0, 2],  # k chunks that do not divide nz; species chain on a third stream
     [0, 1, 2, 16, 0, 1, 1, 1, 1],  # per-cell k_visc_div, stored metric arrays everywhere
 ]
 
@@ -60,9 +60,23 @@ def test_autotune_choice_and_solution():
     assert choice[0] in (0, 1, 2) and choice[1] in (0, 1, 2) and choice[2] in (0, 1, 2)
     assert choice[3] in (8, 16, 32, 64) and choice[4] in (0, 8, 16, 32, 64)
     assert all(x in (0, 1) for x in choice[5:]) and len(choice) == 9
-    assert all(t > 0 for t in ms), ms  # viscous separable case: every candidate timed
+    assert all(t > 0 for t in ms[:25]), ms  # viscous separable case: every candidate timed
+    assert ms[25:27] == [-1.0, -1.0]  # one species: no species chain to place
     for d in range(3):
         assert ms[3 * d + choice[d]] == min(ms[3 * d:3 * d + 3])
+    for a, b in zip(ref, st):
+        assert np.array_equal(a, b)
+
+
+def test_autotune_places_the_species_chain():
+    """the reacting jet: the tuner times a stage's right-hand sides with the species chain in order
+    and on the third stream, keeps the faster, and leaves the solution as it was"""
+    c = _case("jet")
+    ref, _ = _run(c)
+    st, (choice, ms) = _run(c, tune=True)
+    assert choice[8] in (0, 1, 2, 3)
+    assert ms[25] > 0 and ms[26] > 0
+    assert bool(choice[8] & 2) == (ms[26] < ms[25])
     for a, b in zip(ref, st):
         assert np.array_equal(a, b)
 
@@ -83,7 +97,8 @@ def test_bad_tile_choice_is_rejected():
     c = _case("isotropic")
     g = solver.Solver(c)
     g.init_state()
-    for bad in ([3, 0, 0, 16, 16], [0, -1, 0, 16, 16], [0, 0, 0, 0, 16], [0, 0, 0, 16, -1], [0, 0, 0, 16, 16, 2], [0, 0, 0, 16, 16, 0, 0, 0, 3]):
+    for bad in ([3, 0, 0, 16, 16], [0, -1, 0, 16, 16], [0, 0, 0, 0, 16], [0, 0, 0, 16, -1], [0, 0, 0, 16, 16, 2],
+                [0, 0, 0, 16, 16, 0, 0, 0, 4], [0, 0, 0, 16, 16, 0, 0, 0, -1]):
         with pytest.raises(solver.OcfdError):
             g.set_tiles(bad)
     g.close()
