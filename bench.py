@@ -775,7 +775,7 @@ def main_jet(a):
         ms_sg, _, clk_sg = timed_run(L, dt, tt, a.steps, 1, nsub)
         ranks.barrier()
         tt += a.steps * dt
-        reasons = (C.c_longlong * 5)()
+        reasons = (C.c_longlong * 6)()
         rejected = L.ocfd_gpu_chem_surrogate_rejected(reasons)
         rest = total - (1 + a.warmup + a.steps)
         if rest > 0:
@@ -799,7 +799,7 @@ def main_jet(a):
                    "meets_target": bool(peak <= 0.01 and yerr <= 1e-3)},
                "fallback_fraction_last_step": rejected / N,
                "rejection_reasons_last_step": dict(zip(["negative_Y", "T_check", "T_range", "logp_range",
-                                                         "logdt_range"], list(reasons))),
+                                                         "logdt_range", "Y_range"], list(reasons))),
                "tol_T_K": a.sg_tol, "train": train,
                "chemistry_share_of_plain_step": chem_share,
                "amdahl_bound_on_speedup": (1.0 / (1.0 - chem_share)) if chem_share else None,

@@ -411,9 +411,10 @@ int ocfd_gpu_surrogate_fused(int on);
  * take the FP64 sub-steps; the step stays one CUDA graph. Mode 1 needs a trained or loaded
  * surrogate for this mechanism. ocfd_gpu_chem_surrogate_rejected: cells that took the FP64 path in
  * the last chemistry call; reasons (when not NULL) gets how many failed each test: negative
- * composition, temperature check, T / log p / log dt outside the training range. */
+ * composition, temperature check, T / log p / log dt outside the training range, a mass fraction
+ * outside its training range widened by half its normalisation scale. */
 int ocfd_gpu_chem_mode(int mode, double tol_T);
-long long ocfd_gpu_chem_surrogate_rejected(long long* reasons /* 5 counts or NULL */);
+long long ocfd_gpu_chem_surrogate_rejected(long long* reasons /* 6 counts or NULL */);
 
 #ifdef __cplusplus
 }

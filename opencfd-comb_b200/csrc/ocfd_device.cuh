@@ -9,12 +9,21 @@
 #include "../../include/ocfd_gpu.h"
 
 #define OCFD_L 4  // halo width LAP
+// 1 in the contracted multiply-add build (libocfd_gpu_fma.so): algebraic forms with fewer FP64
+// divisions that give the same values up to rounding
+#ifndef OCFD_FMA_BUILD
+#define OCFD_FMA_BUILD 0
+#endif
 
 namespace ocfd {
 
 // ---------------------------------------------------------------- constant memory
 struct DevConst {
   int nx, ny, nz, ns;
+  // division of a 31-bit cell index by nx and ny as a multiply-high and a shift (magic numbers of
+  // fast_divisor, filled by the host)
+  unsigned mx, my;
+  int sx, sy;
   int HX, HY, HZ;
   long long H, N;
   int iper[3];
@@ -87,6 +96,12 @@ __device__ __forceinline__ int hidx(int i, int j, int k) {
   return (i + OCFD_L - 1) + cC.HX * ((j + OCFD_L - 1) + cC.HY * (k + OCFD_L - 1));
 }
 __device__ __forceinline__ int nidx(int i, int j, int k) { return (i - 1) + cC.nx * ((j - 1) + cC.ny * (k - 1)); }
+// n / d for n < 2^31 with the host's magic pair (m, s) of d (fast_divisor): floor(n m / 2^(32 + s)),
+// and n itself for d = 1 (Granlund and Montgomery, "Division by invariant integers using
+// multiplication", PLDI 1994: m = ceil(2^(31 + l) / d), l = ceil(log2 d), s = l - 1)
+__device__ __forceinline__ unsigned fast_div(unsigned n, unsigned d, unsigned m, int s) {
+  return d == 1 ? n : __umulhi(n, m) >> s;
+}
 __device__ __forceinline__ int hstride(int dir) { return dir == 0 ? 1 : (dir == 1 ? cC.HX : cC.HX * cC.HY); }
 
 // gfortran -O3 integer-power chains (GCC powi table): x**3 = x**2*x, x**4 = (x**2)**2, x**5 = x**2*x**3
@@ -172,9 +187,14 @@ __device__ __forceinline__ void metric_dir(const Geo& g, int dir, int i, int j, 
     bool cross;
     sep_derivs(g, i, j, k, xi, yi, zi, xj, yj, zj, xk, yk, zk, cross);
     if (!cross) {
+#if OCFD_FMA_BUILD
+      // (jac (yj zk)) / jac is yj zk up to rounding: the contracted build skips both divisions
+      const double d = dir == 0 ? yj * zk : (dir == 1 ? zk * xi : xi * yj);
+#else
       double jac = 1.0 / (xi * yj * zk);
       double a = dir == 0 ? jac * (yj * zk) : (dir == 1 ? jac * (zk * xi) : jac * (xi * yj));
       double d = a / jac;
+#endif
       A1 = dir == 0 ? d : 0.0;
       A2 = dir == 1 ? d : 0.0;
       A3 = dir == 2 ? d : 0.0;
@@ -223,7 +243,11 @@ __device__ __forceinline__ void metric_all(const Geo& g, int i, int j, int k, in
 #pragma unroll
       for (int m = 0; m < 9; m++) { a[m] = 0.0; a1[m] = 0.0; }
       a[0] = akx; a[4] = aiy; a[8] = asz;
+#if OCFD_FMA_BUILD
+      a1[0] = yj * zk; a1[4] = zk * xi; a1[8] = xi * yj;  // akx / jac etc. up to rounding
+#else
       a1[0] = akx / jac; a1[4] = aiy / jac; a1[8] = asz / jac;
+#endif
     } else {
       double jac;
       jac_full(xi, yi, zi, xj, yj, zj, xk, yk, zk, a, jac);
@@ -466,9 +490,6 @@ __device__ __forceinline__ void dev_diffusion(double* amd, double amu, double T,
 }
 
 // ---------------------------------------------------------------- reconstructions
-#ifndef OCFD_FMA_BUILD
-#define OCFD_FMA_BUILD 0
-#endif
 #if OCFD_FMA_BUILD
 // WENO5 nonlinear weights with one division instead of four (contracted build only): the weights
 // a_k = C_k / t_k, t_k = (ep + S_k)^2, and their sum are all multiplied by t0 t1 t2, which leaves

@@ -541,9 +541,9 @@ __device__ __forceinline__ void cdiff3(const double* __restrict__ fx, const doub
 __device__ __forceinline__ bool cell_of(long long t64, int& i, int& j, int& k) {
   if (t64 >= cC.N) return false;
   const unsigned t = (unsigned)t64, nx = (unsigned)cC.nx, ny = (unsigned)cC.ny;
-  const unsigned r = t / nx;
+  const unsigned r = fast_div(t, nx, cC.mx, cC.sx);
   i = (int)(t - r * nx) + 1;
-  const unsigned s = r / ny;
+  const unsigned s = fast_div(r, ny, cC.my, cC.sy);
   j = (int)(r - s * ny) + 1;
   k = (int)s + 1;
   return true;

@@ -1035,6 +1035,23 @@ void fill_thermo(DevConst& c, const ocfd_thermo* th, int realgas) {
   for (int i = 0; i < th->n_spec; i++)
     for (int j = 0; j < th->n_spec; j++) c.mratio[i][j] = th->mi[i] / th->mi[j];
 }
+// magic pair of fast_div for a divisor d >= 1: m = ceil(2^(31 + l) / d) with l = ceil(log2 d) and
+// s = l - 1, exact for every dividend below 2^31 (d = 1 is special-cased on the device); checked
+// here against the hardware division on the largest dividends and a sweep of small ones
+void fast_divisor(unsigned d, unsigned& m, int& s) {
+  int l = 0;
+  while ((1ull << l) < d) l++;
+  const unsigned long long p = 1ull << (31 + l);
+  m = (unsigned)((p + d - 1) / d);
+  s = l > 0 ? l - 1 : 0;
+  if (d <= 1) return;
+  auto q = [&](unsigned n) { return (unsigned)(((unsigned long long)n * m) >> 32) >> s; };
+  for (unsigned n = 0; n < 4096; n++)
+    if (q(n) != n / d) throw std::runtime_error("fast_divisor");
+  for (unsigned n = 0x7fffffffu; n > 0x7fffffffu - 4096; n--)
+    if (q(n) != n / d) throw std::runtime_error("fast_divisor");
+}
+
 void fill_kin(DevConst& c, const ocfd_kinetics* kin) {
   c.nreac = kin->n_reac;
   c.rereac = kin->rereac;
@@ -1437,6 +1454,8 @@ int ocfd_gpu_init(const ocfd_params* p, const ocfd_thermo* th, const ocfd_kineti
     CK(cudaEventCreateWithFlags(&L->ev_sp_join, cudaEventDisableTiming));
     DevConst& c = L->hc;
     c.nx = p->nx; c.ny = p->ny; c.nz = p->nz; c.ns = p->n_spec;
+    fast_divisor((unsigned)p->nx, c.mx, c.sx);
+    fast_divisor((unsigned)p->ny, c.my, c.sy);
     c.HX = p->nx + 2 * OCFD_L; c.HY = p->ny + 2 * OCFD_L; c.HZ = p->nz + 2 * OCFD_L;
     c.H = (long long)c.HX * c.HY * c.HZ;
     c.N = (long long)p->nx * p->ny * p->nz;

@@ -35,6 +35,7 @@ namespace sg {
 
 constexpr int HID = 256, PAD = 16;  // hidden width; padded input / output width
 constexpr int NLAYER = 4;
+constexpr double Y_STD_FLOOR = 1.0e-3;  // smallest normalisation scale of a mass fraction input
 
 struct Norm {  // per-column affine maps and the training range of the raw inputs
   float in_mean[PAD], in_std[PAD], out_mean[PAD], out_std[PAD];
@@ -214,6 +215,23 @@ __global__ void k_to_bf16(long long n, const float* __restrict__ p, __nv_bfloat1
 // subspace, the energy follows update_et, T comes from the energy; the gate compares that T with
 // the network's own dT. mode 0: write every reactor to the outputs (ungated); mode 1: write the
 // accepted reactors in place and list the others for the FP64 integrator.
+// every mass fraction input inside its training range widened by half a normalised unit (its
+// training standard deviation, at least Y_STD_FLOOR): the network sees no input far outside what
+// it was trained on. A trace species whose level grows past what the training states held (radicals
+// of a mixture that starts to react) would otherwise reach the network as tens or thousands of
+// normalised units.
+template <int NS>
+__device__ __forceinline__ bool mass_fractions_in_range(const float* ri, const Norm* nm) {
+  bool in = true;
+#pragma unroll
+  for (int k = 0; k < NS; k++) {
+    const int c = 2 + k;
+    const float w = 0.5f * nm->in_std[c];
+    in = in && ri[c] >= nm->in_min[c] - w && ri[c] <= nm->in_max[c] + w;
+  }
+  return in;
+}
+
 template <int NS>
 __global__ void k_post(int n, int mode, double* __restrict__ di, double* __restrict__ e,
                        const double* __restrict__ T0, const float* __restrict__ raw, const float* __restrict__ out,
@@ -254,6 +272,7 @@ __global__ void k_post(int n, int mode, double* __restrict__ di, double* __restr
     const int c = chk[q];
     if (!(ri[c] >= nm->in_min[c] && ri[c] <= nm->in_max[c])) ok = false;
   }
+  if (!mass_fractions_in_range<NS>(ri, nm)) ok = false;
   if (T_pred) T_pred[r] = T + dTp;
   if (T_energy) T_energy[r] = T1;
   if (mode == 0) {
@@ -493,8 +512,8 @@ __global__ void k_cell_post(int c0, int rows, double* __restrict__ f, double* __
 #pragma unroll
   for (int m = 0; m < NS; m++) dy[m] = (double)o[m] * nm->out_std[m] + nm->out_mean[m];
   const double dTp = (double)o[NS] * nm->out_std[NS] + nm->out_mean[NS];
-  // rejection reasons, counted in count[2..6]: negative composition, temperature check, T, log p and
-  // log dt outside the training range
+  // rejection reasons, counted in count[2..7]: negative composition, temperature check, T, log p and
+  // log dt outside the training range, a mass fraction outside its (widened) training range
   int why = 0;
 #pragma unroll
   for (int a = 0; a < NS; a++) {
@@ -517,10 +536,11 @@ __global__ void k_cell_post(int c0, int rows, double* __restrict__ f, double* __
     const int c = chk[qq];
     if (!(ri[c] >= nm->in_min[c] && ri[c] <= nm->in_max[c])) why |= 4 << qq;
   }
+  if (!mass_fractions_in_range<NS>(ri, nm)) why |= 32;
   if (why) {
     list[atomicAdd(count, 1)] = t;
 #pragma unroll
-    for (int b = 0; b < 5; b++)
+    for (int b = 0; b < 6; b++)
       if (why >> b & 1) atomicAdd(count + 2 + b, 1);
     return;
   }
@@ -650,7 +670,7 @@ long long sg_cells_rejected(long long* reasons) {
   int h[8] = {};
   if (CS.count) cudaMemcpy(h, CS.count, sizeof(h), cudaMemcpyDeviceToHost);
   if (reasons)
-    for (int b = 0; b < 5; b++) reasons[b] = h[2 + b];
+    for (int b = 0; b < 6; b++) reasons[b] = h[2 + b];
   return h[0];
 }
 }  // namespace ocfd
@@ -821,6 +841,9 @@ int ocfd_gpu_surrogate_train(int n, const double* d_di0, const double* d_e0, con
   double mean[PAD], sd[PAD], mn[PAD], mx[PAD];
   if ((rc = column_stats(n, raw_in, mean, sd, mn, mx, 1.0, st))) return rc;
   for (int c = 0; c < PAD; c++) {
+    // a mass fraction's scale is at least Y_STD_FLOOR: differences far below it (trace species
+    // near zero in every training state) do not become O(1) inputs
+    if (c >= 2 && c < 2 + ns && sd[c] < Y_STD_FLOOR) sd[c] = Y_STD_FLOOR;
     S.norm.in_mean[c] = (float)mean[c];
     S.norm.in_std[c] = (float)sd[c];
     S.norm.in_min[c] = (float)mn[c];
