@@ -716,7 +716,8 @@ def main_jet(a):
         choice, tms = g.autotune(reps=5)
         tiles = {"mode": "auto", "choice": choice,
                  "flow_rhs_visc_after_beside_ms": tms[23:25],
-                 "stage_rhs_species_in_order_beside_ms": tms[25:27]}
+                 "stage_rhs_species_in_order_beside_ms": tms[25:27],
+                 "stage_rhs_species_visc_old_sweeps_ms": tms[27:29]}
     elif a.tiles != "default":
         g.set_tiles([int(x) for x in a.tiles.split(",")])
         tiles = {"mode": "given", "choice": g.tiles()}
@@ -862,10 +863,12 @@ def main_ours(a):
                                   "visc_div_kc8_16_32_64_percell": tms[13:18],
                                   "stored_metrics_flux_xyz_ev_div": tms[18:23],
                                   "flow_rhs_visc_after_beside": tms[23:25],
-                                  "stage_rhs_species_in_order_beside": tms[25:27]},
+                                  "stage_rhs_species_in_order_beside": tms[25:27],
+                                  "stage_rhs_species_visc_old_sweeps": tms[27:29]},
                  "choice_keys": ["flux_x_shape", "flux_y_shape", "flux_z_shape", "visc_ev_kc", "visc_div_kc",
                                  "flux_stored_metrics", "visc_ev_stored_metrics", "visc_div_stored_metrics",
-                                 "stream_switches (1 visc_ev beside the flux sweeps, 2 species chain on a third stream)"]}
+                                 "switches (1 visc_ev beside the flux sweeps, 2 species chain on a third stream, "
+                                 "4 species viscous terms as pencil sweeps)"]}
     chk(L.ocfd_gpu_run(dt, tt, a.warmup, reac, nsub))
     tt += a.warmup * dt
 

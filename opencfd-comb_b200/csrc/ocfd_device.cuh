@@ -102,6 +102,16 @@ __device__ __forceinline__ int nidx(int i, int j, int k) { return (i - 1) + cC.n
 __device__ __forceinline__ unsigned fast_div(unsigned n, unsigned d, unsigned m, int s) {
   return d == 1 ? n : __umulhi(n, m) >> s;
 }
+// x / N for a small integer N: the division the reference evaluates in the exact build, a
+// multiplication by the rounded reciprocal (the same value up to rounding) in the contracted one
+template <int N>
+__device__ __forceinline__ double divc(double x) {
+#if OCFD_FMA_BUILD
+  return x * (1.0 / N);
+#else
+  return x / N;
+#endif
+}
 __device__ __forceinline__ int hstride(int dir) { return dir == 0 ? 1 : (dir == 1 ? cC.HX : cC.HX * cC.HY); }
 
 // gfortran -O3 integer-power chains (GCC powi table): x**3 = x**2*x, x**4 = (x**2)**2, x**5 = x**2*x**3
@@ -291,10 +301,10 @@ __device__ __forceinline__ double dev_E(const double* di, double T) {
     E1 = E1 + c[4] * R1 * di[k];
     Ec = Ec + c[7] * R1 * di[k];
   }
-  if (T <= cC.tct_max) return A1 * T + B1 * q2(T) / 2.0 + C1 * q3(T) / 3.0 + D1 * q4(T) / 4.0 + E1 * q5(T) / 5.0 + Ec;
+  if (T <= cC.tct_max) return A1 * T + B1 * q2(T) / 2.0 + divc<3>(C1 * q3(T)) + D1 * q4(T) / 4.0 + divc<5>(E1 * q5(T)) + Ec;
   double tm = cC.tct_max;
   double cv2 = A1 + B1 * tm + C1 * q2(tm) + D1 * q3(tm) + E1 * q4(tm);
-  return A1 * tm + B1 * q2(tm) / 2.0 + C1 * q3(tm) / 3.0 + D1 * q4(tm) / 4.0 + E1 * q5(tm) / 5.0 + Ec + cv2 * (T - tm);
+  return A1 * tm + B1 * q2(tm) / 2.0 + divc<3>(C1 * q3(tm)) + D1 * q4(tm) / 4.0 + divc<5>(E1 * q5(tm)) + Ec + cv2 * (T - tm);
 }
 template <int NS>
 __device__ __forceinline__ double dev_Cp(double d, const double* di, double T) {
@@ -362,12 +372,12 @@ __device__ __forceinline__ double dev_T(const double* di, double Ein, int* nfail
     }
     double Et1, Ex;
     if (T1 <= cC.tct_max) {
-      Et1 = A1 * T1 + B1 * q2(T1) / 2.0 + C1 * q3(T1) / 3.0 + D1 * q4(T1) / 4.0 + E1 * q5(T1) / 5.0 + Ec;
+      Et1 = A1 * T1 + B1 * q2(T1) / 2.0 + divc<3>(C1 * q3(T1)) + D1 * q4(T1) / 4.0 + divc<5>(E1 * q5(T1)) + Ec;
       Ex = A1 + B1 * T1 + C1 * q2(T1) + D1 * q3(T1) + E1 * q4(T1);
     } else {
       double tm = cC.tct_max;
       Ex = A1 + B1 * tm + C1 * q2(tm) + D1 * q3(tm) + E1 * q4(tm);
-      Et1 = A1 * tm + B1 * q2(tm) / 2.0 + C1 * q3(tm) / 3.0 + D1 * q4(tm) / 4.0 + E1 * q5(tm) / 5.0 + Ec +
+      Et1 = A1 * tm + B1 * q2(tm) / 2.0 + divc<3>(C1 * q3(tm)) + D1 * q4(tm) / 4.0 + divc<5>(E1 * q5(tm)) + Ec +
             Ex * (T1 - tm);
     }
     T2 = T1 - (Et1 - Ein) / Ex;
@@ -398,11 +408,11 @@ __device__ __forceinline__ double dev_hi(int k, double T) {
   int jc = trange(T);
   const double* c = cC.cf[k][jc];
   if (T <= cC.tct_max)
-    return (c[0] * T + c[1] * q2(T) / 2.0 + c[2] * q3(T) / 3.0 + c[3] * q4(T) / 4.0 + c[4] * q5(T) / 5.0 + c[7]) *
+    return (c[0] * T + c[1] * q2(T) / 2.0 + divc<3>(c[2] * q3(T)) + c[3] * q4(T) / 4.0 + divc<5>(c[4] * q5(T)) + c[7]) *
            cC.Ri[k];
   double tm = cC.tct_max;
   double cpm = c[0] + c[1] * tm + c[2] * q2(tm) + c[3] * q3(tm) + c[4] * q4(tm);
-  return (c[0] * tm + c[1] * q2(tm) / 2.0 + c[2] * q3(tm) / 3.0 + c[3] * q4(tm) / 4.0 + c[4] * q5(tm) / 5.0 + c[7] +
+  return (c[0] * tm + c[1] * q2(tm) / 2.0 + divc<3>(c[2] * q3(tm)) + c[3] * q4(tm) / 4.0 + divc<5>(c[4] * q5(tm)) + c[7] +
           cpm * (T - tm)) *
          cC.Ri[k];
 }
@@ -410,12 +420,12 @@ __device__ __forceinline__ double dev_hi(int k, double T) {
 __device__ __forceinline__ double dev_gibbs_jc(int k, int jc, double T, double logT) {
   const double* c = cC.cf[k][jc];
   if (T <= cC.tct_max)
-    return c[0] * (1.0 - logT) * T - c[1] * q2(T) / 2.0 - c[2] * q3(T) / 6.0 - c[3] * q4(T) / 12.0 -
-           c[4] * q5(T) / 20.0 + c[5] - c[6] * T;
+    return c[0] * (1.0 - logT) * T - c[1] * q2(T) / 2.0 - divc<6>(c[2] * q3(T)) - divc<12>(c[3] * q4(T)) -
+           divc<20>(c[4] * q5(T)) + c[5] - c[6] * T;
   double tm = cC.tct_max;
   double cpm = c[0] + c[1] * tm + c[2] * q2(tm) + c[3] * q3(tm) + c[4] * q4(tm);
-  double hm = c[0] * tm + c[1] * q2(tm) / 2.0 + c[2] * q3(tm) / 3.0 + c[3] * q4(tm) / 4.0 + c[4] * q5(tm) / 5.0 + c[5];
-  double sm = c[0] * log(tm) + c[1] * tm + c[2] * q2(tm) / 2.0 + c[3] * q3(tm) / 3.0 + c[4] * q4(tm) / 4.0 + c[6];
+  double hm = c[0] * tm + c[1] * q2(tm) / 2.0 + divc<3>(c[2] * q3(tm)) + c[3] * q4(tm) / 4.0 + divc<5>(c[4] * q5(tm)) + c[5];
+  double sm = c[0] * log(tm) + c[1] * tm + c[2] * q2(tm) / 2.0 + divc<3>(c[3] * q3(tm)) + c[4] * q4(tm) / 4.0 + c[6];
   return hm + cpm * (T - tm) - T * (sm + cpm * log(T / tm));
 }
 __device__ __forceinline__ double dev_gibbs(int k, double T, double logT) { return dev_gibbs_jc(k, trange(T), T, logT); }
