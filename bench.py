@@ -470,8 +470,10 @@ def main_surrogate(a):
 #    write Ev(27),Qp(3) (50); k_scal_div read Ev(27), read + write Dus(9) (45)         = 114
 #  species_rk (k_scal_rk): read Dus(9), din(9), di(9); write di(9)                      = 36
 #  chem (once per step, k_chem_cells): read + write di(9), Et, f5; read T, p            = 22
+# species_visc: k_ci + k_scal_ev + k_scal_div with the species RK update fused in (912 B of the
+# viscous kernels + 288 B of the update - the 144 B of Dus that no longer travel)
 JET_ALG_BYTES = {"flux_x": 88, "flux_y": 128, "flux_z": 128, "visc_ev": 168, "visc_div": 160, "rk_prims": 360,
-                 "transport": 184, "species_flux": 648, "species_visc": 912, "species_rk": 288}
+                 "transport": 184, "species_flux": 648, "species_visc": 1056, "species_rk": 288}
 JET_CHEM_BYTES = 176
 JET_STAGES_PER_STEP = 6
 
@@ -716,8 +718,7 @@ def main_jet(a):
         choice, tms = g.autotune(reps=5)
         tiles = {"mode": "auto", "choice": choice,
                  "flow_rhs_visc_after_beside_ms": tms[23:25],
-                 "stage_rhs_species_in_order_beside_ms": tms[25:27],
-                 "stage_rhs_species_visc_old_sweeps_ms": tms[27:29]}
+                 "stage_rhs_species_in_order_beside_ms": tms[25:27]}
     elif a.tiles != "default":
         g.set_tiles([int(x) for x in a.tiles.split(",")])
         tiles = {"mode": "given", "choice": g.tiles()}
@@ -863,12 +864,10 @@ def main_ours(a):
                                   "visc_div_kc8_16_32_64_percell": tms[13:18],
                                   "stored_metrics_flux_xyz_ev_div": tms[18:23],
                                   "flow_rhs_visc_after_beside": tms[23:25],
-                                  "stage_rhs_species_in_order_beside": tms[25:27],
-                                  "stage_rhs_species_visc_old_sweeps": tms[27:29]},
+                                  "stage_rhs_species_in_order_beside": tms[25:27]},
                  "choice_keys": ["flux_x_shape", "flux_y_shape", "flux_z_shape", "visc_ev_kc", "visc_div_kc",
                                  "flux_stored_metrics", "visc_ev_stored_metrics", "visc_div_stored_metrics",
-                                 "switches (1 visc_ev beside the flux sweeps, 2 species chain on a third stream, "
-                                 "4 species viscous terms as pencil sweeps)"]}
+                                 "stream_switches (1 visc_ev beside the flux sweeps, 2 species chain on a third stream)"]}
     chk(L.ocfd_gpu_run(dt, tt, a.warmup, reac, nsub))
     tt += a.warmup * dt
 

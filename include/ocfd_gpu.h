@@ -298,26 +298,23 @@ int ocfd_gpu_ana_average(int upload, double* fields, int* k_average, double* t_a
  * the viscous-flux kernel and of its divergence kernel; metric form of the flux sweeps, the
  * viscous-flux kernel and the divergence kernel (0 computed from the 1-D grid derivatives of a
  * tensor-product grid, 1 read from the 19 stored arrays, which are then computed once; a general
- * grid always reads them); switches, bit 0: the viscous-flux kernel runs beside the flux sweeps
- * on a second stream (a parallel branch of the step's graph) instead of after them, bit 1: the
- * species chain (species sweeps, then divergence and RK update) runs on a third stream beside the
- * species viscous fluxes and the flow part instead of in order, bit 2: on a tensor-product grid the
- * species viscous terms run as three pencil sweeps instead of the per-point flux and divergence
- * kernels}. Shapes (cells along the
+ * grid always reads them); stream switches, bit 0: the viscous-flux kernel runs beside the flux
+ * sweeps on a second stream (a parallel branch of the step's graph) instead of after them, bit 1:
+ * the species chain (species sweeps, then divergence and RK update) runs on a third stream beside
+ * the species viscous fluxes and the flow part instead of in order}. Shapes (cells along the
  * sweep x pencils): x 56x4, 120x2, 24x8; y / z 24x16, 24x8, 56x8. Every choice gives
  * bit-identical results.
  * ocfd_gpu_autotune times each candidate on the current state (after ocfd_gpu_init_state) over reps
  * launches, applies the fastest and remembers it for this configuration (grid, schemes, species)
  * in the process; reps = 0 applies a remembered choice without timing when there is one. choice
- * (may be NULL) receives the choice; ms (may be NULL, 29 doubles) the mean ms per launch of each
+ * (may be NULL) receives the choice; ms (may be NULL, 27 doubles) the mean ms per launch of each
  * candidate: flux x, y, z shapes 0..2, k_visc_ev at 8, 16, 32, 64 planes, k_visc_div at 8, 16,
  * 32, 64 planes and in its per-cell form (k planes 0), then with the stored metric arrays at the
  * best tiles: flux x, y, z, k_visc_ev, k_visc_div, then the flow right-hand side of a stage with
  * the viscous flux after and beside the flux sweeps, then a stage's right-hand sides without the
- * species RK update with the species chain in order and on the third stream, then with the
- * per-point species viscous kernels and the better of the two before (-1 where not timed). The
- * launches write only scratch arrays, so the solution is unchanged. Default choice
- * {0, 0, 0, 16, 16, 0, 0, 0, 7}. */
+ * species RK update with the species chain in order and on the third stream (-1 where not timed).
+ * The launches write only scratch arrays, so the solution is unchanged. Default choice
+ * {0, 0, 0, 16, 16, 0, 0, 0, 3}. */
 int ocfd_gpu_autotune(int reps, int* choice, double* ms);
 int ocfd_gpu_set_tiles(const int* choice);
 int ocfd_gpu_get_tiles(int* choice);

@@ -45,6 +45,7 @@ struct DevConst {
   int n_tct;
   double tct[OCFD_NTCT_MAX], tct_max;
   double Mi[OCFD_MAX_SPEC], Ri[OCFD_MAX_SPEC];
+  double rMi[OCFD_MAX_SPEC];  // 1 / Mi (the contracted build's mole numbers)
   double cf[OCFD_MAX_SPEC][OCFD_NTCT_MAX][8];  // A,B,C,D,E,F,G,Ect
   double mratio[OCFD_MAX_SPEC][OCFD_MAX_SPEC];  // Mi(i) / Mi(j), for the implicit-Euler matrix
   // transport
@@ -59,6 +60,7 @@ struct DevConst {
   double wk_c[OCFD_MAX_SPEC][OCFD_MAX_SPEC], wk_binv[OCFD_MAX_SPEC][OCFD_MAX_SPEC];
   // species pairs (a, b), a < b, enumerated a-major: pair p = (pair_a[p], pair_b[p])
   unsigned char pair_a[OCFD_MAX_SPEC * (OCFD_MAX_SPEC - 1) / 2], pair_b[OCFD_MAX_SPEC * (OCFD_MAX_SPEC - 1) / 2];
+  unsigned char pair_of[OCFD_MAX_SPEC][OCFD_MAX_SPEC];  // the pair number of (a, b) and (b, a)
   // kinetics
   int nreac, rereac, timeadv;
   int const_p;  // batched reactors: hold each reactor's pressure (extension; the reference is constant-volume)

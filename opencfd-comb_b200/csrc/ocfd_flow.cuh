@@ -960,9 +960,14 @@ __global__ void __launch_bounds__(32 * NS, OCFD_SPECIES_MINB) k_scal_ev(const do
 #ifndef OCFD_SCAL_DIV_MINB
 #define OCFD_SCAL_DIV_MINB 7
 #endif
-template <int NS, bool SEP>
+// RK: the species RK update (k_scal_rk's expressions on the finished Dus value, which then stays in
+// a register instead of making a round trip through HBM; nothing else reads Dus afterwards)
+template <int NS, bool SEP, bool RK = false>
 __global__ void __launch_bounds__(32 * NS, OCFD_SCAL_DIV_MINB) k_scal_div(const double* e1, const double* e2,
-                                                                          const double* e3, double* dus, Geo g) {
+                                                                          const double* e3, double* dus, Geo g,
+                                                                          int krk = 0, double dt = 0.0,
+                                                                          const double* din = nullptr,
+                                                                          double* di = nullptr) {
   const int ks = threadIdx.y;
   int i, j, k;
   const bool ok = cell_of((long long)blockIdx.x * 32 + threadIdx.x, i, j, k);
@@ -973,177 +978,16 @@ __global__ void __launch_bounds__(32 * NS, OCFD_SCAL_DIV_MINB) k_scal_div(const 
   double uk, ui, us;
   cdiff3(e1 + o, e2 + o, e3 + o, q, i, j, k, uk, ui, us);
   double* du = dus + (size_t)ks * cC.N + nn;
-  *du = *du + (uk + ui + us) * jac;
-}
-// du_scaler_viscous on a tensor-product grid as three pencil sweeps instead of k_scal_ev +
-// k_scal_div. Where a cell's metric matrix is diagonal (every cell off the non-periodic end planes),
-// the species diffusion flux along direction d, e_d = (d_s D_s sum_m (dc/dxi_m) A_m,d) A1_d,d + the
-// other terms (exact zeros there), depends only on the derivative of c = d_s / d along d, so one
-// sweep along d forms c's derivative, e_d and its derivative from a pencil tile in shared memory,
-// with no gathers and no e_d arrays in HBM. Cells on the end planes (where the closure residues make
-// the metric full) and the pencil ends take the general point formula of k_scal_ev (all three
-// derivatives of c from the ci array). The x sweep writes P = d e1 / dxi, the y sweep P = P +
-// d e2 / deta, the z sweep du = du + (P + d e3 / dzeta) Jac: the sums of k_scal_div in its order.
-// Each sweep also forms its component of the enthalpy flux Qp in species order. The values equal
-// k_scal_ev / k_scal_div's: each is the same expression (the omitted products are exact zeros of
-// the diagonal metric, which change no finite nonzero result).
-struct ScalSweepArgs {
-  const double *ci, *d, *T, *amd;
-  double* qp;   // the component of Qp along the sweep (N)
-  double* P;    // partial divergence (NS x N)
-  double* dus;  // Dus (NS x N), updated by the z sweep
-  Geo g;
-};
-template <int DIR, int NS, int CD>
-__global__ void __launch_bounds__(FLUX_THREADS) k_scal_sweep(ScalSweepArgs a) {
-  using TL = Tile<DIR, 0>;
-  constexpr int C = TL::C, NL = TL::NL;
-  constexpr int HE = CD == 8 ? 4 : 3;       // stencil half-width of the CD6 / CD8 derivative
-  constexpr int HW = 2 * HE, PC = C + 2 * HW;  // c points of a pencil: the cells and HW each side
-  constexpr int PE = C + 2 * HE;               // e points: the cells and HE on each side
-  __shared__ double sc[PC * NL], se[PE * NL], sA[PE * NL], sA1[PE * NL], sd[PE * NL];
-  __shared__ double sT[C * NL], sq[C * NL];
-  __shared__ int sq_e[PE * NL];  // the e point's cell (hidx) or -1; bit 30 set: general formula
-  __shared__ int sn_e[PE * NL];  // its nidx
-  const int n = DIR == 0 ? cC.nx : (DIR == 1 ? cC.ny : cC.nz);
-  const int nl_max = DIR == 0 ? cC.ny : cC.nx;
-  const int s0 = (DIR == 0 ? blockIdx.x : blockIdx.y) * C + 1;
-  const int l0 = DIR == 0 ? blockIdx.y * NL + 1 : blockIdx.x * NL + 1;
-  const int bz = blockIdx.z + 1;
-  const int ncell = min(C, n - s0 + 1);
-  const bool per = cC.iper[DIR] != 0;
-  auto slot = [&](int p, int l, int P) { return DIR == 0 ? l * P + p : p * NL + l; };
-  auto split = [&](int idx, int P, int& p, int& l) {
-    if (DIR == 0) { p = idx % P; l = idx / P; }
-    else { l = idx % NL; p = idx / NL; }
-  };
-  auto coords = [&](int sw, int l, int& i, int& j, int& k) {
-    if (DIR == 0) { i = sw; j = l0 + l; k = bz; }
-    else if (DIR == 1) { i = l0 + l; j = sw; k = bz; }
-    else { i = l0 + l; j = bz; k = sw; }
-  };
-  // the sweep index a point of a periodic direction takes its values from (the halo copies of an
-  // exchange)
-  auto wrap = [&](int sw) { return per ? ((sw - 1) % n + n) % n + 1 : sw; };
-
-  // per-point set-up shared by the species: the e points' cells, diagonal metrics and density,
-  // the cells' temperature
-  for (int idx = threadIdx.x; idx < PE * NL; idx += FLUX_THREADS) {
-    int p, l;
-    split(idx, PE, p, l);
-    const int sw = s0 - HE + p;
-    int e = -1, nn = 0;
-    if (l0 + l <= nl_max && (per || (sw >= 1 && sw <= n))) {
-      int i, j, k;
-      coords(wrap(sw), l, i, j, k);
-      const int q = hidx(i, j, k);
-      nn = nidx(i, j, k);
-      double xi, yi, zi, xj, yj, zj, xk, yk, zk;
-      bool cross;
-      sep_derivs(a.g, i, j, k, xi, yi, zi, xj, yj, zj, xk, yk, zk, cross);
-      double A[9], A1[9];
-      metric_all<true>(a.g, i, j, k, q, A, A1);
-      sA[idx] = A[4 * DIR];
-      sA1[idx] = A1[4 * DIR];
-      sd[idx] = a.d[q];
-      e = q | (cross ? (1 << 30) : 0);
-    }
-    sq_e[idx] = e;
-    sn_e[idx] = nn;
-  }
-  for (int idx = threadIdx.x; idx < C * NL; idx += FLUX_THREADS) {
-    int p, l;
-    split(idx, C, p, l);
-    if (l0 + l <= nl_max && p < ncell) {
-      int i, j, k;
-      coords(s0 + p, l, i, j, k);
-      sT[idx] = a.T[hidx(i, j, k)];
-    }
-  }
-  const long long H = cC.H, N = cC.N;
-  for (int ks = 0; ks < NS; ks++) {
-    const double* c = a.ci + (size_t)ks * H;
-    const double* amd = a.amd + (size_t)ks * N;
-    __syncthreads();  // the previous species' e values are consumed
-    for (int idx = threadIdx.x; idx < PC * NL; idx += FLUX_THREADS) {
-      int p, l;
-      split(idx, PC, p, l);
-      const int sw = s0 - HW + p;
-      double v = 0.0;
-      if (l0 + l <= nl_max && (per || (sw >= 1 - OCFD_L && sw <= n + OCFD_L))) {
-        int i, j, k;
-        coords(wrap(sw), l, i, j, k);
-        v = __ldg(c + hidx(i, j, k));
-      }
-      sc[idx] = v;
-    }
-    __syncthreads();
-    for (int idx = threadIdx.x; idx < PE * NL; idx += FLUX_THREADS) {
-      const int e = sq_e[idx];
-      if (e < 0) continue;
-      int p, l;
-      split(idx, PE, p, l);
-      const int sw = s0 - HE + p;
-      const int q = e & ((1 << 30) - 1);
-      const double dD = sd[idx] * amd[sn_e[idx]];
-      double Ed, ed;
-      if (!(e >> 30)) {
-        // c's derivative along the sweep from the pencil (closures at non-periodic ends)
-        const double dc = cdiff_g<CD>([&](int m) { return sc[slot(p + HE + m, l, PC)]; }, DIR, wrap(sw), n);
-        Ed = dD * (dc * sA[idx]);
-        ed = Ed * sA1[idx];
-      } else {  // full metric: k_scal_ev's expressions with all three derivatives
-        int i, j, k;
-        coords(wrap(sw), l, i, j, k);
-        double uk, ui, us, A[9], A1[9];
-        cdiff3(c, c, c, q, i, j, k, uk, ui, us);
-        metric_all<true>(a.g, i, j, k, q, A, A1);
-        const double cix = uk * A[0] + ui * A[3] + us * A[6];
-        const double ciy = uk * A[1] + ui * A[4] + us * A[7];
-        const double ciz = uk * A[2] + ui * A[5] + us * A[8];
-        const double E1 = dD * cix, E2 = dD * ciy, E3 = dD * ciz;
-        Ed = DIR == 0 ? E1 : (DIR == 1 ? E2 : E3);
-        ed = E1 * A1[3 * DIR] + E2 * A1[3 * DIR + 1] + E3 * A1[3 * DIR + 2];
-      }
-      se[idx] = ed;
-      const int pc = p - HE;  // the tile's own cells: Qp = 0 before the first species, then + E h
-      if (pc >= 0 && pc < ncell) {
-        const int ic = slot(pc, l, C);
-        const double hq = Ed * dev_hi(ks, sT[ic]);
-        sq[ic] = ks == 0 ? 0.0 + hq : sq[ic] + hq;
-      }
-    }
-    __syncthreads();
-    double* P = a.P + (size_t)ks * N;
-    for (int idx = threadIdx.x; idx < C * NL; idx += FLUX_THREADS) {
-      int p, l;
-      split(idx, C, p, l);
-      if (l0 + l > nl_max || p >= ncell) continue;
-      const double de = cdiff_g<CD>([&](int m) { return se[slot(p + HE + m, l, PE)]; }, DIR, s0 + p, n);
-      int i, j, k;
-      coords(s0 + p, l, i, j, k);
-      const int nn = nidx(i, j, k);
-      if (DIR == 0) {
-        P[nn] = de;
-      } else if (DIR == 1) {
-        P[nn] = P[nn] + de;
-      } else {
-        double* du = a.dus + (size_t)ks * N + nn;
-        *du = *du + (P[nn] + de) * metric_jac<true>(a.g, i, j, k, hidx(i, j, k));
-      }
-    }
-  }
-  __syncthreads();
-  for (int idx = threadIdx.x; idx < C * NL; idx += FLUX_THREADS) {
-    int p, l;
-    split(idx, C, p, l);
-    if (l0 + l > nl_max || p >= ncell) continue;
-    int i, j, k;
-    coords(s0 + p, l, i, j, k);
-    a.qp[nidx(i, j, k)] = sq[idx];
+  const double d1 = *du + (uk + ui + us) * jac;
+  if constexpr (RK) {  // Scalar_time_adv_RK3 (OCFD_Time_Adv.f90:134-166)
+    const double ra[3] = {0.0, 3.0 / 4.0, 1.0 / 3.0}, rb[3] = {1.0, 1.0 / 4.0, 2.0 / 3.0};
+    const size_t oh = o + q, on = (size_t)ks * cC.N + nn;
+    if (krk == 1) di[oh] = din[on] + dt * d1;
+    else di[oh] = ra[krk - 1] * din[on] + rb[krk - 1] * (di[oh] + dt * d1);
+  } else {
+    *du = d1;
   }
 }
-
 // Scalar_time_adv_RK3 (OCFD_Time_Adv.f90:134-166), blockIdx.y = species
 static __global__ void k_scal_rk(int krk, double dt, const double* dus, const double* din, double* di) {
   int i, j, k;
@@ -1186,7 +1030,11 @@ __global__ void __launch_bounds__(32 * NS, OCFD_TRANSPORT_MINB) k_transport(cons
   if (ok) {
     const double d0 = di[(size_t)ks * cC.H + q];
     sD0[ks][lane] = d0;
+#if OCFD_FMA_BUILD
+    sX[ks][lane] = d0 * cC.rMi[ks];  // d0 / Mi up to rounding
+#else
     sX[ks][lane] = d0 / cC.Mi[ks];
+#endif
   }
   if (ks == NS - 1) sL[lane] = log(Tq);
   __syncthreads();
@@ -1280,11 +1128,13 @@ __global__ void __launch_bounds__(32 * NS, OCFD_TRANSPORT_MINB) k_transport(cons
 #pragma unroll
     for (int jj = 0; jj < NS; jj++) {
       if (jj == ks) continue;
-      const int a = ks < jj ? ks : jj, b = ks < jj ? jj : ks;
-      const int pi = a * NS - a * (a + 1) / 2 + (b - a - 1);
-      ds = ds + Xi[jj] * sD2[pi][lane];  // sD2 holds 1 / D2
+      ds = ds + Xi[jj] * sD2[cC.pair_of[ks][jj]][lane];  // sD2 holds 1 / D2
     }
+#if OCFD_FMA_BUILD
+    ad = (1.0 - Xi[ks]) * 1.013e5 / ((ds + 1.0e-20) * p[q]);  // one division; the same up to rounding
+#else
     ad = (1.0 - Xi[ks]) / (ds + 1.0e-20) * 1.013e5 / p[q];
+#endif
   }
   amd[(size_t)ks * cC.N + nn] = ad;
 }

@@ -104,9 +104,8 @@ struct Lib {
   // third stream of a stage with species (N_SPEC > 1): the species sweeps, the species viscous
   // divergence and the species RK update run beside the transport, Qp and flow kernels
   cudaStream_t st3 = nullptr;
-  cudaEvent_t ev_sp_fork = nullptr, ev_se_done = nullptr, ev_sp_join = nullptr, ev_sp_inv = nullptr;
+  cudaEvent_t ev_sp_fork = nullptr, ev_se_done = nullptr, ev_sp_join = nullptr;
   bool fork_species = true;
-  bool scal_sweeps = true;  // species viscous terms as pencil sweeps on a tensor-product grid
   bool fork_visc = true;
   cudaGraph_t gstep = nullptr;
   int* ht_counter = nullptr;
@@ -550,29 +549,6 @@ void stage_t(int krk, double dt1) {
 // divergence, and with rk the species RK update) and the flow (flow_rhs_t). Without rk it writes
 // only arrays that every stage recomputes before reading them (Dus, ci, the species viscous
 // fluxes, Qp, du, Ev), which the tuner uses to time it on the current state.
-// one direction of the species viscous pencil sweeps (tiles of Tile<DIR, 0>, like the flux sweeps)
-template <int NS, int DIR>
-void scal_sweep_dir() {
-  if constexpr (NS > 1) {
-    using TL = Tile<DIR, 0>;
-    const int nx = L->P.nx, ny = L->P.ny, nz = L->P.nz;
-    auto nb = [](int n, int b) { return (unsigned)((n + b - 1) / b); };
-    const dim3 grid = DIR == 0 ? dim3(nb(nx, TL::C), nb(ny, TL::NL), nz)
-                    : DIR == 1 ? dim3(nb(nx, TL::NL), nb(ny, TL::C), nz)
-                               : dim3(nb(nx, TL::NL), nb(nz, TL::C), ny);
-    ScalSweepArgs sa{L->ci, L->d, L->T, L->amd, L->qp[DIR], L->se[0], L->dus, L->geo};
-    if (L->hc.cd8_on) k_scal_sweep<DIR, NS, 8><<<grid, FLUX_THREADS, 0, L->st>>>(sa);
-    else k_scal_sweep<DIR, NS, 6><<<grid, FLUX_THREADS, 0, L->st>>>(sa);
-    LAUNCH_CHECK();
-  }
-}
-template <int NS>
-void scal_sweep(int dir) {
-  if (dir == 0) scal_sweep_dir<NS, 0>();
-  else if (dir == 1) scal_sweep_dir<NS, 1>();
-  else scal_sweep_dir<NS, 2>();
-}
-
 template <int NS>
 void stage_rhs_t(int krk, double dt1, bool rk) {
   const long long N = L->hc.N, H = L->hc.H;
@@ -596,20 +572,26 @@ void stage_rhs_t(int krk, double dt1, bool rk) {
     std::swap(L->st, L->st3);
   };
   const bool sp_visc = NS > 1 && L->P.if_viscous == 1;
-  // on a tensor-product grid the species viscous terms run as three pencil sweeps (k_scal_sweep);
-  // the z sweep adds into Dus, so it follows the species sweeps, and it writes Qp's z component,
-  // which the flow part reads, so it runs on the main stream
-  const bool vsweeps = sp_visc && L->sep && L->scal_sweeps;
   auto species_sweeps = [&]() {
     const int grp = NS % 3 == 0 ? 3 : 1;
     FluxArgs fs = fa;
     fs.fs = L->di;
     fs.out = L->dus;
     for (int dd = 0; dd < 3; dd++) launch_flux(dd, fs, grp, NS / grp);
-    if (spfork && vsweeps) CK(cudaEventRecord(L->ev_sp_inv, L->st));
   };
   auto species_div_rk = [&]() {
-    if (sp_visc && !vsweeps) {
+    if (sp_visc && rk) {  // the divergence with the species RK update fused in
+      KTimer t(KC_SPECIES_VISC);
+      if (L->sep)
+        k_scal_div<NS, true, true><<<nblk(N, 32), dim3(32, NS), 0, L->st>>>(L->se[0], L->se[1], L->se[2], L->dus,
+                                                                          L->geo, krk, dt1, L->din, L->di);
+      else
+        k_scal_div<NS, false, true><<<nblk(N, 32), dim3(32, NS), 0, L->st>>>(L->se[0], L->se[1], L->se[2], L->dus,
+                                                                           L->geo, krk, dt1, L->din, L->di);
+      LAUNCH_CHECK();
+      return;
+    }
+    if (sp_visc) {
       KTimer t(KC_SPECIES_VISC);
       if (L->sep) k_scal_div<NS, true><<<nblk(N, 32), dim3(32, NS), 0, L->st>>>(L->se[0], L->se[1], L->se[2], L->dus, L->geo);
       else k_scal_div<NS, false><<<nblk(N, 32), dim3(32, NS), 0, L->st>>>(L->se[0], L->se[1], L->se[2], L->dus, L->geo);
@@ -629,15 +611,7 @@ void stage_rhs_t(int krk, double dt1, bool rk) {
     } else {
       species_sweeps();
     }
-    if (vsweeps) {
-      KTimer t(KC_SPECIES_VISC);
-      k_ci<<<dim3(nblk(H, 256), NS), 256, 0, L->st>>>(L->di, L->d, L->ci, H);
-      LAUNCH_CHECK();
-      scal_sweep<NS>(0);
-      scal_sweep<NS>(1);
-      if (spfork) CK(cudaStreamWaitEvent(L->st, L->ev_sp_inv, 0));
-      scal_sweep<NS>(2);
-    } else if (sp_visc) {
+    if (sp_visc) {
       {
         KTimer t(KC_SPECIES_VISC);
         k_ci<<<dim3(nblk(H, 256), NS), 256, 0, L->st>>>(L->di, L->d, L->ci, H);
@@ -708,7 +682,7 @@ void chem_t(double dt2, int nsub) {
 // which block computes a point, not how; the stored metric arrays hold the values the separable
 // form computes), so the tuner is free to pick by time alone. Choices are remembered per
 // configuration in the process.
-constexpr int TUNE_N = 9, TUNE_TIMES = 3 * FLUX_TILE_SHAPES + 9 + 5 + 2 + 2 + 2;
+constexpr int TUNE_N = 9, TUNE_TIMES = 3 * FLUX_TILE_SHAPES + 9 + 5 + 2 + 2;
 std::map<std::string, std::array<int, TUNE_N>> g_tune_cache;
 
 std::string tune_key() {
@@ -761,7 +735,6 @@ void apply_tiles(const int* c) {
   L->met_div = c[7] != 0;
   L->fork_visc = (c[8] & 1) != 0;
   L->fork_species = (c[8] & 2) != 0;
-  L->scal_sweeps = (c[8] & 4) != 0;
   drop_graphs();  // the captured step holds the old launches
 }
 
@@ -805,7 +778,7 @@ void tune_t(int reps, int* best, double* ms) {
     }
     best[3] = best[4] = VE_KC;
     best[5] = best[6] = best[7] = L->sep ? 0 : 1;
-    best[8] = NS > 1 ? 7 : 1;
+    best[8] = NS > 1 ? 3 : 1;
     for (int m = 3 * FLUX_TILE_SHAPES; m < TUNE_TIMES; m++) ms[m] = -1.0;
     if (P.if_viscous == 1) {
       double t_ev = 1e300, t_div = 1e300;
@@ -887,21 +860,11 @@ void tune_t(int reps, int* best, double* ms) {
       L->met_ev = best[6] && L->sep;
       L->met_div = best[7] && L->sep;
       L->fork_visc = (best[8] & 1) != 0;
-      L->scal_sweeps = true;
       L->fork_species = false;
       ms[M2] = timed([&] { stage_rhs_t<NS>(1, 0.0, false); });
       L->fork_species = true;
       ms[M2 + 1] = timed([&] { stage_rhs_t<NS>(1, 0.0, false); });
-      best[8] = (best[8] & 1) | (ms[M2 + 1] < ms[M2] ? 2 : 0) | 4;
-      if (P.if_viscous == 1 && L->sep) {  // the species viscous terms as k_scal_ev + k_scal_div instead
-        const int M3 = M2 + 2;
-        L->fork_species = (best[8] & 2) != 0;
-        L->scal_sweeps = false;
-        ms[M3] = timed([&] { stage_rhs_t<NS>(1, 0.0, false); });
-        L->scal_sweeps = true;
-        ms[M3 + 1] = std::min(ms[M2], ms[M2 + 1]);
-        if (ms[M3] < ms[M3 + 1]) best[8] &= ~4;
-      }
+      best[8] = (best[8] & 1) | (ms[M2 + 1] < ms[M2] ? 2 : 0);
     }
   } catch (...) {
     cudaEventDestroy(e0);
@@ -1062,6 +1025,7 @@ void fill_thermo(DevConst& c, const ocfd_thermo* th, int realgas) {
   c.tct_max = th->tct_max;
   for (int k = 0; k < th->n_spec; k++) {
     c.Mi[k] = th->mi[k];
+    c.rMi[k] = 1.0 / th->mi[k];
     c.Ri[k] = 8.314 / th->mi[k];
     double ect = 0.0;
     for (int j = 0; j < th->n_tct; j++) {
@@ -1143,6 +1107,7 @@ void fill_trans(DevConst& c, const ocfd_transport* tr, int ns) {
     for (int b = a + 1; b < ns; b++) {
       c.pair_a[np] = (unsigned char)a;
       c.pair_b[np] = (unsigned char)b;
+      c.pair_of[a][b] = c.pair_of[b][a] = (unsigned char)np;
       np++;
     }
 }
@@ -1184,7 +1149,6 @@ void release() {
   if (L->ev_sp_fork) cudaEventDestroy(L->ev_sp_fork);
   if (L->ev_se_done) cudaEventDestroy(L->ev_se_done);
   if (L->ev_sp_join) cudaEventDestroy(L->ev_sp_join);
-  if (L->ev_sp_inv) cudaEventDestroy(L->ev_sp_inv);
   if (L->st3) cudaStreamDestroy(L->st3);
   if (L->st) cudaStreamDestroy(L->st);
   delete L;
@@ -1501,7 +1465,6 @@ int ocfd_gpu_init(const ocfd_params* p, const ocfd_thermo* th, const ocfd_kineti
     CK(cudaEventCreateWithFlags(&L->ev_sp_fork, cudaEventDisableTiming));
     CK(cudaEventCreateWithFlags(&L->ev_se_done, cudaEventDisableTiming));
     CK(cudaEventCreateWithFlags(&L->ev_sp_join, cudaEventDisableTiming));
-    CK(cudaEventCreateWithFlags(&L->ev_sp_inv, cudaEventDisableTiming));
     DevConst& c = L->hc;
     c.nx = p->nx; c.ny = p->ny; c.nz = p->nz; c.ns = p->n_spec;
     fast_divisor((unsigned)p->nx, c.mx, c.sx);
@@ -2499,8 +2462,8 @@ int ocfd_gpu_set_tiles(const int* choice) {
         g_err = "metric forms must be 0 or 1";
         return OCFD_ERR_PARAM;
       }
-    if (choice[8] < 0 || choice[8] > 7) {
-      g_err = "the stream and species-sweep switches (choice[8]) must be 0..7";
+    if (choice[8] < 0 || choice[8] > 3) {
+      g_err = "the stream switches (choice[8]) must be 0..3";
       return OCFD_ERR_PARAM;
     }
     apply_tiles(choice);
@@ -2516,7 +2479,7 @@ int ocfd_gpu_get_tiles(int* choice) {
   choice[5] = L->sep ? (int)L->met_flux : 1;
   choice[6] = L->sep ? (int)L->met_ev : 1;
   choice[7] = L->sep ? (int)L->met_div : 1;
-  choice[8] = (int)L->fork_visc | (int)L->fork_species << 1 | (int)L->scal_sweeps << 2;
+  choice[8] = (int)L->fork_visc | (int)L->fork_species << 1;
   return 0;
 }
 

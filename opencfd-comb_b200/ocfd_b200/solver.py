@@ -229,15 +229,14 @@ class Solver:
         """Times the candidate tile shapes on the current state and applies the fastest; returns
         (choice, ms per launch of each candidate)."""
         ch = (C.c_int * 9)()
-        ms = (C.c_double * 29)()
+        ms = (C.c_double * 27)()
         _chk(lib().ocfd_gpu_autotune(reps, ch, ms))
         return list(ch), list(ms)
 
     def set_tiles(self, choice):
         """choice: 9 ints (see ocfd_gpu_autotune); a shorter choice keeps the computed metric
-        form and the switches of the defaults (choice[8] = 7: both side streams, species viscous
-        pencil sweeps)."""
-        choice = list(choice) + [0, 0, 0, 7][len(choice) - 5:] if len(choice) < 9 else list(choice)
+        form and the stream switches of the defaults (choice[8] = 3: both side streams)."""
+        choice = list(choice) + [0, 0, 0, 3][len(choice) - 5:] if len(choice) < 9 else list(choice)
         ch = (C.c_int * 9)(*choice)
         _chk(lib().ocfd_gpu_set_tiles(ch))
 
