@@ -871,14 +871,22 @@ __global__ void __launch_bounds__(256, OCFD_VDIV_MINB) k_visc_div_pc(DivArgs a) 
 #pragma unroll
   for (int m = 0; m < 4; m++) duc[m] = a.du[(size_t)(m + 1) * N + nn];
   const double ajac = metric_jac<SEP>(a.g, i, j, k, q);
+  // an interior cell (most cells) takes cdiff3's straight-line path: each component's 18 (CD6) or
+  // 24 (CD8) stencil loads are issued together; the closures of the end planes go per direction
+  const bool inner = cdiff_interior(0, i, cC.nx) && cdiff_interior(1, j, cC.ny) && cdiff_interior(2, k, cC.nz);
 #pragma unroll
   for (int m = 0; m < 4; m++) {
-    const double* e1 = a.ev[m] + q;
-    const double* e2 = a.ev[4 + m] + q;
-    const double* e3 = a.ev[8 + m] + q;
-    double uk = cdiff_g<CD>([&](int o) { return __ldg(e1 + o); }, 0, i, cC.nx);
-    double ui = cdiff_g<CD>([&](int o) { return __ldg(e2 + o * sy); }, 1, j, cC.ny);
-    double us = cdiff_g<CD>([&](int o) { return __ldg(e3 + o * sz); }, 2, k, cC.nz);
+    double uk, ui, us;
+    if (inner) {
+      cdiff3(a.ev[m], a.ev[4 + m], a.ev[8 + m], q, i, j, k, uk, ui, us);
+    } else {
+      const double* e1 = a.ev[m] + q;
+      const double* e2 = a.ev[4 + m] + q;
+      const double* e3 = a.ev[8 + m] + q;
+      uk = cdiff_g<CD>([&](int o) { return __ldg(e1 + o); }, 0, i, cC.nx);
+      ui = cdiff_g<CD>([&](int o) { return __ldg(e2 + o * sy); }, 1, j, cC.ny);
+      us = cdiff_g<CD>([&](int o) { return __ldg(e3 + o * sz); }, 2, k, cC.nz);
+    }
     a.du[(size_t)(m + 1) * N + nn] = duc[m] + (uk + ui + us) * ajac;
   }
 }
