@@ -1,4 +1,4 @@
-"""Save and show without a host sync (SURVEY f1): snapshots packed on the device and copied to
+"""Save and show without a host sync: snapshots packed on the device and copied to
 pinned memory on a copy stream while the next steps run equal the state at the snapshot bit for
 bit; the asynchronous show_flow_msg equals the synchronous one; save_flow_data_async writes the
 reference's OCFD-comb<Istep>.dat layout byte for byte as a synchronous save would."""
