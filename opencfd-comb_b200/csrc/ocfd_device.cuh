@@ -24,6 +24,12 @@ struct DevConst {
   // fast_divisor, filled by the host)
   unsigned mx, my;
   int sx, sy;
+  // slab order of the gather-bound per-cell kernels: tiles of jt rows (a power of two dividing ny),
+  // each walked plane by plane (k), so the z neighbours of a cell were read a few planes earlier
+  // by the same tile; magic pairs of the slab (jt nx) and tile (jt nx nz) cell counts
+  int jt;
+  unsigned m_slab, m_tile;
+  int s_slab, s_tile;
   int HX, HY, HZ;
   long long H, N;
   int iper[3];

@@ -553,6 +553,24 @@ __device__ __forceinline__ bool cell_of(long long t64, int& i, int& j, int& k) {
   return true;
 }
 
+// the cell of linear index t in slab order (DevConst::jt): tiles of jt rows, each plane by plane;
+// consecutive threads still take consecutive i (a warp reads one row), and every cell is visited
+// once, so kernels give the same values in either order
+__device__ __forceinline__ bool cell_of_slab(long long t64, int& i, int& j, int& k) {
+  if (t64 >= cC.N) return false;
+  const unsigned t = (unsigned)t64, nx = (unsigned)cC.nx, jt = (unsigned)cC.jt;
+  const unsigned tile = jt * nx * (unsigned)cC.nz, slab = jt * nx;
+  const unsigned tj = fast_div(t, tile, cC.m_tile, cC.s_tile);
+  const unsigned r = t - tj * tile;
+  const unsigned k0 = fast_div(r, slab, cC.m_slab, cC.s_slab);
+  const unsigned r2 = r - k0 * slab;
+  const unsigned jj = fast_div(r2, nx, cC.mx, cC.sx);
+  i = (int)(r2 - jj * nx) + 1;
+  j = (int)(tj * jt + jj) + 1;
+  k = (int)k0 + 1;
+  return true;
+}
+
 struct ViscArgs {
   const double *d, *u, *v, *w, *T, *di;
   const double *amu, *amk;        // precomputed transport (NS > 1) or nullptr
@@ -863,7 +881,7 @@ template <bool SEP, int HZ>
 __global__ void __launch_bounds__(256, OCFD_VDIV_MINB) k_visc_div_pc(DivArgs a) {
   constexpr int CD = HZ == 3 ? 6 : 8;
   int i, j, k;
-  if (!cell_of((long long)blockIdx.x * blockDim.x + threadIdx.x, i, j, k)) return;
+  if (!cell_of_slab((long long)blockIdx.x * blockDim.x + threadIdx.x, i, j, k)) return;
   const int q = hidx(i, j, k), nn = nidx(i, j, k);
   const int sy = hstride(1), sz = hstride(2);
   const long long N = cC.N;
@@ -920,7 +938,7 @@ __global__ void __launch_bounds__(32 * NS, OCFD_SPECIES_MINB) k_scal_ev(const do
   __shared__ double sq[3][NS][32];
   const int ks = threadIdx.y, lane = threadIdx.x;
   int i, j, k;
-  const bool ok = cell_of((long long)blockIdx.x * 32 + lane, i, j, k);
+  const bool ok = cell_of_slab((long long)blockIdx.x * 32 + lane, i, j, k);
   int nn = 0;
   if (ok) {
     const int q = hidx(i, j, k);
@@ -978,7 +996,7 @@ __global__ void __launch_bounds__(32 * NS, OCFD_SCAL_DIV_MINB) k_scal_div(const 
                                                                           double* di = nullptr) {
   const int ks = threadIdx.y;
   int i, j, k;
-  const bool ok = cell_of((long long)blockIdx.x * 32 + threadIdx.x, i, j, k);
+  const bool ok = cell_of_slab((long long)blockIdx.x * 32 + threadIdx.x, i, j, k);
   if (!ok) return;
   const int q = hidx(i, j, k), nn = nidx(i, j, k);
   const double jac = metric_jac<SEP>(g, i, j, k, q);  // every species' thread (no barrier)

@@ -1469,6 +1469,10 @@ int ocfd_gpu_init(const ocfd_params* p, const ocfd_thermo* th, const ocfd_kineti
     c.nx = p->nx; c.ny = p->ny; c.nz = p->nz; c.ns = p->n_spec;
     fast_divisor((unsigned)p->nx, c.mx, c.sx);
     fast_divisor((unsigned)p->ny, c.my, c.sy);
+    c.jt = 1;
+    while (c.jt < 32 && p->ny % (2 * c.jt) == 0) c.jt *= 2;
+    fast_divisor((unsigned)(c.jt * p->nx), c.m_slab, c.s_slab);
+    fast_divisor((unsigned)(c.jt * p->nx * p->nz), c.m_tile, c.s_tile);
     c.HX = p->nx + 2 * OCFD_L; c.HY = p->ny + 2 * OCFD_L; c.HZ = p->nz + 2 * OCFD_L;
     c.H = (long long)c.HX * c.HY * c.HZ;
     c.N = (long long)p->nx * p->ny * p->nz;
